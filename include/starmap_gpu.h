@@ -1,0 +1,160 @@
+/*
+ * starmap_gpu.h -- C ABI of the B200 (sm_100a, FP64) time-stepping library
+ * that replaces the time loop of StaRMAP's starmap_solver(par).
+ *
+ * The reference is MATLAB/GNU Octave.  Its solver function
+ *     output = starmap_solver(par)            (starmap_solver.m:1)
+ * keeps its host-side setup (starmap_solver.m:55-157: flags, grid-type
+ * classification, staggered grids, hook sampling, first-step materials,
+ * decay factors, source and filter tables, starmap_solver.m:165-305) and hands
+ * the arrays to this library once; the library runs the whole Strang-split loop
+ * (starmap_solver.m:307-421) on one GPU and returns the final components.
+ * A MEX/oct gateway, a ctypes binding or any other FFI binds these symbols:
+ * only plain pointers, sizes and POD structs cross the boundary.
+ *
+ * Conventions
+ *   - Every entry point returns SMG_OK (0) or a negative SMG_E* code; the
+ *     message of the last failure on a handle is smg_last_error(handle), and
+ *     of a failed smg_create / handle-less call smg_last_error(NULL).
+ *   - Arrays follow MATLAB's column-major order.  Component j lives on the
+ *     staggered grid gt[3*j+d] (1 = cell centres, 2 = staggered points) and
+ *     has extent n[d] along solver dimension d, or n[d]+1 when gt == 2 and
+ *     bc[d] == 1 (starmap_solver.m:113-126).
+ *   - Components and fields are 0-based here (component 0 = MATLAB U{1}).
+ *   - Host buffers are borrowed for the duration of the call only.
+ *   - A handle is used by one host thread at a time.  All GPU work of a
+ *     handle runs on its own CUDA stream; entry points that return host data
+ *     synchronise that stream.
+ */
+#ifndef STARMAP_GPU_H
+#define STARMAP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden default visibility; everything declared
+ * here is exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define SMG_OK          0
+#define SMG_EINVAL     -1   /* inconsistent or unsupported input (MATLAB would error()) */
+#define SMG_ECUDA      -2   /* CUDA runtime/launch failure */
+#define SMG_ETIMEOUT   -3   /* a bounded device wait gave up (batched grid barrier) */
+#define SMG_ENONFINITE -4   /* non-finite state detected by smg_check_finite */
+#define SMG_ENOMEM     -5   /* device allocation failed */
+#define SMG_ESTATE     -6   /* call out of order (e.g. run before the state is set) */
+
+#define SMG_FILTER_NONE    0   /* par.f_position = ''          */
+#define SMG_FILTER_SUBSTEP 1   /* par.f_position = 'substep'   */
+#define SMG_FILTER_FULL    2   /* par.f_position = 'full'      */
+
+typedef struct smg_handle smg_handle;
+
+/* One coefficient array of the solver: sT1{g,m}, ET{g,m}, sA1, EA, Q{j} or a
+ * filterTerm{g,m[,k]}.  data == NULL means the reference held a scalar
+ * (hooks may return scalars, which MATLAB broadcasts); otherwise data points to
+ * a column-major array with the extents of grid `grid`. */
+typedef struct smg_field {
+    const double* data;
+    double scalar;
+    int32_t grid[3];            /* grid type per solver dimension, 1 or 2 */
+} smg_field;
+
+/* Problem descriptor: everything starmap_solver.m holds when it enters the
+ * update loop at starmap_solver.m:307. */
+typedef struct smg_problem {
+    int32_t n_sys;              /* number of moment components, length(par.Mz) */
+    int32_t n[3];               /* par.n (solver ordering; 2D: [1 nx ny]) */
+    int32_t bc[3];              /* par.bc: 0 periodic, 1 extrapolation */
+    double  h[3];               /* grid spacing, starmap_solver.m:101 */
+    const int32_t* gt;          /* [3*n_sys] grid type per component and dimension */
+    const double* Mx;           /* [n_sys*n_sys] column-major par.Mx */
+    const double* My;           /* [n_sys*n_sys] column-major par.My */
+    const double* Mz;           /* [n_sys*n_sys] column-major par.Mz */
+    int32_t n_fields;           /* number of entries in `fields` */
+    const smg_field* fields;
+    const int32_t* sigma_t;     /* [n_sys] field of sT1{gt(j),mom_order(j)} (entry 0 unused) */
+    const int32_t* decay_t;     /* [n_sys] field of ET{...}, or NULL: computed on the GPU by smg_set_dt */
+    int32_t sigma_a;            /* field of sA1 = sA{1,1,1} */
+    int32_t decay_a;            /* field of EA, or -1: computed on the GPU by smg_set_dt */
+    const int32_t* source;      /* [n_sys] field of Q{j}, -1 = zero (not in par.source_ind) */
+    int32_t filter_mode;        /* SMG_FILTER_* */
+    const int32_t* filter1;     /* [n_sys] filterTerm{..,k=1} (substep) or filterTerm (full); -1 = 1 */
+    const int32_t* filter2;     /* [n_sys] filterTerm{..,k=2} (substep only); -1 = 1 */
+} smg_problem;
+
+/* Library version string. */
+const char* smg_version(void);
+
+/* Message of the last failure on `h` (or of the last handle-less failure). */
+const char* smg_last_error(const smg_handle* h);
+
+/* Number of visible CUDA devices (>= 0), or a negative SMG_E* code. */
+int smg_device_count(void);
+
+/* Validate the descriptor, build the coupling tables (the Ix/Iy/Iz lists of
+ * starmap_solver.m:77-79 in sumcell order, starmap_solver.m:350-351/398-399),
+ * allocate device memory and upload the coefficient fields.
+ * Replaces: starmap_solver.m:136-157 (field allocation) on the device side. */
+int smg_create(const smg_problem* p, smg_handle** out);
+
+/* Release all device memory and the stream of `h`. */
+void smg_destroy(smg_handle* h);
+
+/* Upload the state: U[j] is the column-major host array of component j
+ * (U{j} of starmap_solver.m:140-146).  Pointers may not be NULL. */
+int smg_set_state(smg_handle* h, const double* const* U);
+
+/* Download the state into per-component host arrays; a NULL entry skips that
+ * component (used for par.mom_output subsets).  Synchronises the stream. */
+int smg_get_state(smg_handle* h, double* const* U);
+
+/* Replace the values of one coefficient field (time-dependent sources,
+ * materials or filters re-evaluated by the host between steps,
+ * starmap_solver.m:214-252, 278-305). */
+int smg_set_field(smg_handle* h, int32_t field, const double* data, double scalar);
+
+/* Set the time step.  Decay factors not supplied by the host (decay_t NULL,
+ * decay_a -1) are computed on the GPU as expm1div(-sigma*dt/2)
+ * (starmap_solver.m:267-274, 531-535) at this point. */
+int smg_set_dt(smg_handle* h, double dt);
+
+/* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
+ * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
+ * handle's stream; the step loop is replayed from a captured CUDA graph. */
+int smg_run(smg_handle* h, int64_t nsteps);
+
+/* Wait for all work of `h`. */
+int smg_sync(smg_handle* h);
+
+/* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the
+ * handle's stream) and its launch count. */
+int smg_last_run_stats(smg_handle* h, double* ms, int64_t* launches);
+
+/* Device bytes held by `h`, and the padded device layout of one component
+ * (elements per row, rows per plane, planes, component stride). */
+int smg_layout(const smg_handle* h, int64_t* bytes, int64_t dims_out[4]);
+
+/* Scan the state for NaN/Inf on the GPU; returns SMG_ENONFINITE if any. */
+int smg_check_finite(smg_handle* h);
+
+/* Grid-type classification of starmap_solver.m:76-98 from the sparsity of
+ * par.Mx/My/Mz (column-major n_sys x n_sys): writes gt_out[3*j+d] in {1,2}.
+ * Host-only helper for callers that do not classify themselves. */
+int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz,
+                 int32_t* gt_out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STARMAP_GPU_H */

@@ -1,0 +1,532 @@
+// smg_api.cu -- C ABI entry points of libstarmap_gpu (include/starmap_gpu.h).
+//
+// Host runtime: descriptor validation, kernel-axis layout, the coupling lists
+// of the reference (Ix/Iy/Iz, starmap_solver.m:77-79, folded in sumcell order,
+// starmap_solver.m:350-351, 516-519), coefficient upload, the step loop
+// (starmap_solver.m:310-421) replayed from a captured CUDA graph, and state
+// transfer in MATLAB's column-major component layout.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/starmap_gpu.h"
+#include "smg_internal.h"
+
+using smg::DevComp;
+using smg::DevCoup;
+using smg::DevField;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;   // last handle-less failure
+
+int fail(smg_handle* h, int code, const std::string& msg) {
+    if (h) {
+        h->err = msg;
+    } else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_err = msg;
+    }
+    return code;
+}
+
+int cuda_fail(smg_handle* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return fail(h, SMG_ENOMEM, m);
+    return fail(h, SMG_ECUDA, m);
+}
+
+#define SMG_CUDA(h, expr)                                      \
+    do {                                                       \
+        cudaError_t e_ = (expr);                               \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, #expr); \
+    } while (0)
+
+// expm1div of the reference (starmap_solver.m:531-535) for scalar fields.
+double expm1div_host(double x) {
+    double y = 1 + x * .5 + x * x / 6;
+    if (std::fabs(x) > 2e-4) y = (std::exp(x) - 1) / x;
+    return y;
+}
+
+int extent(int n, int bc, int g) { return (g == 2 && bc == 1) ? n + 1 : n; }
+
+void free_device(smg_handle* h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    cudaFree(h->dU);
+    cudaFree(h->dFields);
+    cudaFree(h->dComps);
+    cudaFree(h->dCoups);
+    cudaFree(h->dFieldTab);
+    cudaFree(h->dDest);
+    cudaFree(h->dFlag);
+    h->dU = h->dFields = nullptr;
+    h->dComps = nullptr;
+    h->dCoups = nullptr;
+    h->dFieldTab = nullptr;
+    h->dDest = h->dFlag = nullptr;
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->ev0 = h->ev1 = nullptr;
+    h->stream = nullptr;
+}
+
+// Copy a column-major host array with extents e[] (kernel axes) into a
+// padded device slot (and back).
+cudaError_t put_slot(const smg_handle* h, double* dst, const double* src, const int e[3]) {
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
+    p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+    p.kind = cudaMemcpyHostToDevice;
+    return cudaMemcpy3DAsync(&p, h->stream);
+}
+
+cudaError_t get_slot(const smg_handle* h, double* dst, const double* src, const int e[3]) {
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
+    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+    p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+    p.kind = cudaMemcpyDeviceToHost;
+    return cudaMemcpy3DAsync(&p, h->stream);
+}
+
+void grid_extents(const smg_handle* h, const int gt_solver[3], int e[3]) {
+    for (int a = 0; a < 3; ++a) {
+        const int d = h->sd[a];
+        e[a] = extent(h->g.n[a], h->g.bc[a], gt_solver[d]);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* smg_version(void) { return "starmap_b200 0.1 (sm_100a, fp64)"; }
+
+const char* smg_last_error(const smg_handle* h) {
+    if (h) return h->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_err.c_str();
+}
+
+int smg_device_count(void) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return 0;
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    return n;
+}
+
+int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz, int32_t* gt_out) {
+    if (n_sys < 1 || !Mx || !My || !Mz || !gt_out) return fail(nullptr, SMG_EINVAL, "smg_classify: bad arguments");
+    const double* M[3] = {Mx, My, Mz};
+    // I[d][j]: sorted columns i with M_d(j,i) != 0 (starmap_solver.m:77-79)
+    std::vector<std::vector<int>> I[3];
+    for (int d = 0; d < 3; ++d) {
+        I[d].resize(n_sys);
+        for (int j = 0; j < n_sys; ++j)
+            for (int i = 0; i < n_sys; ++i)
+                if (M[d][j + (size_t)i * n_sys] != 0.0) I[d][j].push_back(i);
+    }
+    // class index = (gx-1) + 2(gy-1) + 4(gz-1); membership flags
+    std::vector<int> cls(n_sys, -1);
+    cls[0] = 0;
+    int assigned = 1;
+    // Fixed-point propagation: a component reached from class (gx,gy,gz) via
+    // direction d lies on the class with that axis flipped (starmap_solver.m:82-91).
+    for (int iter = 0; iter < 4 * n_sys + 8 && assigned < n_sys; ++iter) {
+        bool changed = false;
+        for (int j = 0; j < n_sys; ++j) {
+            if (cls[j] < 0) continue;
+            for (int d = 0; d < 3; ++d)
+                for (int i : I[d][j]) {
+                    const int c = cls[j] ^ (1 << d);
+                    if (cls[i] < 0) { cls[i] = c; ++assigned; changed = true; }
+                }
+        }
+        if (!changed) break;
+    }
+    if (assigned < n_sys)
+        return fail(nullptr, SMG_EINVAL, "smg_classify: components not connected to component 1");
+    for (int j = 0; j < n_sys; ++j)
+        for (int d = 0; d < 3; ++d) gt_out[3 * j + d] = 1 + ((cls[j] >> d) & 1);
+    return SMG_OK;
+}
+
+int smg_create(const smg_problem* p, smg_handle** out) {
+    if (!p || !out) return fail(nullptr, SMG_EINVAL, "smg_create: NULL argument");
+    *out = nullptr;
+    const int ns = p->n_sys;
+    if (ns < 1) return fail(nullptr, SMG_EINVAL, "n_sys must be >= 1");
+    if (!p->gt || !p->Mx || !p->My || !p->Mz) return fail(nullptr, SMG_EINVAL, "gt/Mx/My/Mz must be given");
+    if (!p->sigma_t || !p->source) return fail(nullptr, SMG_EINVAL, "sigma_t/source tables must be given");
+    if (p->n_fields < 0 || (p->n_fields > 0 && !p->fields)) return fail(nullptr, SMG_EINVAL, "bad field table");
+    if (p->filter_mode < 0 || p->filter_mode > 2) return fail(nullptr, SMG_EINVAL, "filter_mode must be 0, 1 or 2");
+    if (p->filter_mode != 0 && !p->filter1) return fail(nullptr, SMG_EINVAL, "filter1 table required");
+    if (p->filter_mode == 1 && !p->filter2) return fail(nullptr, SMG_EINVAL, "filter2 table required for substep");
+    for (int d = 0; d < 3; ++d) {
+        if (p->n[d] < 1) return fail(nullptr, SMG_EINVAL, "n[d] must be >= 1");
+        if (p->bc[d] != 0 && p->bc[d] != 1) return fail(nullptr, SMG_EINVAL, "bc[d] must be 0 or 1");
+        if (!(p->h[d] > 0.0) || !std::isfinite(p->h[d])) return fail(nullptr, SMG_EINVAL, "h[d] must be finite and > 0");
+    }
+    for (int j = 0; j < ns; ++j)
+        for (int d = 0; d < 3; ++d)
+            if (p->gt[3 * j + d] != 1 && p->gt[3 * j + d] != 2) return fail(nullptr, SMG_EINVAL, "gt entries must be 1 or 2");
+    auto bad_field = [&](int f, bool allow_none) {
+        return allow_none ? (f < -1 || f >= p->n_fields) : (f < 0 || f >= p->n_fields);
+    };
+    for (int f = 0; f < p->n_fields; ++f)
+        for (int d = 0; d < 3; ++d)
+            if (p->fields[f].grid[d] != 1 && p->fields[f].grid[d] != 2)
+                return fail(nullptr, SMG_EINVAL, "field grid types must be 1 or 2");
+    if (bad_field(p->sigma_a, false)) return fail(nullptr, SMG_EINVAL, "sigma_a field index out of range");
+    if (bad_field(p->decay_a, true)) return fail(nullptr, SMG_EINVAL, "decay_a field index out of range");
+    for (int j = 1; j < ns; ++j) {
+        if (bad_field(p->sigma_t[j], false)) return fail(nullptr, SMG_EINVAL, "sigma_t field index out of range");
+        if (p->decay_t && bad_field(p->decay_t[j], false)) return fail(nullptr, SMG_EINVAL, "decay_t field index out of range");
+    }
+    for (int j = 0; j < ns; ++j) {
+        if (bad_field(p->source[j], true)) return fail(nullptr, SMG_EINVAL, "source field index out of range");
+        if (p->filter_mode != 0 && bad_field(p->filter1[j], true)) return fail(nullptr, SMG_EINVAL, "filter1 index out of range");
+        if (p->filter_mode == 1 && bad_field(p->filter2[j], true)) return fail(nullptr, SMG_EINVAL, "filter2 index out of range");
+    }
+
+    smg_handle* h = new smg_handle();
+    h->n_sys = ns;
+    // kernel axes: non-singleton solver dimensions first, in solver order
+    int gt2[3] = {0, 0, 0};
+    for (int j = 0; j < ns; ++j)
+        for (int d = 0; d < 3; ++d) gt2[d] |= (p->gt[3 * j + d] == 2);
+    bool active[3];
+    for (int d = 0; d < 3; ++d) active[d] = p->n[d] > 1 || (p->bc[d] == 1 && gt2[d]);
+    int a = 0;
+    for (int d = 0; d < 3; ++d) if (active[d]) h->sd[a++] = d;
+    for (int d = 0; d < 3; ++d) if (!active[d]) h->sd[a++] = d;
+    int axis_of[3];
+    for (int k = 0; k < 3; ++k) axis_of[h->sd[k]] = k;
+    for (int k = 0; k < 3; ++k) {
+        const int d = h->sd[k];
+        h->g.n[k] = p->n[d];
+        h->g.bc[k] = p->bc[d];
+        h->g.h[k] = p->h[d];
+        h->g.B[k] = p->n[d] + ((p->bc[d] == 1 && gt2[d]) ? 1 : 0);
+    }
+    h->g.s1 = ((long long)h->g.B[0] + 7) / 8 * 8;
+    h->g.s2 = h->g.s1 * h->g.B[1];
+    h->g.cs = (h->g.s2 * h->g.B[2] + 31) / 32 * 32;
+
+    // components and couplings in sumcell order
+    h->comps.resize(ns);
+    const double* M[3] = {p->Mx, p->My, p->Mz};
+    for (int j = 0; j < ns; ++j) {
+        DevComp& c = h->comps[j];
+        grid_extents(h, &p->gt[3 * j], c.ext);
+        c.cbeg = (int)h->coups.size();
+        for (int d = 0; d < 3; ++d) {
+            for (int i = 0; i < ns; ++i) {
+                const double w = M[d][j + (size_t)i * ns];
+                if (w == 0.0) continue;
+                const int gi = p->gt[3 * i + d];
+                // the staggered difference of component i along d lives on the
+                // grid of i with axis d flipped; MATLAB adds it elementwise to
+                // W_j, so the extents must agree (else the reference errors).
+                int eD[3];
+                int gflip[3] = {p->gt[3 * i], p->gt[3 * i + 1], p->gt[3 * i + 2]};
+                gflip[d] = 3 - gi;
+                grid_extents(h, gflip, eD);
+                if (eD[0] != c.ext[0] || eD[1] != c.ext[1] || eD[2] != c.ext[2]) {
+                    delete h;
+                    char buf[160];
+                    std::snprintf(buf, sizeof buf, "coupling M%c(%d,%d) joins grids of different extents", "xyz"[d], j + 1, i + 1);
+                    return fail(nullptr, SMG_EINVAL, buf);
+                }
+                h->coups.push_back(DevCoup{i, axis_of[d] * 2 + (gi == 2 ? 1 : 0), w});
+            }
+        }
+        c.cend = (int)h->coups.size();
+        int ntwo = (p->gt[3 * j] == 2) + (p->gt[3 * j + 1] == 2) + (p->gt[3 * j + 2] == 2);
+        c.order = 0;
+        (ntwo % 2 ? h->destA : h->destB).push_back(j);
+    }
+    if (h->destB.empty() || h->destB[0] != 0) {
+        delete h;
+        return fail(nullptr, SMG_EINVAL, "component 1 must lie on grid (1,1,1)");
+    }
+
+    // field table: user fields, then constants ONE and ZERO, then device-derived decays
+    const int nf = p->n_fields;
+    h->field_one = nf;
+    h->field_zero = nf + 1;
+    int nfields = nf + 2;
+    h->derived_decay.assign(nf, -1);
+    h->sigma_t_field.assign(ns, -1);
+    h->decay_t_field.assign(ns, -1);
+    h->sigma_a = p->sigma_a;
+    h->decay_a = p->decay_a;
+    h->filter_mode = p->filter_mode;
+    auto need_derived = [&](int sf) {
+        if (h->derived_decay[sf] < 0) h->derived_decay[sf] = nfields++;
+        return h->derived_decay[sf];
+    };
+    for (int j = 1; j < ns; ++j) {
+        h->sigma_t_field[j] = p->sigma_t[j];
+        h->decay_t_field[j] = p->decay_t ? p->decay_t[j] : need_derived(p->sigma_t[j]);
+    }
+    if (p->decay_a < 0) h->derived_decay_a = need_derived(p->sigma_a);
+    h->fields_host.assign(nfields, DevField{nullptr, 0.0});
+    h->field_grid.assign(nfields, 0);
+    // slots for array fields
+    std::vector<int> slot(nfields, -1);
+    int nslots = 0;
+    for (int f = 0; f < nf; ++f) {
+        h->field_grid[f] = (p->fields[f].grid[0] - 1) | ((p->fields[f].grid[1] - 1) << 1) | ((p->fields[f].grid[2] - 1) << 2);
+        if (p->fields[f].data) slot[f] = nslots++;
+        h->fields_host[f].s = p->fields[f].scalar;
+    }
+    h->fields_host[h->field_one].s = 1.0;
+    h->fields_host[h->field_zero].s = 0.0;
+    for (int f = 0; f < nf; ++f) {
+        const int df = h->derived_decay[f];
+        if (df >= 0) {
+            h->field_grid[df] = h->field_grid[f];
+            if (p->fields[f].data) slot[df] = nslots++;
+        }
+    }
+    h->nslots = nslots;
+    for (int j = 0; j < ns; ++j) {
+        DevComp& c = h->comps[j];
+        c.sT = j ? h->sigma_t_field[j] : h->field_zero;
+        c.ET = j ? h->decay_t_field[j] : h->field_one;
+        c.Q = p->source[j] >= 0 ? p->source[j] : h->field_zero;
+        c.F1 = (p->filter_mode != 0 && p->filter1[j] >= 0) ? p->filter1[j] : h->field_one;
+        c.F2 = (p->filter_mode == 1 && p->filter2[j] >= 0) ? p->filter2[j] : h->field_one;
+    }
+
+    // device allocations
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "cudaStreamCreate");
+        delete h;
+        return r;
+    }
+    auto alloc = [&](void** ptr, size_t bytes) -> cudaError_t {
+        if (bytes == 0) bytes = 16;
+        cudaError_t r = cudaMalloc(ptr, bytes);
+        if (r == cudaSuccess) h->bytes += bytes;
+        return r;
+    };
+    const size_t slot_bytes = (size_t)h->g.cs * 8;
+    if ((e = alloc((void**)&h->dU, slot_bytes * ns)) != cudaSuccess ||
+        (e = alloc((void**)&h->dFields, slot_bytes * (size_t)std::max(nslots, 1))) != cudaSuccess ||
+        (e = alloc((void**)&h->dComps, sizeof(DevComp) * ns)) != cudaSuccess ||
+        (e = alloc((void**)&h->dCoups, sizeof(DevCoup) * std::max<size_t>(h->coups.size(), 1))) != cudaSuccess ||
+        (e = alloc((void**)&h->dFieldTab, sizeof(DevField) * nfields)) != cudaSuccess ||
+        (e = alloc((void**)&h->dDest, sizeof(int) * ns)) != cudaSuccess ||
+        (e = alloc((void**)&h->dFlag, sizeof(int))) != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "cudaMalloc");
+        free_device(h);
+        delete h;
+        return r;
+    }
+    for (int f = 0; f < nfields; ++f)
+        if (slot[f] >= 0) h->fields_host[f].p = h->dFields + (size_t)slot[f] * h->g.cs;
+    std::vector<int> dest(h->destA);
+    dest.insert(dest.end(), h->destB.begin(), h->destB.end());
+#define CREATE_CUDA(expr)                                   \
+    do {                                                    \
+        cudaError_t e_ = (expr);                            \
+        if (e_ != cudaSuccess) {                            \
+            int r_ = cuda_fail(nullptr, e_, #expr);         \
+            free_device(h);                                 \
+            delete h;                                       \
+            return r_;                                      \
+        }                                                   \
+    } while (0)
+    CREATE_CUDA(cudaMemsetAsync(h->dU, 0, slot_bytes * ns, h->stream));
+    CREATE_CUDA(cudaMemsetAsync(h->dFields, 0, slot_bytes * (size_t)std::max(nslots, 1), h->stream));
+    CREATE_CUDA(cudaMemcpyAsync(h->dComps, h->comps.data(), sizeof(DevComp) * ns, cudaMemcpyHostToDevice, h->stream));
+    if (!h->coups.empty())
+        CREATE_CUDA(cudaMemcpyAsync(h->dCoups, h->coups.data(), sizeof(DevCoup) * h->coups.size(), cudaMemcpyHostToDevice, h->stream));
+    CREATE_CUDA(cudaMemcpyAsync(h->dDest, dest.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, h->stream));
+    for (int f = 0; f < nf; ++f) {
+        if (!p->fields[f].data) continue;
+        int e3[3];
+        grid_extents(h, p->fields[f].grid, e3);
+        CREATE_CUDA(put_slot(h, const_cast<double*>(h->fields_host[f].p), p->fields[f].data, e3));
+    }
+    CREATE_CUDA(cudaMemcpyAsync(h->dFieldTab, h->fields_host.data(), sizeof(DevField) * nfields, cudaMemcpyHostToDevice, h->stream));
+    CREATE_CUDA(cudaEventCreate(&h->ev0));
+    CREATE_CUDA(cudaEventCreate(&h->ev1));
+    CREATE_CUDA(cudaStreamSynchronize(h->stream));
+#undef CREATE_CUDA
+    *out = h;
+    return SMG_OK;
+}
+
+void smg_destroy(smg_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_device(h);
+    delete h;
+}
+
+int smg_set_state(smg_handle* h, const double* const* U) {
+    if (!h || !U) return fail(h, SMG_EINVAL, "smg_set_state: NULL argument");
+    for (int j = 0; j < h->n_sys; ++j)
+        if (!U[j]) return fail(h, SMG_EINVAL, "smg_set_state: NULL component pointer");
+    for (int j = 0; j < h->n_sys; ++j)
+        SMG_CUDA(h, put_slot(h, h->dU + (size_t)j * h->g.cs, U[j], h->comps[j].ext));
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->state_set = true;
+    return SMG_OK;
+}
+
+int smg_get_state(smg_handle* h, double* const* U) {
+    if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_state: NULL argument");
+    for (int j = 0; j < h->n_sys; ++j)
+        if (U[j]) SMG_CUDA(h, get_slot(h, U[j], h->dU + (size_t)j * h->g.cs, h->comps[j].ext));
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
+int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_field: NULL handle");
+    if (f < 0 || f >= h->field_one) return fail(h, SMG_EINVAL, "smg_set_field: field index out of range");
+    DevField& F = h->fields_host[f];
+    if ((F.p == nullptr) != (data == nullptr))
+        return fail(h, SMG_EINVAL, "smg_set_field: a field cannot change between scalar and array");
+    if (data) {
+        int gts[3] = {1 + (h->field_grid[f] & 1), 1 + ((h->field_grid[f] >> 1) & 1), 1 + ((h->field_grid[f] >> 2) & 1)};
+        int e3[3];
+        grid_extents(h, gts, e3);
+        SMG_CUDA(h, put_slot(h, const_cast<double*>(F.p), data, e3));
+    } else {
+        F.s = scalar;
+        SMG_CUDA(h, cudaMemcpyAsync(h->dFieldTab + f, &F, sizeof(DevField), cudaMemcpyHostToDevice, h->stream));
+    }
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (h->dt_set) return smg_set_dt(h, h->dt);   // refresh derived decays
+    return SMG_OK;
+}
+
+int smg_set_dt(smg_handle* h, double dt) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_dt: NULL handle");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, SMG_EINVAL, "smg_set_dt: dt must be finite and > 0");
+    h->dt = dt;
+    h->hdt = dt / 2;
+    for (int f = 0; f < (int)h->derived_decay.size(); ++f) {
+        const int df = h->derived_decay[f];
+        if (df < 0) continue;
+        DevField& S = h->fields_host[f];
+        DevField& D = h->fields_host[df];
+        if (S.p) {
+            SMG_CUDA(h, smg::launch_decay(const_cast<double*>(D.p), S.p, h->g.cs, dt, h->stream));
+        } else {
+            D.s = expm1div_host(-S.s * dt / 2);
+        }
+    }
+    SMG_CUDA(h, cudaMemcpyAsync(h->dFieldTab, h->fields_host.data(), sizeof(DevField) * h->fields_host.size(),
+                                cudaMemcpyHostToDevice, h->stream));
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (h->graph) {   // kernel arguments (dt/2) are baked into the graph
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        h->graph_steps = 0;
+    }
+    h->dt_set = true;
+    return SMG_OK;
+}
+
+static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s) {
+    for (int64_t k = 0; k < nsteps; ++k) {
+        cudaError_t e;
+        if ((e = smg::launch_phase(h, 0, 1, s)) != cudaSuccess) return e;
+        if ((e = smg::launch_phase(h, 1, 0, s)) != cudaSuccess) return e;
+        if ((e = smg::launch_phase(h, 0, 2, s)) != cudaSuccess) return e;
+        if (h->filter_mode == 2 && (e = smg::launch_full_filter(h, s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int smg_run(smg_handle* h, int64_t nsteps) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_run: NULL handle");
+    if (nsteps < 0) return fail(h, SMG_EINVAL, "smg_run: nsteps must be >= 0");
+    if (!h->dt_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_dt has not been called");
+    if (!h->state_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_state has not been called");
+    const int64_t kBlock = 16;   // steps per captured graph
+    int64_t left = nsteps;
+    if (left >= kBlock) {
+        if (!h->graph || h->graph_steps != kBlock) {
+            if (h->graph) cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+            cudaGraph_t gr;
+            SMG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = enqueue_steps(h, kBlock, h->stream);
+            cudaError_t e2 = cudaStreamEndCapture(h->stream, &gr);
+            if (e != cudaSuccess) return cuda_fail(h, e, "capture step block");
+            if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&h->graph, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+            h->graph_steps = kBlock;
+        }
+    }
+    SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    for (; left >= kBlock; left -= kBlock) SMG_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
+    SMG_CUDA(h, enqueue_steps(h, left, h->stream));
+    SMG_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    h->last_launches = nsteps * smg::launches_per_step(h);
+    return SMG_OK;
+}
+
+int smg_sync(smg_handle* h) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_sync: NULL handle");
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
+int smg_last_run_stats(smg_handle* h, double* ms, int64_t* launches) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_last_run_stats: NULL handle");
+    SMG_CUDA(h, cudaEventSynchronize(h->ev1));
+    float f = 0.f;
+    SMG_CUDA(h, cudaEventElapsedTime(&f, h->ev0, h->ev1));
+    if (ms) *ms = f;
+    if (launches) *launches = h->last_launches;
+    return SMG_OK;
+}
+
+int smg_layout(const smg_handle* h, int64_t* bytes, int64_t dims_out[4]) {
+    if (!h) return fail(nullptr, SMG_EINVAL, "smg_layout: NULL handle");
+    if (bytes) *bytes = (int64_t)h->bytes;
+    if (dims_out) {
+        dims_out[0] = h->g.s1;
+        dims_out[1] = h->g.B[1];
+        dims_out[2] = h->g.B[2];
+        dims_out[3] = h->g.cs;
+    }
+    return SMG_OK;
+}
+
+int smg_check_finite(smg_handle* h) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_check_finite: NULL handle");
+    int flag = 0;
+    SMG_CUDA(h, cudaMemsetAsync(h->dFlag, 0, sizeof(int), h->stream));
+    SMG_CUDA(h, smg::launch_finite(h, h->dFlag, h->stream));
+    SMG_CUDA(h, cudaMemcpyAsync(&flag, h->dFlag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (flag) return fail(h, SMG_ENONFINITE, "state holds NaN or Inf");
+    return SMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// smg_device.cuh -- device-side data structures and arithmetic of the
+// staggered-grid moment update (StaRMAP starmap_solver.m:307-421).
+//
+// Layout in HBM: every component (and every coefficient field) occupies one
+// slot of `cs` doubles, a padded box of B[0] x B[1] x B[2] points with row
+// pitch s1 (>= B[0], a multiple of 8 doubles) and plane pitch s2 = s1*B[1].
+// Kernel axis 0 is the first non-singleton solver dimension, so the padded box
+// keeps MATLAB's column-major order of each component.  A component on a grid
+// with a smaller extent simply leaves the last row/plane of its slot unused.
+//
+// Arithmetic: the update is written with explicit round-to-nearest intrinsics
+// (no FMA contraction) in the order MATLAB/Octave evaluates the reference's
+// array expressions, so that with identical decay/filter factors the GPU
+// reproduces the CPU restatement bit for bit.
+#pragma once
+#include <cstdint>
+
+namespace smg {
+
+constexpr int kMaxDims = 3;
+
+struct DevGrid {
+    int n[3];          // cells per kernel axis
+    int bc[3];         // boundary condition per kernel axis
+    int B[3];          // box extents per kernel axis
+    long long s1;      // row pitch (elements)
+    long long s2;      // plane pitch (elements)
+    long long cs;      // component slot stride (elements)
+    double h[3];       // grid spacing per kernel axis
+};
+
+struct DevField {      // coefficient: array slot (p != nullptr) or scalar s
+    const double* p;
+    double s;
+};
+
+struct DevComp {
+    int ext[3];        // extents of this component's grid per kernel axis
+    int cbeg, cend;    // range in the coupling table
+    int sT, ET, Q, F1, F2;   // field indices
+    int order;         // moment order (ordering helper; not used by arithmetic)
+};
+
+// One term of W_j = -sum_i M_d(j,i) * d_d U_i, in sumcell order.
+// code = axis*2 + (source grid type along that axis == 2 ? 1 : 0)
+struct DevCoup {
+    int src;
+    int code;
+    double w;
+};
+
+struct DevArgs {
+    DevGrid g;
+    double* U;                 // state, n_sys slots
+    const DevComp* comps;
+    const DevCoup* coups;
+    const DevField* fields;
+    const int* dest;           // component list updated by this phase
+    int ndest;
+    int group;                 // destinations per CTA
+    int sA, EA;                // fields of component 0 in phase B
+    double hdt;                // dt/2
+    int filter_substep;        // 1 if f_position == 'substep'
+};
+
+__device__ __forceinline__ double fld(const DevField* f, int i, long long pt) {
+    const DevField F = f[i];
+    return F.p ? __ldg(F.p + pt) : F.s;
+}
+
+// U + (dt/2)*(W + Q - s.*U).*E  with MATLAB's evaluation order
+// (starmap_solver.m:352-354, 402, 404-406).
+__device__ __forceinline__ double upd(double u, double W, double q, double s, double E, double hdt) {
+    const double t1 = __dadd_rn(W, q);
+    const double t2 = __dmul_rn(s, u);
+    const double t3 = __dsub_rn(t1, t2);
+    const double t4 = __dmul_rn(hdt, t3);
+    const double t5 = __dmul_rn(t4, E);
+    return __dadd_rn(u, t5);
+}
+
+// Neighbour indices of the staggered difference along one axis, expressed as
+// the reference's diff over the extension vectors (starmap_solver.m:127-132):
+//   source on centres (g = 1) -> value on staggered points
+//     bc 0: U[(p+1) mod n] - U[p]           bc 1: U[min(p,n-1)] - U[max(p-1,0)]
+//   source on staggered points (g = 2) -> value on centres
+//     bc 0: U[p] - U[(p-1) mod n]           bc 1: U[p+1] - U[p]
+__device__ __forceinline__ void stencil(int p, int n, int bc, int g2, int& hi, int& lo) {
+    if (!g2) {
+        if (bc) { hi = p < n - 1 ? p : n - 1; lo = p > 0 ? p - 1 : 0; }
+        else    { hi = (p + 1 == n) ? 0 : p + 1; lo = p; }
+    } else {
+        if (bc) { hi = p + 1; lo = p; }
+        else    { hi = p; lo = (p == 0) ? n - 1 : p - 1; }
+    }
+}
+
+}  // namespace smg

@@ -1,0 +1,57 @@
+// smg_internal.h -- host-side structures shared by the library's translation
+// units (not part of the public ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "smg_device.cuh"
+
+struct smg_handle {
+    // problem
+    int n_sys = 0;
+    int sd[3] = {0, 1, 2};           // solver dimension of each kernel axis
+    smg::DevGrid g{};
+    std::vector<smg::DevComp> comps;
+    std::vector<smg::DevCoup> coups;
+    std::vector<int> destA, destB;   // outer set (phase A), inner set (phase B)
+    std::vector<smg::DevField> fields_host;  // device view of the field table
+    std::vector<int> field_grid;     // packed grid type of each field (for uploads)
+    std::vector<int> sigma_t_field, decay_t_field;   // per component
+    std::vector<int> derived_decay;  // field index -> decay field computed on device (or -1)
+    int sigma_a = -1, decay_a = -1, derived_decay_a = -1;
+    int filter_mode = 0;
+    int field_one = -1, field_zero = -1;
+    // device memory
+    double* dU = nullptr;
+    double* dFields = nullptr;       // slots for array fields
+    smg::DevComp* dComps = nullptr;
+    smg::DevCoup* dCoups = nullptr;
+    smg::DevField* dFieldTab = nullptr;
+    int* dDest = nullptr;            // destA followed by destB
+    int* dFlag = nullptr;            // device status word (finite check)
+    size_t bytes = 0;
+    int nslots = 0;
+    // run state
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double dt = 0.0, hdt = 0.0;
+    bool dt_set = false, state_set = false;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    // CUDA graph of a block of steps
+    cudaGraphExec_t graph = nullptr;
+    int64_t graph_steps = 0;
+    std::string err;
+};
+
+namespace smg {
+// kernels (smg_phase.cu)
+cudaError_t launch_phase(const smg_handle* h, int phase, int kfilter, cudaStream_t s);
+cudaError_t launch_full_filter(const smg_handle* h, cudaStream_t s);
+cudaError_t launch_decay(double* out, const double* sigma, long long n, double dt, cudaStream_t s);
+cudaError_t launch_finite(const smg_handle* h, int* flag, cudaStream_t s);
+int launches_per_step(const smg_handle* h);
+}  // namespace smg

@@ -1,0 +1,529 @@
+"""``output = starmap_solver(par)`` on the GPU.
+
+Host side of the drop-in for StaRMAP's ``starmap_solver.m``.  The setup that
+the reference performs before its update loop stays on the host and follows
+the reference statement by statement (flags :58-71, grid-type classification
+:76-98 -- computed by the library's ``smg_classify`` --, h and dt :100-110,
+staggered grids :112-134, initial and source fields :136-146, materials, dt,
+decay factors, source and filter tables at the first step :165-305).  The time
+loop itself (:307-421) runs in ``libstarmap_gpu.so`` through the C ABI of
+``include/starmap_gpu.h``; the final components come back in the reference's
+``output`` layout (:484-500) and the reference's summary is printed (:477-482).
+
+Autonomous problems run the whole loop in one library call (a replayed CUDA
+graph).  Time-dependent materials, sources or filters are re-evaluated on the
+host every step exactly where the reference does, uploaded with
+``smg_set_field`` and advanced one step at a time.  Output times ``t_plot``
+with a user ``output`` hook are served by running the loop in segments and
+interpolating linearly in time as the reference does (:425-473).
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import FILTER_FULL, FILTER_NONE, FILTER_SUBSTEP, SmgError, check, dptr, iptr
+from .init import _noop_output, capargs, nargin, zero
+
+__all__ = ["starmap_solver", "GpuSolver", "prepare", "expm1div", "colon", "step_times"]
+
+
+def expm1div(x):
+    """(exp(x)-1)/x with the reference's Taylor branch (starmap_solver.m:531-535)."""
+    x = np.asarray(x, dtype=np.float64)
+    y = 1 + x * .5 + x ** 2 / 6
+    ind = np.abs(x) > 2e-4
+    if y.ndim == 0:
+        return np.float64((np.exp(x) - 1) / x) if ind else np.float64(y)
+    y = y.copy()
+    y[ind] = (np.exp(x[ind]) - 1) / x[ind]
+    return y
+
+
+def colon(a, d, b):
+    """Octave range ``a:d:b``: base + k*increment, last element clamped to the limit."""
+    n = int(math.floor((b - a) / d + 1e-10)) + 1
+    if n <= 0:
+        return np.zeros(0)
+    v = a + np.arange(n) * d
+    if n > 1:
+        v[-1] = min(a + (n - 1) * d, b)
+    return v
+
+
+def step_times(dt: float, tfinal: float):
+    """Times after each step of the autonomous loop (starmap_solver.m:165, 276).
+
+    dt is fixed after the first step, so the loop overshoots tfinal."""
+    ts = []
+    t = 0.0
+    while t < tfinal:
+        t = t + dt
+        ts.append(t)
+    return ts
+
+
+class GpuSolver:
+    """Owner of one ``smg_handle``: the problem on the GPU."""
+
+    def __init__(self, n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
+                 decay_t=None, decay_a=-1, filter_mode=FILTER_NONE, filter1=None, filter2=None):
+        L = _lib.lib()
+        self._L = L
+        n_sys = int(np.asarray(Mz).shape[0])
+        self.n_sys = n_sys
+        self.n = [int(v) for v in n]
+        self.bc = [int(v) for v in bc]
+        self.gt = np.ascontiguousarray(np.asarray(gt, dtype=np.int32).reshape(n_sys, 3))
+        self._keep = []
+
+        def i32(a):
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+            self._keep.append(arr)
+            return arr
+
+        mats = [np.asfortranarray(np.asarray(M, dtype=np.float64)) for M in (Mx, My, Mz)]
+        self._keep += mats
+        fa = (_lib.smg_field * max(len(fields), 1))()
+        for k, (val, grid) in enumerate(fields):
+            fa[k].grid[:] = [int(g) for g in grid]
+            if np.ndim(val) == 0:
+                fa[k].data = None
+                fa[k].scalar = float(val)
+            else:
+                arr = np.asfortranarray(np.asarray(val, dtype=np.float64)).ravel(order="F")
+                arr = np.ascontiguousarray(arr)
+                self._keep.append(arr)
+                fa[k].data = dptr(arr)
+                fa[k].scalar = 0.0
+        self._fields = fa
+        self.field_grids = [tuple(int(g) for g in grid) for _, grid in fields]
+        p = _lib.smg_problem()
+        p.n_sys = n_sys
+        p.n[:] = self.n
+        p.bc[:] = self.bc
+        p.h[:] = [float(v) for v in h]
+        gtf = i32(self.gt.ravel())
+        p.gt = iptr(gtf)
+        p.Mx, p.My, p.Mz = (dptr(m) for m in mats)
+        p.n_fields = len(fields)
+        p.fields = C_cast_fields(fa)
+        p.sigma_t = iptr(i32(sigma_t))
+        p.decay_t = iptr(i32(decay_t)) if decay_t is not None else None
+        p.sigma_a = int(sigma_a)
+        p.decay_a = int(decay_a)
+        p.source = iptr(i32(source))
+        p.filter_mode = int(filter_mode)
+        p.filter1 = iptr(i32(filter1)) if filter1 is not None else None
+        p.filter2 = iptr(i32(filter2)) if filter2 is not None else None
+        handle = _lib.C.c_void_p()
+        check(L.smg_create(_lib.C.byref(p), _lib.C.byref(handle)))
+        self.h = handle
+        self._keep = []
+
+    # ------------------------------------------------------------------
+    def extents(self, j):
+        return tuple((self.n[d] + 1) if (self.gt[j, d] == 2 and self.bc[d] == 1) else self.n[d] for d in range(3))
+
+    def grid_extents(self, grid):
+        return tuple((self.n[d] + 1) if (grid[d] == 2 and self.bc[d] == 1) else self.n[d] for d in range(3))
+
+    def set_state(self, U):
+        arrs = []
+        for j in range(self.n_sys):
+            a = np.broadcast_to(np.asarray(U[j], dtype=np.float64), self.extents(j))
+            arrs.append(np.ascontiguousarray(np.asfortranarray(a).ravel(order="F")))
+        ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)(*[dptr(a) for a in arrs])
+        check(self._L.smg_set_state(self.h, ptrs), self.h)
+
+    def get_state(self, which=None):
+        which = range(self.n_sys) if which is None else which
+        out = {}
+        ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
+        for j in which:
+            e = self.extents(j)
+            buf = np.empty(int(np.prod(e)), dtype=np.float64)
+            out[j] = (buf, e)
+            ptrs[j] = dptr(buf)
+        check(self._L.smg_get_state(self.h, ptrs), self.h)
+        return {j: buf.reshape(e, order="F") for j, (buf, e) in out.items()}
+
+    def set_field(self, k, val):
+        if np.ndim(val) == 0:
+            check(self._L.smg_set_field(self.h, int(k), None, float(val)), self.h)
+        else:
+            e = self.grid_extents(self.field_grids[k])
+            arr = np.ascontiguousarray(np.asfortranarray(
+                np.broadcast_to(np.asarray(val, dtype=np.float64), e)).ravel(order="F"))
+            check(self._L.smg_set_field(self.h, int(k), dptr(arr), 0.0), self.h)
+
+    def set_dt(self, dt):
+        check(self._L.smg_set_dt(self.h, float(dt)), self.h)
+
+    def run(self, nsteps):
+        check(self._L.smg_run(self.h, int(nsteps)), self.h)
+
+    def sync(self):
+        check(self._L.smg_sync(self.h), self.h)
+
+    def last_run_stats(self):
+        ms = _lib.C.c_double()
+        nl = _lib.C.c_int64()
+        check(self._L.smg_last_run_stats(self.h, _lib.C.byref(ms), _lib.C.byref(nl)), self.h)
+        return ms.value, nl.value
+
+    def layout(self):
+        b = _lib.C.c_int64()
+        d = (_lib.C.c_int64 * 4)()
+        check(self._L.smg_layout(self.h, _lib.C.byref(b), d), self.h)
+        return b.value, list(d)
+
+    def check_finite(self):
+        return self._L.smg_check_finite(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.smg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def C_cast_fields(fa):
+    return _lib.C.cast(fa, _lib.C.POINTER(_lib.smg_field))
+
+
+# ----------------------------------------------------------------------
+# Reference setup (starmap_solver.m:55-305) and the loop driver
+# ----------------------------------------------------------------------
+class _Setup:
+    pass
+
+
+def _as_field(v, shape):
+    a = np.asarray(v, dtype=np.float64)
+    if a.ndim == 0:
+        return np.float64(a)
+    return np.broadcast_to(a, shape)
+
+
+def prepare(par: dict) -> _Setup:
+    """Host-side setup of starmap_solver.m:55-157 (no GPU work)."""
+    S = _Setup()
+    par = dict(par)
+    Mx, My, Mz = (np.asarray(par[k], dtype=np.float64) for k in ("Mx", "My", "Mz"))
+    n_sys = Mz.shape[0]
+    flag_filter = ("filterfunction" in par) and ("f_position" in par) and ("mom_order" in par)
+    f_mom_order = np.atleast_1d(np.asarray(par["mom_order"])).astype(int) if "mom_order" in par else None
+    if not flag_filter:
+        par["filterfunction"] = _ones
+        par["f_position"] = ""
+    flag_ani = ("sigma_sm" in par) and ("mom_order" in par)
+    if not flag_ani:
+        par["mom_order"] = np.concatenate([[0], np.ones(n_sys - 1, dtype=int)])
+        par["sigma_sm"] = zero
+    mom_order = np.atleast_1d(np.asarray(par["mom_order"])).astype(int)
+    mo = par.get("mom_output", 1)
+    if isinstance(mo, str) and mo == "all":
+        mo = np.arange(1, n_sys + 1)
+    S.mom_output = [int(v) for v in np.atleast_1d(mo)]
+    gt = _lib.classify(Mx, My, Mz)
+    ax = np.asarray(par["ax"], dtype=np.float64)
+    n = np.asarray(par["n"], dtype=int)
+    bc = np.asarray(par["bc"], dtype=int)
+    h = (ax[[1, 3, 5]] - ax[[0, 2, 4]]) / n
+    lam = np.max(np.abs(np.linalg.eigvals(Mz)))
+    dt_hyp = np.min(h) / abs(lam)
+    if n[0] != 1:
+        dt_hyp = dt_hyp / 3
+    elif n[1] != 1:
+        dt_hyp = dt_hyp / 2
+    if par.get("timestep", 0) != 0:
+        raise NotImplementedError("timestep > 0 (parabolic step search) is handled by the reference's host code only")
+    S.time_dependent = np.array([nargin(par["sigma_a"]) > 3, nargin(par["sigma_s0"]) > 3,
+                                 nargin(par["sigma_sm"]) > 4])
+    xs = [colon(ax[0] + h[0] / 2, h[0], ax[1] - h[0] / 2), colon(ax[0] + h[0] * (1 - bc[0]), h[0], ax[1])]
+    ys = [colon(ax[2] + h[1] / 2, h[1], ax[3] - h[1] / 2), colon(ax[2] + h[1] * (1 - bc[1]), h[1], ax[3])]
+    zs = [colon(ax[4] + h[2] / 2, h[2], ax[5] - h[2] / 2), colon(ax[4] + h[2] * (1 - bc[2]), h[2], ax[5])]
+    grids = {}
+
+    def XYZ(g):
+        if g not in grids:
+            grids[g] = np.meshgrid(xs[g[0] - 1], ys[g[1] - 1], zs[g[2] - 1], indexing="ij")
+        return grids[g]
+
+    S.par, S.n_sys, S.Mx, S.My, S.Mz = par, n_sys, Mx, My, Mz
+    S.gt, S.n, S.bc, S.h, S.dt_hyp = gt, n, bc, h, dt_hyp
+    S.xs, S.ys, S.zs, S.XYZ = xs, ys, zs, XYZ
+    S.mom_order, S.f_mom_order = mom_order, f_mom_order
+    S.flag_filter, S.flag_ani = flag_filter, flag_ani
+    S.f_position = par["f_position"]
+    S.G = lambda j: (int(gt[j, 0]), int(gt[j, 1]), int(gt[j, 2]))
+    S.sg = sorted(set((*S.G(j), int(mom_order[j])) for j in range(1, n_sys)))
+    S.f_sg = sorted(set((*S.G(j), int(f_mom_order[j])) for j in range(1, n_sys))) if flag_filter else []
+    # initial condition (starmap_solver.m:140-146)
+    ic = par["ic"]
+    U = []
+    for j in range(n_sys):
+        X, Y, Z = XYZ(S.G(j))
+        val = capargs(ic, X, Y, Z, j + 1)
+        U.append(X * 0 + np.asarray(val, dtype=np.float64) * float(nargin(ic) > 3 or j == 0))
+    S.U0 = U
+    S.source_ind = [int(v) for v in np.atleast_1d(np.asarray(par.get("source_ind", [])))]
+    S.src_td = nargin(par["source"]) >= 4 and len(S.source_ind) > 0
+    S.filter_td = flag_filter and nargin(par["filterfunction"]) > 6
+    return S
+
+
+def _ones(*args):
+    return 1.0
+
+
+_ones._nargin = -1
+
+
+def _materials(S, t):
+    """sA{g}, sT{g,m} evaluated at time t (starmap_solver.m:215-243)."""
+    par = S.par
+    grids_used = sorted(set([(1, 1, 1)] + [row[:3] for row in S.sg]))
+    sA = {g: _as_field(capargs(par["sigma_a"], *S.XYZ(g), t), S.XYZ(g)[0].shape) for g in grids_used}
+    sT = {}
+    for row in S.sg:
+        g, m = row[:3], row[3]
+        X, Y, Z = S.XYZ(g)
+        sS = np.asarray(capargs(par["sigma_s0"], X, Y, Z, t), dtype=np.float64)
+        if S.flag_ani:
+            sS = sS - np.asarray(capargs(par["sigma_sm"], X, Y, Z, m, t), dtype=np.float64)
+        sT[row] = _as_field(sA[g] + sS, X.shape)
+    return sA, sT
+
+
+def _filters(S, dt, t):
+    par = S.par
+    F = {}
+    for row in S.f_sg:
+        g, m = row[:3], row[3]
+        X, Y, Z = S.XYZ(g)
+        if S.f_position == "full":
+            F[row] = _as_field(capargs(par["filterfunction"], par, dt, m, X, Y, Z, t), X.shape)
+        elif S.f_position == "substep":
+            F[row + (1,)] = _as_field(capargs(par["filterfunction"], par, dt, m, X, Y, Z, t - dt / 2), X.shape)
+            F[row + (2,)] = _as_field(capargs(par["filterfunction"], par, dt, m, X, Y, Z, t), X.shape)
+    return F
+
+
+def _sources(S, t, dt):
+    par = S.par
+    Q = {}
+    for j1 in S.source_ind:
+        j = j1 - 1
+        X, Y, Z = S.XYZ(S.G(j))
+        Q[j] = _as_field(capargs(par["source"], X, Y, Z, t - dt / 2, j1), X.shape)
+    return Q
+
+
+class _Tables:
+    """Field table of the C ABI with stable indices for later updates."""
+
+    def __init__(self):
+        self.fields = []
+        self.index = {}
+
+    def add(self, key, val, grid):
+        self.index[key] = len(self.fields)
+        self.fields.append((val, grid))
+        return self.index[key]
+
+
+def _build(S, sA1, sT1, EA, ET, Q, F):
+    n_sys = S.n_sys
+    T = _Tables()
+    for row in S.sg:
+        T.add(("sT",) + row, sT1[row], row[:3])
+        T.add(("ET",) + row, ET[row], row[:3])
+    T.add(("sA",), sA1, (1, 1, 1))
+    T.add(("EA",), EA, (1, 1, 1))
+    for j, q in Q.items():
+        T.add(("Q", j), q, S.G(j))
+    for key, val in F.items():
+        T.add(("F",) + key, val, key[:3])
+    key = lambda j: (*S.G(j), int(S.mom_order[j]))
+    sigma_t = [0] + [T.index[("sT",) + key(j)] for j in range(1, n_sys)]
+    decay_t = [0] + [T.index[("ET",) + key(j)] for j in range(1, n_sys)]
+    source = [T.index.get(("Q", j), -1) for j in range(n_sys)]
+    mode = {"": FILTER_NONE, "substep": FILTER_SUBSTEP, "full": FILTER_FULL}.get(S.f_position, FILTER_NONE)
+    if not S.flag_filter:
+        mode = FILTER_NONE
+    f1 = f2 = None
+    if mode != FILTER_NONE:
+        fkey = lambda j: (*S.G(j), int(S.f_mom_order[j]))
+        if mode == FILTER_SUBSTEP:
+            f1 = [-1] + [T.index[("F",) + fkey(j) + (1,)] for j in range(1, n_sys)]
+            f2 = [-1] + [T.index[("F",) + fkey(j) + (2,)] for j in range(1, n_sys)]
+        else:
+            f1 = [-1] + [T.index[("F",) + fkey(j)] for j in range(1, n_sys)]
+    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, sigma_t, T.index[("sA",)], source,
+                       decay_t=decay_t, decay_a=T.index[("EA",)], filter_mode=mode, filter1=f1, filter2=f2)
+    return solver, T
+
+
+def _output_struct(S, U):
+    dim = S.par.get("dim", 3)
+    out = []
+    for j in range(S.n_sys):
+        g = S.G(j)
+        if dim == 1:
+            out.append({"x": S.zs[g[2] - 1], "U": U[j].reshape(len(S.zs[g[2] - 1]), -1, order="F")})
+        elif dim == 2:
+            out.append({"x": S.ys[g[1] - 1], "y": S.zs[g[2] - 1],
+                        "U": U[j].reshape(len(S.ys[g[1] - 1]), -1, order="F")})
+        else:
+            out.append({"x": S.xs[g[0] - 1], "y": S.ys[g[1] - 1], "z": S.zs[g[2] - 1], "U": U[j]})
+    return out
+
+
+def starmap_solver(par: dict):
+    """Run the StaRMAP time loop on the GPU; returns the reference's ``output``.
+
+    ``output[j]`` is a dict with keys ``x``, ``y`` (2D), ``z`` (3D) and ``U`` for
+    component j+1, exactly the struct array of starmap_solver.m:484-500."""
+    t_start = time.perf_counter()
+    S = prepare(par)
+    par = S.par
+    tfinal = float(par["tfinal"])
+    cn = float(par["cn"])
+    td_any = bool(S.time_dependent.any())
+    # first-step materials and dt (starmap_solver.m:165-213)
+    sA, sT = _materials(S, 0.0)
+    dt = min(S.dt_hyp, (tfinal - 0.0) / cn) * cn
+    if td_any:
+        sA0, sT0 = sA, sT
+        sA, sT = _materials(S, dt)
+        sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
+        sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
+    else:
+        sA1, sT1 = sA[1, 1, 1], sT
+    EA = expm1div(-sA1 * dt / 2)
+    ET = {k: expm1div(-sT1[k] * dt / 2) for k in S.sg}
+    t = dt
+    Q = _sources(S, t, dt)
+    F = _filters(S, dt, t) if S.flag_filter else {}
+    cpu_setup = time.perf_counter() - t_start
+
+    solver, T = _build(S, sA1, sT1, EA, ET, Q, F)
+    t_gpu0 = time.perf_counter()
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(dt)
+        t_plot = list(np.atleast_1d(np.asarray(par.get("t_plot", [])))) + [np.inf]
+        want_plot = par.get("output", _noop_output) is not _noop_output
+        per_step = td_any or S.src_td or S.filter_td
+        step_count = 0
+        t_cur = 0.0
+        plot_count = 0
+        outfn = par.get("output", _noop_output)
+        while t_cur < tfinal:
+            if per_step and step_count > 0:
+                # time-dependent data re-evaluated where the reference does
+                tleft = (tfinal - t_cur) / cn
+                if td_any:
+                    dt_new = min(S.dt_hyp, tleft) * cn
+                    sA0, sT0 = sA, sT
+                    sA, sT = _materials(S, t_cur + dt_new)
+                    sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
+                    sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
+                    if dt_new != dt:
+                        dt = dt_new
+                        solver.set_dt(dt)
+                    solver.set_field(T.index[("sA",)], sA1)
+                    solver.set_field(T.index[("EA",)], expm1div(-sA1 * dt / 2))
+                    for k in S.sg:
+                        solver.set_field(T.index[("sT",) + k], sT1[k])
+                        solver.set_field(T.index[("ET",) + k], expm1div(-sT1[k] * dt / 2))
+                tn = t_cur + dt
+                if S.src_td:
+                    for j, q in _sources(S, tn, dt).items():
+                        solver.set_field(T.index[("Q", j)], q)
+                if S.filter_td:
+                    for key, val in _filters(S, dt, tn).items():
+                        solver.set_field(T.index[("F",) + key], val)
+            # how many steps can run before the next plot time
+            if per_step:
+                nrun = 1
+            else:
+                ts = step_times(dt, tfinal)[step_count:]
+                nrun = len(ts)
+                if want_plot:
+                    for k, tk in enumerate(ts):
+                        if tk >= t_plot[plot_count] - 1e-14:
+                            nrun = k + 1
+                            break
+            U0 = None
+            if want_plot and nrun >= 1:
+                if nrun > 1:
+                    solver.run(nrun - 1)
+                    for _ in range(nrun - 1):
+                        t_cur = t_cur + dt
+                    step_count += nrun - 1
+                    nrun = 1
+                U0 = solver.get_state([j - 1 for j in S.mom_output])
+            solver.run(nrun)
+            for _ in range(nrun):
+                t_cur = t_cur + dt
+            step_count += nrun
+            if want_plot:
+                Un = solver.get_state([j - 1 for j in S.mom_output])
+                while t_cur >= t_plot[plot_count] - 1e-14:
+                    lam = (t_plot[plot_count] - t_cur + dt) / dt
+                    Uplot = [(1 - lam) * U0[j - 1] + lam * Un[j - 1] for j in S.mom_output]
+                    ret = _call_output(S, outfn, par, Uplot, plot_count + 1)
+                    if isinstance(ret, dict):
+                        par = ret
+                        S.par = par
+                    plot_count += 1
+        Ufin = solver.get_state()
+    finally:
+        solver.close()
+    gpu_s = time.perf_counter() - t_gpu0
+    U = [Ufin[j] for j in range(S.n_sys)]
+    if not par.get("quiet", False):
+        n = list(S.n)
+        print(f"{par.get('name', 'Output')} with {par.get('closure_mod', '')}{par['closure']}{par['n_mom']}\n"
+              f" {S.n_sys} moments, {n[0]}x{n[1]}x{n[2]} grid, {step_count} time steps")
+        tot = max(cpu_setup + gpu_s, 1e-30)
+        print(f"CPU-times\n advection:{gpu_s:12.2f}s{gpu_s / tot * 100:5.0f}%\n "
+              f"absorb/scatter:{cpu_setup:7.2f}s{cpu_setup / tot * 100:5.0f}%\n plotting:{0.0:13.2f}s{0:5.0f}%")
+    return _output_struct(S, U)
+
+
+def _call_output(S, outfn, par, Uplot, step):
+    """Plot callback with the reference's argument layout (starmap_solver.m:432-471)."""
+    dim = par.get("dim", 3)
+    mo = [j - 1 for j in S.mom_output]
+    if dim == 1:
+        zp = [S.zs[S.gt[j, 2] - 1] for j in mo]
+        Up = [u.reshape(len(z), -1, order="F") for u, z in zip(Uplot, zp)]
+        if len(mo) == 1:
+            zp, Up = zp[0], Up[0]
+        return outfn(par, zp, Up, step)
+    if dim == 2:
+        yp = [S.ys[S.gt[j, 1] - 1] for j in mo]
+        zp = [S.zs[S.gt[j, 2] - 1] for j in mo]
+        Up = [u.reshape(len(y), -1, order="F") for u, y in zip(Uplot, yp)]
+        if len(mo) == 1:
+            yp, zp, Up = yp[0], zp[0], Up[0]
+        return outfn(par, yp, zp, Up, step)
+    xp = [S.xs[S.gt[j, 0] - 1] for j in mo]
+    yp = [S.ys[S.gt[j, 1] - 1] for j in mo]
+    zp = [S.zs[S.gt[j, 2] - 1] for j in mo]
+    Up = list(Uplot)
+    if len(mo) == 1:
+        xp, yp, zp, Up = xp[0], yp[0], zp[0], Up[0]
+    return outfn(par, xp, yp, zp, Up, step)

@@ -1,0 +1,125 @@
+"""CPU-only tests: library exports, closures, classification, host logic."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import solver_np as O
+from starmap_b200 import _lib, closure_pn, closure_spn, starmap_init
+from starmap_b200.init import capargs, hook, nargin
+from starmap_b200.solver import colon, expm1div, step_times
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "starmap_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(smg_[a-z_]+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_every_header_symbol():
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(L, s), f"{s} declared in include/starmap_gpu.h but not exported"
+    assert set(syms) <= set(_lib.SIGNATURES), "ctypes binding lacks a header symbol"
+    assert _lib.lib().smg_version().decode().startswith("starmap_b200")
+    assert _lib.lib().smg_device_count() >= 0
+
+
+def test_create_rejects_bad_descriptor():
+    L = _lib.lib()
+    p = _lib.smg_problem()
+    p.n_sys = 0
+    h = ctypes.c_void_p()
+    assert L.smg_create(ctypes.byref(p), ctypes.byref(h)) == _lib.SMG_EINVAL
+    assert b"n_sys" in L.smg_last_error(None)
+    assert L.smg_create(None, ctypes.byref(h)) == _lib.SMG_EINVAL
+
+
+@pytest.mark.parametrize("N,lam", [(7, 0.960290), (39, 0.998238), (15, 0.989401)])
+def test_pn2d_eigenvalue_pins(N, lam):
+    # largest |eigenvalue| of Mz equals the largest root of the Legendre
+    # polynomial P_{N+1}: an independent known answer for the closure tables
+    _, _, _, Mz = closure_pn(N, 2)
+    roots = np.polynomial.legendre.leggauss(N + 1)[0]
+    ev = np.max(np.abs(np.linalg.eigvalsh(Mz)))
+    assert abs(ev - roots.max()) < 1e-12
+    assert abs(ev - lam) < 5e-7
+
+
+def test_pn3d_tables():
+    o, Mx, My, Mz = closure_pn(9, 3)
+    assert Mz.shape == (100, 100)
+    for M in (Mx, My, Mz):
+        np.testing.assert_array_equal(M, M.T)
+    np.testing.assert_array_equal(o, np.ceil(np.sqrt(np.arange(1, 101)) - 1))
+    roots = np.polynomial.legendre.leggauss(10)[0]
+    assert abs(np.max(np.abs(np.linalg.eigvalsh(Mz))) - roots.max()) < 1e-12
+
+
+@pytest.mark.parametrize("cl,N,dim", [("P", 1, 2), ("P", 7, 2), ("P", 39, 2), ("P", 2, 3), ("P", 9, 3),
+                                      ("SP", 5, 2), ("SP", 9, 3), ("P", 5, 1), ("SP", 4, 2)])
+def test_native_classification_matches_oracle(cl, N, dim):
+    f = closure_pn if cl == "P" else closure_spn
+    _, Mx, My, Mz = f(N, dim)
+    gt = _lib.classify(Mx, My, Mz)
+    _, _, _, _, gx, gy, gz = O._classify(Mx, My, Mz)
+    np.testing.assert_array_equal(gt, np.stack([gx, gy, gz], 1))
+
+
+def test_phase_partition_counts():
+    # component sets of the benchmark configurations
+    def counts(N, dim):
+        _, Mx, My, Mz = closure_pn(N, dim)
+        gt = _lib.classify(Mx, My, Mz)
+        outer = int(np.sum((gt == 2).sum(1) % 2 == 1))
+        return Mz.shape[0], outer, Mz.shape[0] - outer
+    assert counts(7, 2) == (36, 20, 16)
+    assert counts(39, 2) == (820, 420, 400)
+    assert counts(9, 3) == (100, 55, 45)
+    assert counts(15, 2) == (136, 72, 64)
+
+
+def test_expm1div_branch():
+    x = np.array([-1e-5, 1e-4, -2e-4, 2.0000001e-4, -3e-4, -1.0, 0.0])
+    y = expm1div(x)
+    for xi, yi in zip(x, y):
+        if abs(xi) > 2e-4:
+            assert yi == (np.exp(xi) - 1) / xi
+        else:
+            assert yi == 1 + xi * .5 + xi ** 2 / 6
+    assert expm1div(0.0) == 1.0
+
+
+def test_colon_and_step_count():
+    v = colon(0.015, 0.03, 3.0 - 0.015)
+    assert len(v) == 100 and v[0] == 0.015
+    ts = step_times(0.015, 1.0)
+    assert len(ts) == 67 and ts[-1] >= 1.0       # overshoots tfinal
+    assert len(step_times(0.01, 3.2)) in (320, 321)
+
+
+def test_nargin_semantics():
+    assert nargin(lambda x, y: 0) == 2
+    assert nargin(lambda *a: 0) == -1
+    assert nargin(hook(lambda *a: 0, 4)) == 4
+    assert capargs(lambda x: x, 1, 2, 3) == 1
+
+
+def test_init_wraps_2d_hooks_and_defaults():
+    par = starmap_init(dict(closure="P", n_mom=3, ax=[0, 1, 0, 2], n=[4, 5], bc=[1, 0],
+                            ic=lambda x, y: x + 10 * y, source=lambda x, y, t: t))
+    assert par["dim"] == 2 and par["n"] == [1, 4, 5] and par["bc"] == [1, 1, 0]
+    assert par["ax"] == [0, 1, 0, 1, 0, 2]
+    assert nargin(par["ic"]) == 3 and par["ic"](None, 2.0, 3.0) == 32.0
+    assert nargin(par["source"]) == 4
+    assert list(par["source_ind"]) == [1]
+    assert par["tfinal"] == 1.0 and par["cn"] == 0.99
+    with pytest.raises(ValueError):
+        starmap_init(dict(closure="P", n_mom=3, ax=[0, 1, 0, 2], n=[4]))
+    with pytest.raises(ValueError):
+        starmap_init(dict(closure="P", n_mom=3, ax=[0, 1, 0, 1], ic=lambda x: x))
