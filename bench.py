@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the StaRMAP time loop on B200: moment-cell updates/s.
+
+Workload (default): 2D checkerboard lattice, P_39 filtered (820 moments),
+350x350 cells on [0,7]^2, bc = 1, sigma_a = 10 / sigma_s0 = 0 on the absorbing
+squares and 0 / 1 elsewhere, source q = 1 in the central square, zero initial
+condition, dt = 0.5 h, t_final = 3.2 (321 steps), exponential filter of order 4
+and strength 10 applied per substep.  Synthetic, deterministic inputs with the
+shapes of the reference's lattice example.
+
+One bench step = one full Strang time step (phase A, phase B, phase A) of the
+whole problem.  One moment-cell update = one component at one cell advanced
+by one step, so a step is n_sys * nx * ny updates.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU runs (torchrun, one process per GPU) run independent replicas of the
+workload (the path does not shard); value is the aggregate over all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD_NAME = ("2D checkerboard lattice P39 filtered (820 moments), 350x350 cells, bc=1, "
+                 "substep exp filter p=4 f_eff=10, dt=0.5h, t_final=3.2 (321 steps)")
+METRIC = "moment-cell updates/s"
+UNIT = "updates/s"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class Dist:
+    """Barrier and max-over-ranks; torch.distributed only when WORLD_SIZE > 1."""
+
+    def __init__(self, world, local_rank, backend="nccl"):
+        self.world = world
+        self.torch = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local_rank)
+            td.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.torch, self.td = torch, td
+
+    def barrier(self):
+        if self.torch is not None:
+            self.td.barrier()
+            self.torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if self.torch is None:
+            return v
+        t = self.torch.tensor([float(v)], device="cuda", dtype=self.torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.torch is not None:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows
+                                                        if r[3].replace(".", "").isdigit())}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per step of the phase kernels from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "phase_kernels_lattice_p39_350.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_step:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def workload():
+    from starmap_b200 import configs, starmap_init
+    par = starmap_init(configs.lattice(n=350, n_mom=39, tfinal=3.2, filter_order=4, f_eff=10.0,
+                                       f_position="substep"))
+    return par
+
+
+def cpu_sample(par, budget_s: float, nthreads: int, max_steps: int | None = None, warm: int = 0):
+    """Time the oracle's C restatement (all given threads) on a bounded prefix of the run."""
+    from oracle import c_oracle
+    adv = c_oracle.CAdvance(nthreads)
+
+    def stop():
+        done = len(adv.step_seconds)
+        if max_steps is not None and done >= warm + max_steps:
+            return True
+        return sum(adv.step_seconds[warm:]) >= budget_s and done > warm
+
+    c_oracle.run(par, nthreads=nthreads, advance=adv, stop=stop)
+    secs = adv.step_seconds[warm:]
+    return len(secs), sum(secs)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (oracle C port; GNU Octave is not on the box)."""
+    if rank != 0:
+        return 0
+    par = workload()
+    n_sys = par["Mz"].shape[0]
+    cells = int(np.prod(par["n"]))
+    threads = host_threads()
+    warm = max(0, min(args.warmup, 1))
+    steps, secs = cpu_sample(par, budget_s=args.ref_budget, nthreads=threads, max_steps=args.steps, warm=warm)
+    value = n_sys * cells * steps / secs
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": secs / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "n_sys": n_sys, "cells": cells, "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {steps} of 321 steps after {warm} warm-up step(s); "
+                                   "GNU Octave (the reference runtime) is absent on this box, so the "
+                                   "oracle's C restatement of starmap_solver.m stands in"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=321)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--variant", choices=["auto", "generic", "strip"], default="auto",
+                    help="kernel family (all give identical results)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline stepping")
+    ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of reference-arm stepping")
+    args = ap.parse_args()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    from starmap_b200 import _lib
+    from starmap_b200.roofline import algorithmic_bytes_per_step
+    from starmap_b200.solver import GpuSolver, handle_tables, setup_gpu
+
+    _lib.check(_lib.lib().smg_set_device(local_rank))
+    dist = Dist(world, local_rank)
+    par = workload()
+    S, fs, solver, T = setup_gpu(par)
+    n_sys = S.n_sys
+    cells = int(np.prod(S.n))
+    upd_step = n_sys * cells
+    variant = {"auto": 0, "generic": 1, "strip": 2}[args.variant]
+    solver.set_variant(variant)
+    alg = algorithmic_bytes_per_step(S, T, fused=(variant == 0))
+    solver.set_state(S.U0)
+    solver.set_dt(fs["dt"])
+    solver.run(args.warmup)
+    solver.sync()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    dist.barrier()
+    solver.sync()
+    solver.run(args.steps)
+    solver.sync()
+    dist.barrier()
+    ms, launches = solver.last_run_stats()
+    ms_max = dist.max(ms)
+    finite = solver.check_finite() == 0
+    solver.close()
+
+    # end to end through the C ABI with host buffers: create (field upload),
+    # state upload, the K steps and the state download, every byte included
+    e2e = None
+    if not args.no_e2e:
+        fields_bytes = sum(np.asarray(v).size * 8 for v, _ in T.fields)
+        state_bytes = alg["state_bytes"]
+        dist.barrier()
+        t0 = time.perf_counter()
+        s2 = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
+        s2.set_variant(variant)
+        s2.set_state(S.U0)
+        s2.set_dt(fs["dt"])
+        s2.run(args.steps)
+        Ufin = s2.get_state()
+        t1 = time.perf_counter()
+        s2.close()
+        el = dist.max(t1 - t0)
+        e2e = {"value": upd_step * args.steps * world / el, "unit": UNIT,
+               "h2d_bytes_per_step": int((state_bytes + fields_bytes) / args.steps),
+               "d2h_bytes_per_step": int(sum(u.size for u in Ufin.values()) * 8 / args.steps),
+               "seconds": el}
+    clk = clocks.stop()
+
+    peak, peak_kind = measured_peak()
+    t_step = ms_max / 1e3 / args.steps
+    achieved = alg["step"] / t_step / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": upd_step * args.steps * world / (ms_max / 1e3), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "n_sys": n_sys, "cells": cells,
+                   "updates_per_step": upd_step, "state_gb": alg["state_bytes"] / 1e9,
+                   "l2": "inputs larger than L2 (state %.2f GB > 126 MB), no flush" % (alg["state_bytes"] / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU", "variant": args.variant},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_step": alg["step"],
+                     "kernel": "fused staggered half-step kernels (phase A/B), avg over the timed steps"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "finite": finite,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        steps, secs = cpu_sample(par, budget_s=args.cpu_budget, nthreads=threads, warm=0)
+        line["cpu_baseline"] = {"value": upd_step * steps / secs, "unit": UNIT, "cores": threads,
+                                "kind": "port",
+                                "sample": f"first {steps} of 321 steps of the same workload, oracle C "
+                                          f"restatement (OpenMP, {threads} threads)"}
+    dist.barrier()
+    dist.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

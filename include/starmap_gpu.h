@@ -49,6 +49,10 @@ extern "C" {
 #define SMG_ENOMEM     -5   /* device allocation failed */
 #define SMG_ESTATE     -6   /* call out of order (e.g. run before the state is set) */
 
+#define SMG_VARIANT_AUTO    0  /* strip kernels; phase A of consecutive steps fused (default) */
+#define SMG_VARIANT_GENERIC 1  /* point-per-thread kernels, one launch per half step */
+#define SMG_VARIANT_STRIP   2  /* strip kernels, one launch per half step */
+
 #define SMG_FILTER_NONE    0   /* par.f_position = ''          */
 #define SMG_FILTER_SUBSTEP 1   /* par.f_position = 'substep'   */
 #define SMG_FILTER_FULL    2   /* par.f_position = 'full'      */
@@ -97,6 +101,10 @@ const char* smg_last_error(const smg_handle* h);
 /* Number of visible CUDA devices (>= 0), or a negative SMG_E* code. */
 int smg_device_count(void);
 
+/* Select the CUDA device used by handles created afterwards on the calling
+ * thread (one process per GPU: rank r calls smg_set_device(local_rank)). */
+int smg_set_device(int32_t device);
+
 /* Validate the descriptor, build the coupling tables (the Ix/Iy/Iz lists of
  * starmap_solver.m:77-79 in sumcell order, starmap_solver.m:350-351/398-399),
  * allocate device memory and upload the coefficient fields.
@@ -131,6 +139,11 @@ int smg_run(smg_handle* h, int64_t nsteps);
 
 /* Wait for all work of `h`. */
 int smg_sync(smg_handle* h);
+
+/* Choose the kernel family (SMG_VARIANT_*).  All variants produce identical
+ * results; AUTO falls back to GENERIC when a schedule does not fit in shared
+ * memory.  No reference counterpart (the reference has one CPU code path). */
+int smg_set_variant(smg_handle* h, int32_t variant);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the
  * handle's stream) and its launch count. */

@@ -151,7 +151,12 @@ def _classify(Mx, My, Mz):
     return c, Ix, Iy, Iz, gtx, gty, gtz
 
 
-def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int | None = None) -> OracleResult:
+def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int | None = None,
+                   advance=None, stop=None) -> OracleResult:
+    """Run the restated solver.  ``advance`` replaces the numpy step function
+    (same arguments as :func:`_advance`); ``oracle.c_oracle`` passes its C one.
+    ``max_steps`` or a ``stop()`` callable returning True end the loop early
+    (used to time bounded samples)."""
     par = dict(par)
     Mx, My, Mz = (np.asarray(par[k], dtype=np.float64) for k in ("Mx", "My", "Mz"))
     n_sys = Mz.shape[0]
@@ -248,6 +253,8 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
     while t < tfinal:
         if max_steps is not None and step_count >= max_steps:
             break
+        if stop is not None and stop():
+            break
         tleft = (tfinal - t) / cn
         for k in range(int(t > 0), 2):
             if (not time_dependent.any()) and t > 0:
@@ -299,7 +306,7 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
                     filterTerm[a, b, cz, m, 1] = np.asarray(capargs(par["filterfunction"], par, dt, m, X[g], Y[g], Z[g], t - dt / 2), dtype=np.float64)
                     filterTerm[a, b, cz, m, 2] = np.asarray(capargs(par["filterfunction"], par, dt, m, X[g], Y[g], Z[g], t), dtype=np.float64)
         U0 = [U[j - 1] for j in mom_output]
-        _advance(U, Q, Ix, Iy, Iz, c, extend, h, Mx, My, Mz, dt, gtx, gty, gtz, mom_order, f_mom_order if flag_filter else None,
+        (advance or _advance)(U, Q, Ix, Iy, Iz, c, extend, h, Mx, My, Mz, dt, gtx, gty, gtz, mom_order, f_mom_order if flag_filter else None,
                  f_position, sA1, EA, sT1, ET, filterTerm)
         # plotting/interpolation (starmap_solver.m:425-473), headless
         while t >= t_plot[plot_count] - 1e-14:

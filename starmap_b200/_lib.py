@@ -57,6 +57,7 @@ SIGNATURES = {
     "smg_version": (C.c_char_p, []),
     "smg_last_error": (C.c_char_p, [C.c_void_p]),
     "smg_device_count": (C.c_int, []),
+    "smg_set_device": (C.c_int, [C.c_int32]),
     "smg_create": (C.c_int, [C.POINTER(smg_problem), C.POINTER(C.c_void_p)]),
     "smg_destroy": (None, [C.c_void_p]),
     "smg_set_state": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double))]),
@@ -65,6 +66,7 @@ SIGNATURES = {
     "smg_set_dt": (C.c_int, [C.c_void_p, C.c_double]),
     "smg_run": (C.c_int, [C.c_void_p, C.c_int64]),
     "smg_sync": (C.c_int, [C.c_void_p]),
+    "smg_set_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "smg_last_run_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "smg_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_check_finite": (C.c_int, [C.c_void_p]),

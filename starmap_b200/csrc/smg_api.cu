@@ -69,6 +69,10 @@ void free_device(smg_handle* h) {
     cudaFree(h->dFieldTab);
     cudaFree(h->dDest);
     cudaFree(h->dFlag);
+    for (auto& sc : h->sched) {
+        cudaFree(sc.dmem);
+        sc.dmem = nullptr;
+    }
     h->dU = h->dFields = nullptr;
     h->dComps = nullptr;
     h->dCoups = nullptr;
@@ -108,6 +112,126 @@ void grid_extents(const smg_handle* h, const int gt_solver[3], int e[3]) {
     }
 }
 
+// Strip schedule of one phase.  Destinations are grouped into stages by their
+// breadth-first level in the coupling graph rooted at component 0 (for P_N and
+// SP_N this level is the moment order, and a destination of order m only
+// reads sources of orders m-1 and m+1).  Each derivative (source, axis) is
+// computed in the stage of its first use and its shared-memory slot is
+// released after its last use, so at most two source orders are live.
+void build_schedule(smg_handle* h, int phase, const std::vector<int>& level) {
+    using smg::DestJob;
+    using smg::SCoup;
+    using smg::SlotJob;
+    using smg::Stage;
+    auto& S = h->sched[phase];
+    S = smg_handle::HostSched{};
+    const std::vector<int>& D = phase == 0 ? h->destA : h->destB;
+    if (D.empty()) {
+        S.ok = true;
+        return;
+    }
+    std::map<int, std::vector<int>> bylev;
+    for (int j : D) bylev[level[j]].push_back(j);
+    std::vector<std::vector<int>> groups;
+    for (auto& kv : bylev) groups.push_back(kv.second);
+    typedef std::pair<int, int> Key;   // (src, code)
+    std::map<Key, std::pair<int, int>> use;   // first, last stage
+    for (int s = 0; s < (int)groups.size(); ++s)
+        for (int j : groups[s])
+            for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
+                const Key k(h->coups[q].src, h->coups[q].code);
+                auto it = use.find(k);
+                if (it == use.end()) use[k] = std::make_pair(s, s);
+                else it->second.second = s;
+            }
+    std::vector<int> freelist;
+    std::map<Key, int> slot_of;
+    int nslots = 0;
+    for (int s = 0; s < (int)groups.size(); ++s) {
+        Stage st{};
+        st.jbeg = (int)S.jobs.size();
+        for (auto& kv : use) {
+            if (kv.second.first != s) continue;
+            int slot;
+            if (!freelist.empty()) { slot = freelist.back(); freelist.pop_back(); }
+            else slot = nslots++;
+            slot_of[kv.first] = slot;
+            SlotJob jb{};
+            jb.src = kv.first.first;
+            jb.code = kv.first.second;
+            jb.slot = slot;
+            const int ax = jb.code >> 1;
+            for (int a = 0; a < 3; ++a) jb.ext[a] = h->comps[jb.src].ext[a];
+            jb.ext[ax] = (jb.code & 1) ? h->g.n[ax] : h->g.n[ax] + h->g.bc[ax];
+            S.jobs.push_back(jb);
+        }
+        st.jend = (int)S.jobs.size();
+        st.dbeg = (int)S.dests.size();
+        for (int j : groups[s]) {
+            DestJob dj{};
+            dj.comp = j;
+            dj.cbeg = (int)S.coups.size();
+            for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q)
+                S.coups.push_back(SCoup{slot_of[Key(h->coups[q].src, h->coups[q].code)], 0, h->coups[q].w});
+            dj.cend = (int)S.coups.size();
+            S.dests.push_back(dj);
+        }
+        st.dend = (int)S.dests.size();
+        S.stages.push_back(st);
+        for (auto& kv : use)
+            if (kv.second.second == s) freelist.push_back(slot_of[kv.first]);
+    }
+    S.nslots = std::max(nslots, 1);
+    S.ok = S.nslots * 32 * 8 <= smg::kMaxStripSmem;
+}
+
+cudaError_t upload_schedule(smg_handle* h, int phase) {
+    auto& S = h->sched[phase];
+    S.view = smg::StripSched{};
+    if (!S.ok || S.stages.empty()) return cudaSuccess;
+    const size_t b0 = S.stages.size() * sizeof(smg::Stage);
+    const size_t b1 = S.jobs.size() * sizeof(smg::SlotJob);
+    const size_t b2 = S.dests.size() * sizeof(smg::DestJob);
+    const size_t b3 = S.coups.size() * sizeof(smg::SCoup);
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t tot = al(b0) + al(b1) + al(b2) + al(b3) + 256;
+    cudaError_t e = cudaMalloc(&S.dmem, tot);
+    if (e != cudaSuccess) return e;
+    h->bytes += tot;
+    char* p = (char*)S.dmem;
+    char* p0 = p; p += al(b0);
+    char* p1 = p; p += al(b1);
+    char* p2 = p; p += al(b2);
+    char* p3 = p;
+    if ((e = cudaMemcpyAsync(p0, S.stages.data(), b0, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
+    if (b1 && (e = cudaMemcpyAsync(p1, S.jobs.data(), b1, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
+    if (b2 && (e = cudaMemcpyAsync(p2, S.dests.data(), b2, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
+    if (b3 && (e = cudaMemcpyAsync(p3, S.coups.data(), b3, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
+    S.view.stages = (const smg::Stage*)p0;
+    S.view.jobs = (const smg::SlotJob*)p1;
+    S.view.dests = (const smg::DestJob*)p2;
+    S.view.coups = (const smg::SCoup*)p3;
+    S.view.nstages = (int)S.stages.size();
+    S.view.nslots = S.nslots;
+    return cudaSuccess;
+}
+
+// RN(1/h) and whether Markstein's correction from it is exact for every
+// dividend (|RN(1/h)*h - 1| < 2^-55 and normal numbers).
+void reciprocals(smg_handle* h) {
+    for (int a = 0; a < 3; ++a) {
+        const double hv = h->g.h[a];
+        const double r = 1.0 / hv;
+        const double e = std::fma(r, hv, -1.0);
+        h->rh[a] = r;
+        h->exact_recip[a] = std::isnormal(hv) && std::isnormal(r) && std::fabs(e) < std::ldexp(1.0, -55);
+    }
+}
+
+bool strip_usable(const smg_handle* h) {
+    return h->sched[0].ok && h->sched[1].ok && h->variant != SMG_VARIANT_GENERIC;
+}
+
 }  // namespace
 
 extern "C" {
@@ -126,6 +250,12 @@ int smg_device_count(void) {
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return 0;
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
     return n;
+}
+
+int smg_set_device(int32_t device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    return SMG_OK;
 }
 
 int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz, int32_t* gt_out) {
@@ -366,6 +496,28 @@ int smg_create(const smg_problem* p, smg_handle** out) {
         CREATE_CUDA(put_slot(h, const_cast<double*>(h->fields_host[f].p), p->fields[f].data, e3));
     }
     CREATE_CUDA(cudaMemcpyAsync(h->dFieldTab, h->fields_host.data(), sizeof(DevField) * nfields, cudaMemcpyHostToDevice, h->stream));
+    // strip-kernel schedules: stage = breadth-first level of the coupling graph
+    {
+        std::vector<int> level(ns, -1), queue(1, 0);
+        level[0] = 0;
+        for (size_t qi = 0; qi < queue.size(); ++qi) {
+            const int j = queue[qi];
+            for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
+                const int i = h->coups[q].src;
+                if (level[i] < 0) { level[i] = level[j] + 1; queue.push_back(i); }
+            }
+        }
+        int maxl = 0;
+        for (int j = 0; j < ns; ++j) maxl = std::max(maxl, level[j]);
+        for (int j = 0; j < ns; ++j) if (level[j] < 0) level[j] = maxl + 1;
+        build_schedule(h, 0, level);
+        build_schedule(h, 1, level);
+        reciprocals(h);
+        h->nxs = (h->g.B[0] + 31) / 32;
+        CREATE_CUDA(upload_schedule(h, 0));
+        CREATE_CUDA(upload_schedule(h, 1));
+        if (h->sched[0].ok && h->sched[1].ok) CREATE_CUDA(smg::strip_init(h));
+    }
     CREATE_CUDA(cudaEventCreate(&h->ev0));
     CREATE_CUDA(cudaEventCreate(&h->ev1));
     CREATE_CUDA(cudaStreamSynchronize(h->stream));
@@ -448,14 +600,48 @@ int smg_set_dt(smg_handle* h, double dt) {
     return SMG_OK;
 }
 
-static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s) {
-    for (int64_t k = 0; k < nsteps; ++k) {
-        cudaError_t e;
-        if ((e = smg::launch_phase(h, 0, 1, s)) != cudaSuccess) return e;
-        if ((e = smg::launch_phase(h, 1, 0, s)) != cudaSuccess) return e;
-        if ((e = smg::launch_phase(h, 0, 2, s)) != cudaSuccess) return e;
-        if (h->filter_mode == 2 && (e = smg::launch_full_filter(h, s)) != cudaSuccess) return e;
+// Enqueue `nsteps` Strang steps; *launches receives the kernel count.
+// With the strip kernels and no full filter, phase A at the end of a step and
+// phase A at the start of the next are one launch (same sources, the inner
+// set does not change between them): A(k1) B [AA B]... A(k2).
+static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, int64_t* launches) {
+    cudaError_t e;
+    int64_t L = 0;
+    const bool strip = strip_usable(h);
+    const bool fuse = strip && h->variant == SMG_VARIANT_AUTO && h->filter_mode != SMG_FILTER_FULL;
+    const bool hasA = !h->destA.empty();
+    if (fuse && nsteps >= 1) {
+        if (hasA) { if ((e = smg::launch_strip(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
+        for (int64_t k = 0; k < nsteps; ++k) {
+            if ((e = smg::launch_strip(h, 1, 0, s)) != cudaSuccess) return e;
+            ++L;
+            if (!hasA) continue;
+            if (k + 1 < nsteps) e = smg::launch_strip(h, 2, 0, s);
+            else e = smg::launch_strip(h, 0, 2, s);
+            if (e != cudaSuccess) return e;
+            ++L;
+        }
+        if (launches) *launches = L;
+        return cudaSuccess;
     }
+    for (int64_t k = 0; k < nsteps; ++k) {
+        if (strip) {
+            if (hasA) { if ((e = smg::launch_strip(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
+            if ((e = smg::launch_strip(h, 1, 0, s)) != cudaSuccess) return e;
+            ++L;
+            if (hasA) { if ((e = smg::launch_strip(h, 0, 2, s)) != cudaSuccess) return e; ++L; }
+        } else {
+            if (hasA) { if ((e = smg::launch_phase(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
+            if ((e = smg::launch_phase(h, 1, 0, s)) != cudaSuccess) return e;
+            ++L;
+            if (hasA) { if ((e = smg::launch_phase(h, 0, 2, s)) != cudaSuccess) return e; ++L; }
+        }
+        if (h->filter_mode == SMG_FILTER_FULL && h->n_sys > 1) {
+            if ((e = smg::launch_full_filter(h, s)) != cudaSuccess) return e;
+            ++L;
+        }
+    }
+    if (launches) *launches = L;
     return cudaSuccess;
 }
 
@@ -464,7 +650,7 @@ int smg_run(smg_handle* h, int64_t nsteps) {
     if (nsteps < 0) return fail(h, SMG_EINVAL, "smg_run: nsteps must be >= 0");
     if (!h->dt_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_dt has not been called");
     if (!h->state_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_state has not been called");
-    const int64_t kBlock = 16;   // steps per captured graph
+    const int64_t kBlock = 64;   // steps per captured graph
     int64_t left = nsteps;
     if (left >= kBlock) {
         if (!h->graph || h->graph_steps != kBlock) {
@@ -472,7 +658,7 @@ int smg_run(smg_handle* h, int64_t nsteps) {
             h->graph = nullptr;
             cudaGraph_t gr;
             SMG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e = enqueue_steps(h, kBlock, h->stream);
+            cudaError_t e = enqueue_steps(h, kBlock, h->stream, &h->graph_launches);
             cudaError_t e2 = cudaStreamEndCapture(h->stream, &gr);
             if (e != cudaSuccess) return cuda_fail(h, e, "capture step block");
             if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
@@ -482,11 +668,30 @@ int smg_run(smg_handle* h, int64_t nsteps) {
             h->graph_steps = kBlock;
         }
     }
+    int64_t launches = 0, rem = 0;
     SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
-    for (; left >= kBlock; left -= kBlock) SMG_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
-    SMG_CUDA(h, enqueue_steps(h, left, h->stream));
+    for (; left >= kBlock; left -= kBlock) {
+        SMG_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
+        launches += h->graph_launches;
+    }
+    SMG_CUDA(h, enqueue_steps(h, left, h->stream, &rem));
     SMG_CUDA(h, cudaEventRecord(h->ev1, h->stream));
-    h->last_launches = nsteps * smg::launches_per_step(h);
+    h->last_launches = launches + rem;
+    return SMG_OK;
+}
+
+int smg_set_variant(smg_handle* h, int32_t variant) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_variant: NULL handle");
+    if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_STRIP)
+        return fail(h, SMG_EINVAL, "smg_set_variant: unknown variant");
+    if (variant == SMG_VARIANT_STRIP && !(h->sched[0].ok && h->sched[1].ok))
+        return fail(h, SMG_EINVAL, "smg_set_variant: strip schedule does not fit in shared memory");
+    h->variant = variant;
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        h->graph_steps = 0;
+    }
     return SMG_OK;
 }
 

@@ -63,6 +63,75 @@ struct DevArgs {
     int filter_substep;        // 1 if f_position == 'substep'
 };
 
+// ---------------------------------------------------------------------------
+// Strip kernels: a CTA owns 32 consecutive points of one grid row and sweeps a
+// host-built schedule of stages.  A stage first computes derivative slots
+// (one staggered difference of one source component along one axis for the
+// 32 points) into shared memory, then updates destination components whose
+// coupling terms read those slots.  A slot is computed once per phase and
+// freed after its last use; the host assigns ring positions.
+// ---------------------------------------------------------------------------
+struct SlotJob {
+    int src;           // source component
+    int code;          // axis*2 + (source grid type along axis == 2)
+    int slot;          // shared-memory slot
+    int ext[3];        // extents of the difference's output grid
+};
+
+struct DestJob {
+    int comp;
+    int cbeg, cend;    // range in the SCoup table (sumcell order)
+};
+
+struct SCoup {
+    int slot;
+    int pad;
+    double w;
+};
+
+struct Stage {
+    int jbeg, jend;    // slot jobs
+    int dbeg, dend;    // destinations
+};
+
+struct StripSched {
+    const Stage* stages;
+    const SlotJob* jobs;
+    const DestJob* dests;
+    const SCoup* coups;
+    int nstages;
+    int nslots;
+};
+
+struct StripArgs {
+    DevGrid g;
+    double* U;
+    const DevComp* comps;
+    const DevField* fields;
+    StripSched s;
+    int sA, EA;
+    double hdt;
+    double rh[3];      // RN(1/h) per axis
+    int exact_recip[3];  // 1 if the reciprocal correction is exact for this axis
+    int filter_substep;
+};
+
+// (a - b) / h correctly rounded.  When exact_recip is set the quotient is
+// formed from the precomputed reciprocal rh = RN(1/h) and one Markstein
+// correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al.,
+// Handbook of Floating-Point Arithmetic, "Markstein's theorem"): q = RN(d*rh)
+// is within one ulp of d/h whenever |rh*h - 1| < 2^-55 (checked on the host),
+// the residual r = d - q*h is exact in one FMA, and RN(q + r*rh) is the
+// correctly rounded quotient.  Otherwise the IEEE division is used.
+__device__ __forceinline__ double sdiv(double d, double h, double rh, int exact_recip) {
+    if (exact_recip) {
+        const double q = __dmul_rn(d, rh);
+        const double r = __fma_rn(-q, h, d);
+        return __fma_rn(r, rh, q);
+    }
+    return __ddiv_rn(d, h);
+}
+
 __device__ __forceinline__ double fld(const DevField* f, int i, long long pt) {
     const DevField F = f[i];
     return F.p ? __ldg(F.p + pt) : F.s;

@@ -44,14 +44,35 @@ struct smg_handle {
     // CUDA graph of a block of steps
     cudaGraphExec_t graph = nullptr;
     int64_t graph_steps = 0;
+    int64_t graph_launches = 0;
     std::string err;
+    // strip-kernel schedules (phase 0 = A, 1 = B); empty if not usable
+    struct HostSched {
+        std::vector<smg::Stage> stages;
+        std::vector<smg::SlotJob> jobs;
+        std::vector<smg::DestJob> dests;
+        std::vector<smg::SCoup> coups;
+        int nslots = 0;
+        bool ok = false;
+        void* dmem = nullptr;        // device copy of the four tables
+        smg::StripSched view{};
+    } sched[2];
+    int variant = 0;                 // SMG_VARIANT_*
+    double rh[3] = {0, 0, 0};
+    int exact_recip[3] = {0, 0, 0};
+    int nxs = 0;                     // 32-point strips per row
 };
 
 namespace smg {
 // kernels (smg_phase.cu)
 cudaError_t launch_phase(const smg_handle* h, int phase, int kfilter, cudaStream_t s);
+// strip kernels: mode 0 = phase A with filter k, 1 = phase B, 2 = fused A(k=2) A(k=1)
+cudaError_t launch_strip(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
+int strip_smem_bytes(const smg_handle* h, int phase);
+cudaError_t strip_init(const smg_handle* h);
+constexpr int kStripWarps = 8;
+constexpr int kMaxStripSmem = 200 * 1024;
 cudaError_t launch_full_filter(const smg_handle* h, cudaStream_t s);
 cudaError_t launch_decay(double* out, const double* sigma, long long n, double dt, cudaStream_t s);
 cudaError_t launch_finite(const smg_handle* h, int* flag, cudaStream_t s);
-int launches_per_step(const smg_handle* h);
 }  // namespace smg

@@ -30,6 +30,10 @@ from .init import _noop_output, capargs, nargin, zero
 
 __all__ = ["starmap_solver", "GpuSolver", "prepare", "expm1div", "colon", "step_times"]
 
+VARIANT_AUTO, VARIANT_GENERIC, VARIANT_STRIP = 0, 1, 2
+#: kernel family used by :func:`starmap_solver` (all variants give identical results)
+DEFAULT_VARIANT = VARIANT_AUTO
+
 
 def expm1div(x):
     """(exp(x)-1)/x with the reference's Taylor branch (starmap_solver.m:531-535)."""
@@ -162,6 +166,9 @@ class GpuSolver:
 
     def set_dt(self, dt):
         check(self._L.smg_set_dt(self.h, float(dt)), self.h)
+
+    def set_variant(self, variant):
+        check(self._L.smg_set_variant(self.h, int(variant)), self.h)
 
     def run(self, nsteps):
         check(self._L.smg_run(self.h, int(nsteps)), self.h)
@@ -354,6 +361,15 @@ def _build(S, sA1, sT1, EA, ET, Q, F):
         T.add(("Q", j), q, S.G(j))
     for key, val in F.items():
         T.add(("F",) + key, val, key[:3])
+    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
+    if DEFAULT_VARIANT != VARIANT_AUTO:
+        solver.set_variant(DEFAULT_VARIANT)
+    return solver, T
+
+
+def handle_tables(S, T) -> dict:
+    """Per-component field indices of the C-ABI descriptor for setup ``S`` and table ``T``."""
+    n_sys = S.n_sys
     key = lambda j: (*S.G(j), int(S.mom_order[j]))
     sigma_t = [0] + [T.index[("sT",) + key(j)] for j in range(1, n_sys)]
     decay_t = [0] + [T.index[("ET",) + key(j)] for j in range(1, n_sys)]
@@ -369,9 +385,8 @@ def _build(S, sA1, sT1, EA, ET, Q, F):
             f2 = [-1] + [T.index[("F",) + fkey(j) + (2,)] for j in range(1, n_sys)]
         else:
             f1 = [-1] + [T.index[("F",) + fkey(j)] for j in range(1, n_sys)]
-    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, sigma_t, T.index[("sA",)], source,
-                       decay_t=decay_t, decay_a=T.index[("EA",)], filter_mode=mode, filter1=f1, filter2=f2)
-    return solver, T
+    return dict(sigma_t=sigma_t, sigma_a=T.index[("sA",)], source=source, decay_t=decay_t,
+                decay_a=T.index[("EA",)], filter_mode=mode, filter1=f1, filter2=f2)
 
 
 def _output_struct(S, U):
@@ -389,6 +404,38 @@ def _output_struct(S, U):
     return out
 
 
+def first_step(S):
+    """Materials, dt, decay factors, source and filter tables as the reference
+    evaluates them for the first step (starmap_solver.m:165-305)."""
+    tfinal = float(S.par["tfinal"])
+    cn = float(S.par["cn"])
+    sA, sT = _materials(S, 0.0)
+    dt = min(S.dt_hyp, (tfinal - 0.0) / cn) * cn
+    if S.time_dependent.any():
+        sA0, sT0 = sA, sT
+        sA, sT = _materials(S, dt)
+        sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
+        sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
+    else:
+        sA1, sT1 = sA[1, 1, 1], sT
+    EA = expm1div(-sA1 * dt / 2)
+    ET = {k: expm1div(-sT1[k] * dt / 2) for k in S.sg}
+    Q = _sources(S, dt, dt)
+    F = _filters(S, dt, dt) if S.flag_filter else {}
+    return dict(sA=sA, sT=sT, sA1=sA1, sT1=sT1, EA=EA, ET=ET, dt=dt, Q=Q, F=F)
+
+
+def setup_gpu(par: dict):
+    """Host setup plus library handle for ``par`` (state and dt not yet set).
+
+    Returns ``(S, fs, solver, table)``: the setup, the first-step data, the
+    :class:`GpuSolver` and the field table (for later ``set_field`` calls)."""
+    S = prepare(par)
+    fs = first_step(S)
+    solver, T = _build(S, fs["sA1"], fs["sT1"], fs["EA"], fs["ET"], fs["Q"], fs["F"])
+    return S, fs, solver, T
+
+
 def starmap_solver(par: dict):
     """Run the StaRMAP time loop on the GPU; returns the reference's ``output``.
 
@@ -400,24 +447,11 @@ def starmap_solver(par: dict):
     tfinal = float(par["tfinal"])
     cn = float(par["cn"])
     td_any = bool(S.time_dependent.any())
-    # first-step materials and dt (starmap_solver.m:165-213)
-    sA, sT = _materials(S, 0.0)
-    dt = min(S.dt_hyp, (tfinal - 0.0) / cn) * cn
-    if td_any:
-        sA0, sT0 = sA, sT
-        sA, sT = _materials(S, dt)
-        sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
-        sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
-    else:
-        sA1, sT1 = sA[1, 1, 1], sT
-    EA = expm1div(-sA1 * dt / 2)
-    ET = {k: expm1div(-sT1[k] * dt / 2) for k in S.sg}
-    t = dt
-    Q = _sources(S, t, dt)
-    F = _filters(S, dt, t) if S.flag_filter else {}
+    fs = first_step(S)
+    sA, sT, sA1, sT1, dt = fs["sA"], fs["sT"], fs["sA1"], fs["sT1"], fs["dt"]
     cpu_setup = time.perf_counter() - t_start
 
-    solver, T = _build(S, sA1, sT1, EA, ET, Q, F)
+    solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], fs["F"])
     t_gpu0 = time.perf_counter()
     try:
         solver.set_state(S.U0)

@@ -32,8 +32,14 @@ def compare(out_gpu, out_ref):
     return worst, mism
 
 
+VARIANTS = {"auto": 0, "generic": 1, "strip": 2}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("name", sorted(cases.ALL))
-def test_parity_small(name):
+def test_parity_small(name, variant, monkeypatch):
+    from starmap_b200 import solver as solver_mod
+    monkeypatch.setattr(solver_mod, "DEFAULT_VARIANT", VARIANTS[variant])
     par = starmap_init(cases.ALL[name]())
     ref = O.starmap_solver(par)
     out = starmap_solver(par)
@@ -83,3 +89,52 @@ def test_state_roundtrip_and_layout():
         assert solver.check_finite() == 0
     finally:
         solver.close()
+
+
+def test_full_size_lattice_prefix_vs_c_oracle():
+    """The benchmark workload at full size (820 moments, 350x350) for a prefix
+    of 4 steps, GPU (default fused strip kernels) vs the oracle's C restatement."""
+    from oracle import c_oracle
+    from starmap_b200 import configs
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(configs.lattice())
+    nsteps = 4
+    ref = c_oracle.run(par, max_steps=nsteps)
+    S, fs, solver, T = setup_gpu(par)
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.run(nsteps)
+        U = solver.get_state()
+    finally:
+        solver.close()
+    worst = 0.0
+    mism = 0
+    for j in range(S.n_sys):
+        r = ref.U[j]
+        worst = max(worst, rel_l2(U[j], r))
+        mism += int(np.count_nonzero(U[j] != r))
+    assert ref.step_count == nsteps
+    assert worst <= REL_L2_TOL
+    assert mism == 0
+
+
+def test_variants_agree_on_c1_linesource():
+    """Line source P7 100x100 to t=1 (67 steps): all kernel variants bit-identical."""
+    from starmap_b200 import configs
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(configs.linesource())
+    outs = []
+    for v in (0, 1, 2):
+        S, fs, solver, T = setup_gpu(par)
+        try:
+            solver.set_variant(v)
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.run(67)
+            outs.append(solver.get_state())
+        finally:
+            solver.close()
+    for j in outs[0]:
+        np.testing.assert_array_equal(outs[0][j], outs[1][j])
+        np.testing.assert_array_equal(outs[0][j], outs[2][j])
