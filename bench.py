@@ -206,7 +206,7 @@ def main():
     ap.add_argument("--steps", type=int, default=321)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--variant", choices=["auto", "generic", "strip"], default="auto",
+    ap.add_argument("--variant", choices=["auto", "generic", "strip", "staged", "pair"], default="auto",
                     help="kernel family (all give identical results)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -230,9 +230,9 @@ def main():
     n_sys = S.n_sys
     cells = int(np.prod(S.n))
     upd_step = n_sys * cells
-    variant = {"auto": 0, "generic": 1, "strip": 2}[args.variant]
+    variant = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4}[args.variant]
     solver.set_variant(variant)
-    alg = algorithmic_bytes_per_step(S, T, fused=(variant == 0))
+    alg = algorithmic_bytes_per_step(S, T, fused=(variant in (0, 3, 4)))
     solver.set_state(S.U0)
     solver.set_dt(fs["dt"])
     solver.run(args.warmup)

@@ -49,9 +49,11 @@ extern "C" {
 #define SMG_ENOMEM     -5   /* device allocation failed */
 #define SMG_ESTATE     -6   /* call out of order (e.g. run before the state is set) */
 
-#define SMG_VARIANT_AUTO    0  /* strip kernels; phase A of consecutive steps fused (default) */
+#define SMG_VARIANT_AUTO    0  /* best available kernel family (pair, else strip); phase A fused (default) */
 #define SMG_VARIANT_GENERIC 1  /* point-per-thread kernels, one launch per half step */
 #define SMG_VARIANT_STRIP   2  /* strip kernels, one launch per half step */
+#define SMG_VARIANT_STAGED  3  /* strip kernels, slot-job loads staged by cp.async; phase A fused */
+#define SMG_VARIANT_PAIR    4  /* two points per thread, destination-centric; phase A fused */
 
 #define SMG_FILTER_NONE    0   /* par.f_position = ''          */
 #define SMG_FILTER_SUBSTEP 1   /* par.f_position = 'substep'   */
@@ -144,6 +146,14 @@ int smg_sync(smg_handle* h);
  * results; AUTO falls back to GENERIC when a schedule does not fit in shared
  * memory.  No reference counterpart (the reference has one CPU code path). */
 int smg_set_variant(smg_handle* h, int32_t variant);
+
+/* Tuning parameters of the kernels (no reference counterpart).  They change
+ * performance only, never results.  Keys: */
+#define SMG_TUNE_PAIR_GROUP  1   /* destinations per CTA of the pair kernel (1..256) */
+#define SMG_TUNE_PAIR_BLOCK  2   /* threads per CTA of the pair kernel (32..256, multiple of 32) */
+#define SMG_TUNE_PAIR_UNROLL 3   /* couplings per inner iteration (1 or 2) */
+#define SMG_TUNE_PAIR_MINB   4   /* register budget: 3 or 4 resident CTAs of 256 threads (64/85 regs) */
+int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the
  * handle's stream) and its launch count. */

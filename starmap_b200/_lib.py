@@ -67,6 +67,7 @@ SIGNATURES = {
     "smg_run": (C.c_int, [C.c_void_p, C.c_int64]),
     "smg_sync": (C.c_int, [C.c_void_p]),
     "smg_set_variant": (C.c_int, [C.c_void_p, C.c_int32]),
+    "smg_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "smg_last_run_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "smg_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_check_finite": (C.c_int, [C.c_void_p]),

@@ -59,6 +59,9 @@ double expm1div_host(double x) {
 
 int extent(int n, int bc, int g) { return (g == 2 && bc == 1) ? n + 1 : n; }
 
+void resolve_pair(smg_handle* h, int phase);
+cudaError_t upload_pair(smg_handle* h, int phase, bool alloc);
+
 void free_device(smg_handle* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
@@ -72,6 +75,14 @@ void free_device(smg_handle* h) {
     for (auto& sc : h->sched) {
         cudaFree(sc.dmem);
         sc.dmem = nullptr;
+    }
+    for (auto& pr : h->pair) {
+        cudaFree(pr.d_dests);
+        cudaFree(pr.d_coff);
+        cudaFree(pr.d_cw);
+        pr.d_dests = nullptr;
+        pr.d_coff = nullptr;
+        pr.d_cw = nullptr;
     }
     h->dU = h->dFields = nullptr;
     h->dComps = nullptr;
@@ -166,10 +177,22 @@ void build_schedule(smg_handle* h, int phase, const std::vector<int>& level) {
             S.jobs.push_back(jb);
         }
         st.jend = (int)S.jobs.size();
+        // a stage with more slot jobs than the staging buffer holds is split
+        // into job-only stages followed by the stage that updates destinations
+        while (st.jend - st.jbeg > smg::kJobCap) {
+            Stage pre{};
+            pre.jbeg = st.jbeg;
+            pre.jend = st.jbeg + smg::kJobCap;
+            pre.dbeg = pre.dend = (int)S.dests.size();
+            S.stages.push_back(pre);
+            st.jbeg = pre.jend;
+        }
+        S.jcap = std::max(S.jcap, st.jend - st.jbeg);
         st.dbeg = (int)S.dests.size();
         for (int j : groups[s]) {
             DestJob dj{};
             dj.comp = j;
+            for (int a = 0; a < 3; ++a) dj.ext[a] = h->comps[j].ext[a];
             dj.cbeg = (int)S.coups.size();
             for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q)
                 S.coups.push_back(SCoup{slot_of[Key(h->coups[q].src, h->coups[q].code)], 0, h->coups[q].w});
@@ -182,7 +205,46 @@ void build_schedule(smg_handle* h, int phase, const std::vector<int>& level) {
             if (kv.second.second == s) freelist.push_back(slot_of[kv.first]);
     }
     S.nslots = std::max(nslots, 1);
-    S.ok = S.nslots * 32 * 8 <= smg::kMaxStripSmem;
+    S.ok = (S.nslots * 32 + S.jcap * 64) * 8 <= smg::kMaxStripSmem;
+}
+
+// Resolve the coefficients of every destination of a schedule: arrays become
+// rows of the strip's shared-memory cache, scalars are stored in the job.
+// Called at creation and whenever a scalar coefficient changes.
+void resolve_coefs(smg_handle* h, int phase) {
+    auto& S = h->sched[phase];
+    std::map<int, int> row_of;
+    S.frows.clear();
+    for (auto& dj : S.dests) {
+        const smg::DevComp& c = h->comps[dj.comp];
+        int f[smg::kNumCoef];
+        if (phase == 1 && dj.comp == 0) {
+            f[smg::kCoefS] = h->sigma_a;
+            f[smg::kCoefE] = h->decay_a >= 0 ? h->decay_a : h->derived_decay_a;
+            f[smg::kCoefF1] = f[smg::kCoefF2] = h->field_one;
+        } else {
+            f[smg::kCoefS] = c.sT;
+            f[smg::kCoefE] = c.ET;
+            f[smg::kCoefF1] = c.F1;
+            f[smg::kCoefF2] = c.F2;
+        }
+        f[smg::kCoefQ] = c.Q;
+        for (int k = 0; k < smg::kNumCoef; ++k) {
+            const smg::DevField& F = h->fields_host[f[k]];
+            if (F.p) {
+                auto it = row_of.find(f[k]);
+                if (it == row_of.end()) {
+                    it = row_of.emplace(f[k], (int)S.frows.size()).first;
+                    S.frows.push_back(f[k]);
+                }
+                dj.row[k] = it->second;
+                dj.sc[k] = 0.0;
+            } else {
+                dj.row[k] = -1;
+                dj.sc[k] = F.s;
+            }
+        }
+    }
 }
 
 cudaError_t upload_schedule(smg_handle* h, int phase) {
@@ -193,8 +255,9 @@ cudaError_t upload_schedule(smg_handle* h, int phase) {
     const size_t b1 = S.jobs.size() * sizeof(smg::SlotJob);
     const size_t b2 = S.dests.size() * sizeof(smg::DestJob);
     const size_t b3 = S.coups.size() * sizeof(smg::SCoup);
+    const size_t b4 = S.frows.size() * sizeof(int);
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t tot = al(b0) + al(b1) + al(b2) + al(b3) + 256;
+    const size_t tot = al(b0) + al(b1) + al(b2) + al(b3) + al(b4) + 256;
     cudaError_t e = cudaMalloc(&S.dmem, tot);
     if (e != cudaSuccess) return e;
     h->bytes += tot;
@@ -202,29 +265,144 @@ cudaError_t upload_schedule(smg_handle* h, int phase) {
     char* p0 = p; p += al(b0);
     char* p1 = p; p += al(b1);
     char* p2 = p; p += al(b2);
-    char* p3 = p;
+    char* p3 = p; p += al(b3);
+    char* p4 = p;
     if ((e = cudaMemcpyAsync(p0, S.stages.data(), b0, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
     if (b1 && (e = cudaMemcpyAsync(p1, S.jobs.data(), b1, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
     if (b2 && (e = cudaMemcpyAsync(p2, S.dests.data(), b2, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
     if (b3 && (e = cudaMemcpyAsync(p3, S.coups.data(), b3, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
+    if (b4 && (e = cudaMemcpyAsync(p4, S.frows.data(), b4, cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) return e;
     S.view.stages = (const smg::Stage*)p0;
     S.view.jobs = (const smg::SlotJob*)p1;
     S.view.dests = (const smg::DestJob*)p2;
     S.view.coups = (const smg::SCoup*)p3;
+    S.view.frows = (const int*)p4;
     S.view.nstages = (int)S.stages.size();
     S.view.nslots = S.nslots;
+    S.view.jcap = S.jcap;
+    S.view.nfrows = (int)S.frows.size();
     return cudaSuccess;
+}
+
+// Re-resolve scalar coefficients of both schedules and refresh the device copy
+// of the destination tables (same sizes, so the graph stays valid).
+cudaError_t refresh_coefs(smg_handle* h) {
+    for (int ph = 0; ph < 2; ++ph) {
+        if (h->pair[ph].d_dests) {
+            resolve_pair(h, ph);
+            cudaError_t e = upload_pair(h, ph, false);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    for (int ph = 0; ph < 2; ++ph) {
+        auto& S = h->sched[ph];
+        if (!S.ok || S.stages.empty() || !S.view.dests) continue;
+        resolve_coefs(h, ph);
+        cudaError_t e = cudaMemcpyAsync((void*)S.view.dests, S.dests.data(), S.dests.size() * sizeof(smg::DestJob),
+                                        cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Pair-kernel tables of one phase: destinations ordered by coupling-graph
+// level (neighbouring CTAs then share sources in L1/L2), couplings in sumcell
+// order with the source slot offset, coefficients resolved to a device array
+// pointer or a scalar.
+void build_pair(smg_handle* h, int phase, const std::vector<int>& level) {
+    auto& P = h->pair[phase];
+    P.dests.clear();
+    P.coff.clear();
+    P.cw.clear();
+    P.ok = (long long)h->n_sys * h->g.cs < (1LL << 31);   // 32-bit element offsets
+    std::vector<int> D = phase == 0 ? h->destA : h->destB;
+    std::stable_sort(D.begin(), D.end(), [&](int a, int b) { return level[a] < level[b]; });
+    for (int j : D) {
+        smg::PairDest d{};
+        d.off = (int)((long long)j * h->g.cs);
+        for (int k = 0; k < 3; ++k) d.ext[k] = h->comps[j].ext[k];
+        int nr = 0;
+        int prev = -1;
+        for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
+            const int code = h->coups[q].code;
+            if (code != prev) {
+                if (nr == smg::kPairRuns) { P.ok = false; break; }
+                d.run[nr] = (int)P.coff.size();
+                d.code[nr] = code;
+                ++nr;
+                prev = code;
+            }
+            P.coff.push_back((int)((long long)h->coups[q].src * h->g.cs));
+            P.cw.push_back(h->coups[q].w);
+        }
+        for (int r = nr; r <= smg::kPairRuns; ++r) d.run[r] = (int)P.coff.size();
+        for (int r = nr; r < smg::kPairRuns; ++r) d.code[r] = 0;
+        P.dests.push_back(d);
+    }
+    P.ndest = (int)P.dests.size();
+}
+
+void resolve_pair(smg_handle* h, int phase) {
+    auto& P = h->pair[phase];
+    for (auto& d : P.dests) {
+        const int j = (int)((long long)d.off / h->g.cs);
+        const smg::DevComp& c = h->comps[j];
+        int f[smg::kNumCoef];
+        if (phase == 1 && j == 0) {
+            f[smg::kCoefS] = h->sigma_a;
+            f[smg::kCoefE] = h->decay_a >= 0 ? h->decay_a : h->derived_decay_a;
+            f[smg::kCoefF1] = f[smg::kCoefF2] = h->field_one;
+        } else {
+            f[smg::kCoefS] = c.sT;
+            f[smg::kCoefE] = c.ET;
+            f[smg::kCoefF1] = c.F1;
+            f[smg::kCoefF2] = c.F2;
+        }
+        f[smg::kCoefQ] = c.Q;
+        for (int k = 0; k < smg::kNumCoef; ++k) {
+            const smg::DevField& F = h->fields_host[f[k]];
+            d.fp[k] = F.p;
+            d.sc[k] = F.p ? 0.0 : F.s;
+        }
+    }
+}
+
+cudaError_t upload_pair(smg_handle* h, int phase, bool alloc) {
+    auto& P = h->pair[phase];
+    if (P.ndest == 0 || !P.ok) return cudaSuccess;
+    cudaError_t e;
+    if (alloc) {
+        const size_t nc = std::max<size_t>(P.coff.size(), 1);
+        if ((e = cudaMalloc(&P.d_dests, sizeof(smg::PairDest) * P.dests.size())) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&P.d_coff, sizeof(int) * nc)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&P.d_cw, sizeof(double) * nc)) != cudaSuccess) return e;
+        h->bytes += sizeof(smg::PairDest) * P.dests.size() + (sizeof(int) + sizeof(double)) * nc;
+        if (!P.coff.empty()) {
+            if ((e = cudaMemcpyAsync(P.d_coff, P.coff.data(), sizeof(int) * P.coff.size(), cudaMemcpyHostToDevice,
+                                     h->stream)) != cudaSuccess)
+                return e;
+            if ((e = cudaMemcpyAsync(P.d_cw, P.cw.data(), sizeof(double) * P.cw.size(), cudaMemcpyHostToDevice,
+                                     h->stream)) != cudaSuccess)
+                return e;
+        }
+    }
+    return cudaMemcpyAsync(P.d_dests, P.dests.data(), sizeof(smg::PairDest) * P.dests.size(),
+                           cudaMemcpyHostToDevice, h->stream);
 }
 
 // RN(1/h) and whether Markstein's correction from it is exact for every
 // dividend (|RN(1/h)*h - 1| < 2^-55 and normal numbers).
 void reciprocals(smg_handle* h) {
+    bool used[3] = {false, false, false};
+    for (const auto& c : h->coups) used[c.code >> 1] = true;
     for (int a = 0; a < 3; ++a) {
         const double hv = h->g.h[a];
         const double r = 1.0 / hv;
         const double e = std::fma(r, hv, -1.0);
         h->rh[a] = r;
-        h->exact_recip[a] = std::isnormal(hv) && std::isnormal(r) && std::fabs(e) < std::ldexp(1.0, -55);
+        // an axis without differences never divides; it does not restrict the kernels
+        h->exact_recip[a] = !used[a] ||
+                            (std::isnormal(hv) && std::isnormal(r) && std::fabs(e) < std::ldexp(1.0, -55));
     }
 }
 
@@ -512,10 +690,21 @@ int smg_create(const smg_problem* p, smg_handle** out) {
         for (int j = 0; j < ns; ++j) if (level[j] < 0) level[j] = maxl + 1;
         build_schedule(h, 0, level);
         build_schedule(h, 1, level);
+        for (int ph = 0; ph < 2; ++ph) {
+            auto& S = h->sched[ph];
+            resolve_coefs(h, ph);
+            S.ok = S.ok && (int)S.frows.size() <= smg::kMaxFieldRows &&
+                   (S.nslots * 32 + S.jcap * 64 + (int)S.frows.size() * 32) * 8 <= smg::kMaxStripSmem;
+        }
         reciprocals(h);
         h->nxs = (h->g.B[0] + 31) / 32;
         CREATE_CUDA(upload_schedule(h, 0));
         CREATE_CUDA(upload_schedule(h, 1));
+        for (int ph = 0; ph < 2; ++ph) {
+            build_pair(h, ph, level);
+            resolve_pair(h, ph);
+            CREATE_CUDA(upload_pair(h, ph, true));
+        }
         if (h->sched[0].ok && h->sched[1].ok) CREATE_CUDA(smg::strip_init(h));
     }
     CREATE_CUDA(cudaEventCreate(&h->ev0));
@@ -566,6 +755,7 @@ int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {
     } else {
         F.s = scalar;
         SMG_CUDA(h, cudaMemcpyAsync(h->dFieldTab + f, &F, sizeof(DevField), cudaMemcpyHostToDevice, h->stream));
+        SMG_CUDA(h, refresh_coefs(h));
     }
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (h->dt_set) return smg_set_dt(h, h->dt);   // refresh derived decays
@@ -590,6 +780,7 @@ int smg_set_dt(smg_handle* h, double dt) {
     }
     SMG_CUDA(h, cudaMemcpyAsync(h->dFieldTab, h->fields_host.data(), sizeof(DevField) * h->fields_host.size(),
                                 cudaMemcpyHostToDevice, h->stream));
+    SMG_CUDA(h, refresh_coefs(h));
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (h->graph) {   // kernel arguments (dt/2) are baked into the graph
         cudaGraphExecDestroy(h->graph);
@@ -607,17 +798,22 @@ int smg_set_dt(smg_handle* h, double dt) {
 static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, int64_t* launches) {
     cudaError_t e;
     int64_t L = 0;
-    const bool strip = strip_usable(h);
-    const bool fuse = strip && h->variant == SMG_VARIANT_AUTO && h->filter_mode != SMG_FILTER_FULL;
+    // AUTO runs the pair kernel when its tables exist (measured fastest on the
+    // 820-moment lattice workload), else the strip kernel, else the generic one
+    const bool pair = (h->variant == SMG_VARIANT_PAIR || h->variant == SMG_VARIANT_AUTO) && h->pair[0].ok && h->pair[1].ok;
+    const bool strip = !pair && strip_usable(h);
+    const bool fuse = ((strip && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_STAGED)) || pair) &&
+                      h->filter_mode != SMG_FILTER_FULL;
     const bool hasA = !h->destA.empty();
+    auto ph = [&](int mode, int kf) { return pair ? smg::launch_pair(h, mode, kf, s) : smg::launch_strip(h, mode, kf, s); };
     if (fuse && nsteps >= 1) {
-        if (hasA) { if ((e = smg::launch_strip(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
+        if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; ++L; }
         for (int64_t k = 0; k < nsteps; ++k) {
-            if ((e = smg::launch_strip(h, 1, 0, s)) != cudaSuccess) return e;
+            if ((e = ph(1, 0)) != cudaSuccess) return e;
             ++L;
             if (!hasA) continue;
-            if (k + 1 < nsteps) e = smg::launch_strip(h, 2, 0, s);
-            else e = smg::launch_strip(h, 0, 2, s);
+            if (k + 1 < nsteps) e = ph(2, 0);
+            else e = ph(0, 2);
             if (e != cudaSuccess) return e;
             ++L;
         }
@@ -680,13 +876,46 @@ int smg_run(smg_handle* h, int64_t nsteps) {
     return SMG_OK;
 }
 
+int smg_tune(smg_handle* h, int32_t key, int32_t value) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_tune: NULL handle");
+    switch (key) {
+        case SMG_TUNE_PAIR_GROUP:
+            if (value < 1 || value > 256) return fail(h, SMG_EINVAL, "smg_tune: group must be 1..256");
+            h->pair_group = value;
+            break;
+        case SMG_TUNE_PAIR_BLOCK:
+            if (value < 32 || value > 256 || value % 32) return fail(h, SMG_EINVAL, "smg_tune: block must be 32..256, x32");
+            h->pair_block = value;
+            break;
+        case SMG_TUNE_PAIR_UNROLL:
+            if (value != 1 && value != 2) return fail(h, SMG_EINVAL, "smg_tune: unroll must be 1 or 2");
+            h->pair_unroll = value;
+            break;
+        case SMG_TUNE_PAIR_MINB:
+            if (value != 3 && value != 4) return fail(h, SMG_EINVAL, "smg_tune: minb must be 3 or 4");
+            h->pair_minb = value;
+            break;
+        default:
+            return fail(h, SMG_EINVAL, "smg_tune: unknown key");
+    }
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        h->graph_steps = 0;
+    }
+    return SMG_OK;
+}
+
 int smg_set_variant(smg_handle* h, int32_t variant) {
     if (!h) return fail(h, SMG_EINVAL, "smg_set_variant: NULL handle");
-    if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_STRIP)
+    if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_PAIR)
         return fail(h, SMG_EINVAL, "smg_set_variant: unknown variant");
-    if (variant == SMG_VARIANT_STRIP && !(h->sched[0].ok && h->sched[1].ok))
+    if ((variant == SMG_VARIANT_STRIP || variant == SMG_VARIANT_STAGED) && !(h->sched[0].ok && h->sched[1].ok))
         return fail(h, SMG_EINVAL, "smg_set_variant: strip schedule does not fit in shared memory");
+    if (variant == SMG_VARIANT_PAIR && !(h->pair[0].ok && h->pair[1].ok))
+        return fail(h, SMG_EINVAL, "smg_set_variant: pair tables unavailable for this problem");
     h->variant = variant;
+    h->strip_staged = variant == SMG_VARIANT_STAGED;
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;

@@ -78,9 +78,18 @@ struct SlotJob {
     int ext[3];        // extents of the difference's output grid
 };
 
+// Coefficients of a destination are resolved on the host: each of sigma_t,
+// decay, source, filter k=1, filter k=2 is either a row of the CTA's
+// shared-memory field cache (row >= 0) or the scalar sc[].
+enum { kCoefS = 0, kCoefE = 1, kCoefQ = 2, kCoefF1 = 3, kCoefF2 = 4, kNumCoef = 5 };
+
 struct DestJob {
     int comp;
     int cbeg, cend;    // range in the SCoup table (sumcell order)
+    int ext[3];        // extents of the destination's grid
+    int row[kNumCoef];
+    int pad;
+    double sc[kNumCoef];
 };
 
 struct SCoup {
@@ -99,8 +108,11 @@ struct StripSched {
     const SlotJob* jobs;
     const DestJob* dests;
     const SCoup* coups;
+    const int* frows;  // field index of each cached row
     int nstages;
     int nslots;
+    int jcap;          // staging rows (slot jobs) of the largest stage
+    int nfrows;        // cached coefficient rows
 };
 
 struct StripArgs {
@@ -113,6 +125,32 @@ struct StripArgs {
     double hdt;
     double rh[3];      // RN(1/h) per axis
     int exact_recip[3];  // 1 if the reciprocal correction is exact for this axis
+    int filter_substep;
+};
+
+// Pair kernel tables: destinations with resolved coefficients (array pointer
+// or scalar) and couplings with the source's slot offset.
+constexpr int kPairRuns = 6;   // coupling runs per destination (x/y/z lists, split by source grid)
+
+struct PairDest {
+    int off;           // component slot offset (elements)
+    int ext[3];
+    int run[kPairRuns + 1];   // runs [run[r], run[r+1]) of equal source code, in sumcell order
+    int code[kPairRuns];      // source grid code of each run: axis*2 + (grid type == 2)
+    const double* fp[kNumCoef];   // array coefficient, or nullptr -> sc
+    double sc[kNumCoef];
+};
+
+struct PairArgs {
+    DevGrid g;
+    double* U;
+    const PairDest* dests;
+    const int* coff;           // source slot offset (elements) per coupling
+    const double* cw;          // M_d(j,i) per coupling
+    int ndest, group, ngroups, nchunks;
+    double hdt;
+    double rh[3];
+    int exact_recip[3];
     int filter_substep;
 };
 

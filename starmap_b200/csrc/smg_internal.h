@@ -53,14 +53,31 @@ struct smg_handle {
         std::vector<smg::DestJob> dests;
         std::vector<smg::SCoup> coups;
         int nslots = 0;
+        int jcap = 0;                // most slot jobs of one stage (staging rows)
+        std::vector<int> frows;      // field index of each cached coefficient row
         bool ok = false;
         void* dmem = nullptr;        // device copy of the four tables
         smg::StripSched view{};
     } sched[2];
+    struct PairTables {
+        std::vector<smg::PairDest> dests;
+        std::vector<int> coff;
+        std::vector<double> cw;
+        smg::PairDest* d_dests = nullptr;
+        int* d_coff = nullptr;
+        double* d_cw = nullptr;
+        int ndest = 0;
+        bool ok = false;
+    } pair[2];
+    int pair_group = 8;              // destinations per pair-kernel CTA
+    int pair_block = 64;             // threads per pair-kernel CTA (upper bound)
+    int pair_unroll = 1;             // couplings per inner iteration
+    int pair_minb = 4;               // resident CTAs the register budget targets
     int variant = 0;                 // SMG_VARIANT_*
     double rh[3] = {0, 0, 0};
     int exact_recip[3] = {0, 0, 0};
     int nxs = 0;                     // 32-point strips per row
+    bool strip_staged = false;       // stage slot-job loads with cp.async
 };
 
 namespace smg {
@@ -68,10 +85,13 @@ namespace smg {
 cudaError_t launch_phase(const smg_handle* h, int phase, int kfilter, cudaStream_t s);
 // strip kernels: mode 0 = phase A with filter k, 1 = phase B, 2 = fused A(k=2) A(k=1)
 cudaError_t launch_strip(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
+cudaError_t launch_pair(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
 int strip_smem_bytes(const smg_handle* h, int phase);
 cudaError_t strip_init(const smg_handle* h);
 constexpr int kStripWarps = 8;
 constexpr int kMaxStripSmem = 200 * 1024;
+constexpr int kJobCap = 48;          // slot jobs per stage; larger stages are split
+constexpr int kMaxFieldRows = 64;    // coefficient rows cached per strip
 cudaError_t launch_full_filter(const smg_handle* h, cudaStream_t s);
 cudaError_t launch_decay(double* out, const double* sigma, long long n, double dt, cudaStream_t s);
 cudaError_t launch_finite(const smg_handle* h, int* flag, cudaStream_t s);

@@ -14,6 +14,8 @@
 // are disjoint sets, so the update is in place without a race.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "smg_internal.h"
 
 namespace smg {
@@ -79,9 +81,75 @@ __global__ void __launch_bounds__(256) k_phase_generic(DevArgs a, int kf) {
 // of the start of the next (the inner set is unchanged in between, so the
 // differences are the same and the update is applied twice: filter k=2 then
 // k=1, exactly the sequence of two separate launches).
-template <int MODE>
-__global__ void __launch_bounds__(32 * kStripWarps) k_phase_strip(StripArgs a, int kf) {
-    extern __shared__ double sl[];   // [nslots][32]
+//
+// Shared memory: [nslots][32] derivative slots, (STAGED only) [jcap][2][32]
+// staged raw values of the next stage's slot jobs, [nfrows][32] coefficient
+// rows of this strip (loaded once; coefficients are constant in a launch).
+// Per stage s:
+//   (STAGED) wait for the asynchronous copies of stage s;  barrier
+//   load this warp's destination values of stage s into registers
+//   slot jobs of stage s -> (hi-lo)/h -> shared slot: from the staged copies
+//     (STAGED), or from global loads issued kJobBatch jobs at a time
+//   barrier
+//   (STAGED) issue cp.async (8 B per lane, zero-filled outside the
+//     difference's extent) of stage s+1's raw values
+//   destinations of stage s: fold the slots, exponential update, store
+constexpr int kDestBatch = 4;   // destinations per warp whose loads are batched
+constexpr int kJobBatch = 4;    // slot jobs per warp whose loads are batched
+constexpr int kMaxUnrolledCoup = 8;
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Addresses of U_src[hi] and U_src[lo] for this lane's point (base of the
+// component when the point lies outside the difference's extent).
+__device__ __forceinline__ bool job_addr(const StripArgs& a, const SlotJob& jb, int x, int y, int z, long long pt,
+                                         const double*& ph, const double*& pl) {
+    const bool valid = x < jb.ext[0] && y < jb.ext[1] && z < jb.ext[2];
+    const double* base = a.U + (long long)jb.src * a.g.cs;
+    ph = base;
+    pl = base;
+    if (valid) {
+        const int ax = jb.code >> 1;
+        const int pc = ax == 0 ? x : (ax == 1 ? y : z);
+        const long long stv = ax == 0 ? 1 : (ax == 1 ? a.g.s1 : a.g.s2);
+        int hi, lo;
+        stencil(pc, a.g.n[ax], a.g.bc[ax], jb.code & 1, hi, lo);
+        ph = base + pt + (hi - pc) * stv;
+        pl = base + pt + (lo - pc) * stv;
+    }
+    return valid;
+}
+
+__device__ __forceinline__ void stage_jobs(const StripArgs& a, int jbeg, int jend, double* stg, int warp,
+                                           int lane, int x, int y, int z, long long pt) {
+    for (int q = jbeg + warp; q < jend; q += kStripWarps) {
+        const SlotJob jb = a.s.jobs[q];
+        const double *ph, *pl;
+        const bool valid = job_addr(a, jb, x, y, z, pt, ph, pl);
+        double* d = stg + (q - jbeg) * 64;
+        cp_async8(d + lane, ph, valid);
+        cp_async8(d + 32 + lane, pl, valid);
+    }
+    cp_async_commit();
+}
+
+__device__ __forceinline__ double coef(const DestJob& dj, int k, const double* frow, int lane) {
+    return dj.row[k] >= 0 ? frow[dj.row[k] * 32 + lane] : dj.sc[k];
+}
+
+template <int MODE, bool STAGED>
+__global__ void __launch_bounds__(32 * kStripWarps, 3) k_phase_strip(StripArgs a, int kf) {
+    extern __shared__ double smem[];
+    const StripSched& S = a.s;
+    double* sl = smem;                                       // derivative slots
+    double* stg = smem + S.nslots * 32;                      // staged raw values
+    double* frow = stg + (STAGED ? S.jcap * 64 : 0);         // coefficient rows
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nxs = (a.g.B[0] + 31) >> 5;
@@ -92,63 +160,332 @@ __global__ void __launch_bounds__(32 * kStripWarps) k_phase_strip(StripArgs a, i
     const int z = (int)(row / a.g.B[1]);
     const int x = xs * 32 + lane;
     const long long pt = (long long)z * a.g.s2 + (long long)y * a.g.s1 + x;
-    const StripSched S = a.s;
+    if (STAGED && S.nstages > 0) {
+        const Stage st0 = S.stages[0];
+        stage_jobs(a, st0.jbeg, st0.jend, stg, warp, lane, x, y, z, pt);
+    }
+    for (int r = warp; r < S.nfrows; r += kStripWarps) {
+        const DevField F = a.fields[S.frows[r]];
+        frow[r * 32 + lane] = (x < a.g.B[0]) ? __ldg(F.p + pt) : 0.0;
+    }
     for (int s = 0; s < S.nstages; ++s) {
         const Stage st = S.stages[s];
-        for (int q = st.jbeg + warp; q < st.jend; q += kStripWarps) {
-            const SlotJob jb = S.jobs[q];
-            double v = 0.0;
-            if (x < jb.ext[0] && y < jb.ext[1] && z < jb.ext[2]) {
-                const int ax = jb.code >> 1;
-                const int pc = ax == 0 ? x : (ax == 1 ? y : z);
-                const long long stv = ax == 0 ? 1 : (ax == 1 ? a.g.s1 : a.g.s2);
-                int hi, lo;
-                stencil(pc, a.g.n[ax], a.g.bc[ax], jb.code & 1, hi, lo);
-                const double* Us = a.U + (long long)jb.src * a.g.cs + pt;
-                const double d = __dsub_rn(__ldg(Us + (hi - pc) * stv), __ldg(Us + (lo - pc) * stv));
-                v = sdiv(d, a.g.h[ax], a.rh[ax], a.exact_recip[ax]);
+        if (STAGED) cp_async_wait_all();
+        __syncthreads();
+        // destination loads of this stage, issued before the slot-job math
+        double uv[kDestBatch];
+        const int nd = st.dend - st.dbeg;
+#pragma unroll
+        for (int k = 0; k < kDestBatch; ++k) {
+            uv[k] = 0.0;
+            const int q = warp + k * kStripWarps;
+            if (q < nd) {
+                const DestJob& dj = S.dests[st.dbeg + q];
+                const int comp = dj.comp;
+                if (x < dj.ext[0] && y < dj.ext[1] && z < dj.ext[2]) uv[k] = a.U[(long long)comp * a.g.cs + pt];
             }
-            sl[jb.slot * 32 + lane] = v;
+        }
+        if (STAGED) {
+            for (int q = st.jbeg + warp; q < st.jend; q += kStripWarps) {
+                const SlotJob jb = S.jobs[q];
+                const double* d = stg + (q - st.jbeg) * 64;
+                const int ax = jb.code >> 1;
+                sl[jb.slot * 32 + lane] =
+                    sdiv(__dsub_rn(d[lane], d[32 + lane]), a.g.h[ax], a.rh[ax], a.exact_recip[ax]);
+            }
+        } else {
+            for (int q0 = st.jbeg + warp; q0 < st.jend; q0 += kJobBatch * kStripWarps) {
+                double hv[kJobBatch], lv[kJobBatch];
+                int slot[kJobBatch], axv[kJobBatch];
+#pragma unroll
+                for (int k = 0; k < kJobBatch; ++k) {
+                    const int q = q0 + k * kStripWarps;
+                    hv[k] = lv[k] = 0.0;
+                    slot[k] = -1;
+                    axv[k] = 0;
+                    if (q < st.jend) {
+                        const SlotJob jb = S.jobs[q];
+                        const double *ph, *pl;
+                        if (job_addr(a, jb, x, y, z, pt, ph, pl)) {
+                            hv[k] = __ldg(ph);
+                            lv[k] = __ldg(pl);
+                        }
+                        slot[k] = jb.slot;
+                        axv[k] = jb.code >> 1;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kJobBatch; ++k) {
+                    if (slot[k] < 0) continue;
+                    const int ax = axv[k];
+                    sl[slot[k] * 32 + lane] = sdiv(__dsub_rn(hv[k], lv[k]), a.g.h[ax], a.rh[ax], a.exact_recip[ax]);
+                }
+            }
         }
         __syncthreads();
-        for (int q = st.dbeg + warp; q < st.dend; q += kStripWarps) {
-            const DestJob dj = S.dests[q];
-            const int j = dj.comp;
-            const DevComp cj = a.comps[j];
-            if (!(x < cj.ext[0] && y < cj.ext[1] && z < cj.ext[2])) continue;
-            double* Uj = a.U + (long long)j * a.g.cs + pt;
-            double u = *Uj;
-            const double qv = fld(a.fields, cj.Q, pt);
+        if (STAGED && s + 1 < S.nstages) {
+            const Stage sn = S.stages[s + 1];
+            stage_jobs(a, sn.jbeg, sn.jend, stg, warp, lane, x, y, z, pt);
+        }
+        for (int k = 0; k * kStripWarps + warp < nd; ++k) {
+            const DestJob dj = S.dests[st.dbeg + warp + k * kStripWarps];
+            if (!(x < dj.ext[0] && y < dj.ext[1] && z < dj.ext[2])) continue;
+            double* Uj = a.U + (long long)dj.comp * a.g.cs + pt;
+            double u = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < kDestBatch; ++kk)
+                if (kk == k) u = uv[kk];
+            if (k >= kDestBatch) u = *Uj;
+            const double qv = coef(dj, kCoefQ, frow, lane);
+            const double sv = coef(dj, kCoefS, frow, lane);
+            const double E = coef(dj, kCoefE, frow, lane);
             double Ssum = 0.0;
-            for (int c = dj.cbeg; c < dj.cend; ++c) {
-                const SCoup cp = S.coups[c];
-                const double term = __dmul_rn(sl[cp.slot * 32 + lane], cp.w);
-                Ssum = (c == dj.cbeg) ? term : __dadd_rn(Ssum, term);
+            const int cb = dj.cbeg, nc = dj.cend - dj.cbeg;
+            if (nc <= kMaxUnrolledCoup) {
+                // all coupling descriptors and slot values are loaded before the fold
+                double tv[kMaxUnrolledCoup], wv[kMaxUnrolledCoup];
+#pragma unroll
+                for (int c = 0; c < kMaxUnrolledCoup; ++c) {
+                    if (c < nc) {
+                        const SCoup cp = S.coups[cb + c];
+                        tv[c] = sl[cp.slot * 32 + lane];
+                        wv[c] = cp.w;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < kMaxUnrolledCoup; ++c) {
+                    if (c < nc) {
+                        const double term = __dmul_rn(tv[c], wv[c]);
+                        Ssum = c == 0 ? term : __dadd_rn(Ssum, term);
+                    }
+                }
+            } else {
+                for (int c = 0; c < nc; ++c) {
+                    const SCoup cp = S.coups[cb + c];
+                    const double term = __dmul_rn(sl[cp.slot * 32 + lane], cp.w);
+                    Ssum = c == 0 ? term : __dadd_rn(Ssum, term);
+                }
             }
             const double W = -Ssum;
             if (MODE == 0) {
-                u = upd(u, W, qv, fld(a.fields, cj.sT, pt), fld(a.fields, cj.ET, pt), a.hdt);
-                if (a.filter_substep) u = __dmul_rn(u, fld(a.fields, kf == 1 ? cj.F1 : cj.F2, pt));
+                u = upd(u, W, qv, sv, E, a.hdt);
+                if (a.filter_substep) u = __dmul_rn(u, coef(dj, kf == 1 ? kCoefF1 : kCoefF2, frow, lane));
             } else if (MODE == 2) {
-                const double s = fld(a.fields, cj.sT, pt), E = fld(a.fields, cj.ET, pt);
-                u = upd(u, W, qv, s, E, a.hdt);
-                if (a.filter_substep) u = __dmul_rn(u, fld(a.fields, cj.F2, pt));
-                u = upd(u, W, qv, s, E, a.hdt);
-                if (a.filter_substep) u = __dmul_rn(u, fld(a.fields, cj.F1, pt));
-            } else if (j == 0) {
-                const double s = fld(a.fields, a.sA, pt), E = fld(a.fields, a.EA, pt);
-                u = upd(u, W, qv, s, E, a.hdt);
-                u = upd(u, W, qv, s, E, a.hdt);
+                u = upd(u, W, qv, sv, E, a.hdt);
+                if (a.filter_substep) u = __dmul_rn(u, coef(dj, kCoefF2, frow, lane));
+                u = upd(u, W, qv, sv, E, a.hdt);
+                if (a.filter_substep) u = __dmul_rn(u, coef(dj, kCoefF1, frow, lane));
             } else {
-                const double s = fld(a.fields, cj.sT, pt), E = fld(a.fields, cj.ET, pt);
-                u = upd(u, W, qv, s, E, a.hdt);
-                if (a.filter_substep) u = __dmul_rn(u, fld(a.fields, cj.F1, pt));
-                u = upd(u, W, qv, s, E, a.hdt);
-                if (a.filter_substep) u = __dmul_rn(u, fld(a.fields, cj.F2, pt));
+                // phase B: component 0 carries sA/EA and unit filters (resolved on the host)
+                u = upd(u, W, qv, sv, E, a.hdt);
+                if (a.filter_substep) u = __dmul_rn(u, coef(dj, kCoefF1, frow, lane));
+                u = upd(u, W, qv, sv, E, a.hdt);
+                if (a.filter_substep) u = __dmul_rn(u, coef(dj, kCoefF2, frow, lane));
             }
             *Uj = u;
         }
-        __syncthreads();
+    }
+    if (STAGED) cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// Pair kernel: destination-centric, one thread per two adjacent points of a
+// row (x = 2t, 2t+1), a CTA per (group of destinations, row).  Each coupling
+// term is formed from the source values at the stencil neighbours (128-bit
+// loads of the neighbouring rows for y/z differences, 64-bit loads for the x
+// difference), divided exactly by h (sdiv), multiplied by M_d(j,i) and folded
+// in sumcell order; the update runs in registers and the pair is stored once.
+// A destination's couplings come in at most three runs (its x-, y- and
+// z-lists); within a run the stencil offsets, h and the division are fixed,
+// so they are selected once per run.  No shared memory and no barriers.
+// EXACT: every axis admits the exact reciprocal division.
+// ---------------------------------------------------------------------------
+template <bool EXACT>
+__device__ __forceinline__ double pdiv(double d, double h, double rh, int exact) {
+    if (EXACT) {
+        const double q = __dmul_rn(d, rh);
+        const double r = __fma_rn(-q, h, d);
+        return __fma_rn(r, rh, q);
+    }
+    return sdiv(d, h, rh, exact);
+}
+
+__device__ __forceinline__ void pair_coef(const PairDest& dj, int k, const double* Fbase_unused, long long pt,
+                                          bool v1, double& c0, double& c1) {
+    const double* p = dj.fp[k];
+    if (p) {
+        if (v1) {
+            const double2 f = __ldg(reinterpret_cast<const double2*>(p + pt));
+            c0 = f.x;
+            c1 = f.y;
+        } else {
+            c0 = __ldg(p + pt);
+            c1 = 0.0;
+        }
+    } else {
+        c0 = c1 = dj.sc[k];
+    }
+}
+
+template <int MODE, bool EXACT, int UNROLL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_phase_pair(PairArgs a, int kf) {
+    const int ngroups = a.ngroups;
+    const int bid = blockIdx.x;
+    const int grp = bid % ngroups;
+    const int rest = bid / ngroups;
+    const int chunk = rest % a.nchunks;
+    const int row = rest / a.nchunks;
+    const int y = row % a.g.B[1];
+    const int z = row / a.g.B[1];
+    const int t = chunk * blockDim.x + threadIdx.x;
+    const int x0 = 2 * t;
+    if (x0 >= a.g.B[0]) return;
+    const int x1 = x0 + 1;
+    const long long pt = (long long)z * a.g.s2 + (long long)y * a.g.s1 + x0;
+    const double* Upt = a.U + pt;
+    // stencil offsets (elements, relative to x0) for both source grid types
+    int oh0[2], ol0[2], oh1[2], ol1[2], ry[4];   // ry: axis 1 (hi, lo) per g2
+    int rz[4];                                    // axis 2 (hi, lo) per g2
+#pragma unroll
+    for (int g2 = 0; g2 < 2; ++g2) {
+        int hi, lo;
+        stencil(x0, a.g.n[0], a.g.bc[0], g2, hi, lo);
+        oh0[g2] = hi - x0;
+        ol0[g2] = lo - x0;
+        stencil(x1, a.g.n[0], a.g.bc[0], g2, hi, lo);
+        oh1[g2] = hi - x0;
+        ol1[g2] = lo - x0;
+        stencil(y, a.g.n[1], a.g.bc[1], g2, hi, lo);
+        ry[2 * g2] = (hi - y) * (int)a.g.s1;
+        ry[2 * g2 + 1] = (lo - y) * (int)a.g.s1;
+        stencil(z, a.g.n[2], a.g.bc[2], g2, hi, lo);
+        rz[2 * g2] = (hi - z) * (int)a.g.s2;
+        rz[2 * g2 + 1] = (lo - z) * (int)a.g.s2;
+    }
+    const int d0 = grp * a.group;
+    const int d1 = min(d0 + a.group, a.ndest);
+    for (int di = d0; di < d1; ++di) {
+        const PairDest& dj = a.dests[di];
+        const int ex0 = dj.ext[0];
+        if (y >= dj.ext[1] || z >= dj.ext[2] || x0 >= ex0) continue;
+        const bool v1 = x1 < ex0;
+        double* Uj = a.U + pt + dj.off;
+        double u0, u1;
+        if (v1) {
+            const double2 u = *reinterpret_cast<const double2*>(Uj);
+            u0 = u.x;
+            u1 = u.y;
+        } else {
+            u0 = *Uj;
+            u1 = 0.0;
+        }
+        double q0, q1, s0, s1, E0, E1;
+        pair_coef(dj, kCoefQ, nullptr, pt, v1, q0, q1);
+        pair_coef(dj, kCoefS, nullptr, pt, v1, s0, s1);
+        pair_coef(dj, kCoefE, nullptr, pt, v1, E0, E1);
+        double SA = 0.0, SB = 0.0;
+        bool first = true;
+        for (int r = 0; r < kPairRuns; ++r) {
+            const int cb = dj.run[r], ce = dj.run[r + 1];
+            if (cb == ce) continue;
+            const int code = dj.code[r];
+            const int ax = code >> 1, g2 = code & 1;
+            const double hh = ax == 0 ? a.g.h[0] : (ax == 1 ? a.g.h[1] : a.g.h[2]);
+            const double rr = ax == 0 ? a.rh[0] : (ax == 1 ? a.rh[1] : a.rh[2]);
+            const int ee = ax == 0 ? a.exact_recip[0] : (ax == 1 ? a.exact_recip[1] : a.exact_recip[2]);
+            if (ax == 0) {
+                // x difference: four 64-bit loads per coupling (both points)
+                const int ha = g2 ? oh0[1] : oh0[0], la = g2 ? ol0[1] : ol0[0];
+                const int hb = v1 ? (g2 ? oh1[1] : oh1[0]) : 0, lb = v1 ? (g2 ? ol1[1] : ol1[0]) : 0;
+                int c = cb;
+                if (UNROLL >= 2) {
+                    for (; c + 1 < ce; c += 2) {
+                        const int o0 = a.coff[c], o1 = a.coff[c + 1];
+                        const double w0 = a.cw[c], w1 = a.cw[c + 1];
+                        const double a0 = __ldg(Upt + (o0 + ha)), b0 = __ldg(Upt + (o0 + la));
+                        const double c0 = __ldg(Upt + (o0 + hb)), e0 = __ldg(Upt + (o0 + lb));
+                        const double a1 = __ldg(Upt + (o1 + ha)), b1 = __ldg(Upt + (o1 + la));
+                        const double c1 = __ldg(Upt + (o1 + hb)), e1 = __ldg(Upt + (o1 + lb));
+                        const double tA0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(a0, b0), hh, rr, ee), w0);
+                        const double tB0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(c0, e0), hh, rr, ee), w0);
+                        const double tA1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(a1, b1), hh, rr, ee), w1);
+                        const double tB1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(c1, e1), hh, rr, ee), w1);
+                        if (first) { SA = tA0; SB = tB0; first = false; }
+                        else { SA = __dadd_rn(SA, tA0); SB = __dadd_rn(SB, tB0); }
+                        SA = __dadd_rn(SA, tA1);
+                        SB = __dadd_rn(SB, tB1);
+                    }
+                }
+                for (; c < ce; ++c) {
+                    const int o = a.coff[c];
+                    const double w = a.cw[c];
+                    const double dA = pdiv<EXACT>(__dsub_rn(__ldg(Upt + (o + ha)), __ldg(Upt + (o + la))), hh, rr, ee);
+                    const double dB = pdiv<EXACT>(__dsub_rn(__ldg(Upt + (o + hb)), __ldg(Upt + (o + lb))), hh, rr, ee);
+                    const double tA = __dmul_rn(dA, w), tB = __dmul_rn(dB, w);
+                    if (first) { SA = tA; SB = tB; first = false; }
+                    else { SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB); }
+                }
+            } else {
+                // y or z difference: two 128-bit loads per coupling (both points)
+                const int oh = ax == 1 ? (g2 ? ry[2] : ry[0]) : (g2 ? rz[2] : rz[0]);
+                const int ol = ax == 1 ? (g2 ? ry[3] : ry[1]) : (g2 ? rz[3] : rz[1]);
+                int c = cb;
+                if (UNROLL >= 2) {
+                    // two couplings per iteration: all four row loads issued first
+                    for (; c + 1 < ce; c += 2) {
+                        const int o0 = a.coff[c], o1 = a.coff[c + 1];
+                        const double w0 = a.cw[c], w1 = a.cw[c + 1];
+                        const double2 hv0 = __ldg(reinterpret_cast<const double2*>(Upt + (o0 + oh)));
+                        const double2 lv0 = __ldg(reinterpret_cast<const double2*>(Upt + (o0 + ol)));
+                        const double2 hv1 = __ldg(reinterpret_cast<const double2*>(Upt + (o1 + oh)));
+                        const double2 lv1 = __ldg(reinterpret_cast<const double2*>(Upt + (o1 + ol)));
+                        const double tA0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv0.x, lv0.x), hh, rr, ee), w0);
+                        const double tB0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv0.y, lv0.y), hh, rr, ee), w0);
+                        const double tA1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv1.x, lv1.x), hh, rr, ee), w1);
+                        const double tB1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv1.y, lv1.y), hh, rr, ee), w1);
+                        if (first) { SA = tA0; SB = tB0; first = false; }
+                        else { SA = __dadd_rn(SA, tA0); SB = __dadd_rn(SB, tB0); }
+                        SA = __dadd_rn(SA, tA1);
+                        SB = __dadd_rn(SB, tB1);
+                    }
+                }
+                for (; c < ce; ++c) {
+                    const int o = a.coff[c];
+                    const double w = a.cw[c];
+                    const double2 hv = __ldg(reinterpret_cast<const double2*>(Upt + (o + oh)));
+                    const double2 lv = __ldg(reinterpret_cast<const double2*>(Upt + (o + ol)));
+                    const double tA = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv.x, lv.x), hh, rr, ee), w);
+                    const double tB = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv.y, lv.y), hh, rr, ee), w);
+                    if (first) { SA = tA; SB = tB; first = false; }
+                    else { SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB); }
+                }
+            }
+        }
+        const double WA = -SA, WB = -SB;
+        if (MODE == 0) {
+            u0 = upd(u0, WA, q0, s0, E0, a.hdt);
+            u1 = upd(u1, WB, q1, s1, E1, a.hdt);
+            if (a.filter_substep) {
+                double f0, f1;
+                pair_coef(dj, kf == 1 ? kCoefF1 : kCoefF2, nullptr, pt, v1, f0, f1);
+                u0 = __dmul_rn(u0, f0);
+                u1 = __dmul_rn(u1, f1);
+            }
+        } else {
+            double f0 = 1.0, f1 = 1.0, g0 = 1.0, g1 = 1.0;   // first / second substep filter
+            if (a.filter_substep) {
+                pair_coef(dj, MODE == 2 ? kCoefF2 : kCoefF1, nullptr, pt, v1, f0, f1);
+                pair_coef(dj, MODE == 2 ? kCoefF1 : kCoefF2, nullptr, pt, v1, g0, g1);
+            }
+            u0 = upd(u0, WA, q0, s0, E0, a.hdt);
+            u1 = upd(u1, WB, q1, s1, E1, a.hdt);
+            if (a.filter_substep) { u0 = __dmul_rn(u0, f0); u1 = __dmul_rn(u1, f1); }
+            u0 = upd(u0, WA, q0, s0, E0, a.hdt);
+            u1 = upd(u1, WB, q1, s1, E1, a.hdt);
+            if (a.filter_substep) { u0 = __dmul_rn(u0, g0); u1 = __dmul_rn(u1, g1); }
+        }
+        if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1);
+        else *Uj = u0;
     }
 }
 
@@ -217,16 +554,27 @@ cudaError_t launch_phase(const smg_handle* h, int phase, int kfilter, cudaStream
     return cudaGetLastError();
 }
 
-int strip_smem_bytes(const smg_handle* h, int phase) { return h->sched[phase].nslots * 32 * 8; }
+int strip_smem_bytes(const smg_handle* h, int phase) {
+    const auto& S = h->sched[phase];
+    const int staging = h->strip_staged ? S.jcap * 64 : 0;
+    return (S.nslots * 32 + staging + (int)S.frows.size() * 32) * 8;
+}
 
 // Opt the strip kernels into the dynamic shared memory the schedules need
 // (called once at handle creation, outside any stream capture).
 cudaError_t strip_init(const smg_handle* h) {
     const int smem = max(strip_smem_bytes(h, 0), strip_smem_bytes(h, 1));
+    const int smem_st = max((h->sched[0].nslots * 32 + h->sched[0].jcap * 64 + (int)h->sched[0].frows.size() * 32) * 8,
+                            (h->sched[1].nslots * 32 + h->sched[1].jcap * 64 + (int)h->sched[1].frows.size() * 32) * 8);
+    const int big = max(smem, smem_st);
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_phase_strip<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_phase_strip<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_phase_strip<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+#define SMG_ATTR(M, ST)                                                                                       \
+    if ((e = cudaFuncSetAttribute(k_phase_strip<M, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) != \
+        cudaSuccess)                                                                                          \
+        return e;
+    SMG_ATTR(0, false) SMG_ATTR(1, false) SMG_ATTR(2, false) SMG_ATTR(0, true) SMG_ATTR(1, true) SMG_ATTR(2, true)
+#undef SMG_ATTR
+    return cudaSuccess;
 }
 
 cudaError_t launch_strip(const smg_handle* h, int mode, int kfilter, cudaStream_t s) {
@@ -250,17 +598,56 @@ cudaError_t launch_strip(const smg_handle* h, int mode, int kfilter, cudaStream_
     const long long blocks = (long long)h->nxs * h->g.B[1] * h->g.B[2];
     const int smem = strip_smem_bytes(h, phase);
     const dim3 block(32 * kStripWarps);
-    switch (mode) {
-        case 0:
-            k_phase_strip<0><<<(unsigned)blocks, block, smem, s>>>(a, kfilter);
-            break;
-        case 1:
-            k_phase_strip<1><<<(unsigned)blocks, block, smem, s>>>(a, kfilter);
-            break;
-        default:
-            k_phase_strip<2><<<(unsigned)blocks, block, smem, s>>>(a, kfilter);
-            break;
+    const unsigned nb = (unsigned)blocks;
+    if (h->strip_staged) {
+        if (mode == 0) k_phase_strip<0, true><<<nb, block, smem, s>>>(a, kfilter);
+        else if (mode == 1) k_phase_strip<1, true><<<nb, block, smem, s>>>(a, kfilter);
+        else k_phase_strip<2, true><<<nb, block, smem, s>>>(a, kfilter);
+    } else {
+        if (mode == 0) k_phase_strip<0, false><<<nb, block, smem, s>>>(a, kfilter);
+        else if (mode == 1) k_phase_strip<1, false><<<nb, block, smem, s>>>(a, kfilter);
+        else k_phase_strip<2, false><<<nb, block, smem, s>>>(a, kfilter);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair(const smg_handle* h, int mode, int kfilter, cudaStream_t s) {
+    const int phase = mode == 1 ? 1 : 0;
+    const auto& P = h->pair[phase];
+    if (P.ndest == 0) return cudaSuccess;
+    PairArgs a{};
+    a.g = h->g;
+    a.U = h->dU;
+    a.dests = P.d_dests;
+    a.coff = P.d_coff;
+    a.cw = P.d_cw;
+    a.ndest = P.ndest;
+    a.group = h->pair_group;
+    a.ngroups = (P.ndest + a.group - 1) / a.group;
+    const int tpr = (h->g.B[0] + 1) / 2;   // threads per row
+    const int bs = std::min(h->pair_block, (tpr + 31) / 32 * 32);
+    a.nchunks = (tpr + bs - 1) / bs;
+    a.hdt = h->hdt;
+    for (int k = 0; k < 3; ++k) {
+        a.rh[k] = h->rh[k];
+        a.exact_recip[k] = h->exact_recip[k];
+    }
+    a.filter_substep = h->filter_mode == 1;
+    const long long blocks = (long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2];
+    const bool exact = h->exact_recip[0] && h->exact_recip[1] && h->exact_recip[2];
+    const unsigned nb = (unsigned)blocks;
+    const int cfg = (exact ? 1 : 0) | (h->pair_unroll >= 2 ? 2 : 0) | (h->pair_minb >= 4 ? 4 : 0);
+#define SMG_PAIR(E, U, M)                                                                \
+    case (E ? 1 : 0) | (U == 2 ? 2 : 0) | (M == 4 ? 4 : 0):                              \
+        if (mode == 0) k_phase_pair<0, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);          \
+        else if (mode == 1) k_phase_pair<1, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);     \
+        else k_phase_pair<2, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);                    \
+        break;
+    switch (cfg) {
+        SMG_PAIR(true, 1, 3) SMG_PAIR(true, 2, 3) SMG_PAIR(true, 1, 4) SMG_PAIR(true, 2, 4)
+        SMG_PAIR(false, 1, 3) SMG_PAIR(false, 2, 3) SMG_PAIR(false, 1, 4) SMG_PAIR(false, 2, 4)
+    }
+#undef SMG_PAIR
     return cudaGetLastError();
 }
 

@@ -170,6 +170,9 @@ class GpuSolver:
     def set_variant(self, variant):
         check(self._L.smg_set_variant(self.h, int(variant)), self.h)
 
+    def tune(self, key, value):
+        check(self._L.smg_tune(self.h, int(key), int(value)), self.h)
+
     def run(self, nsteps):
         check(self._L.smg_run(self.h, int(nsteps)), self.h)
 

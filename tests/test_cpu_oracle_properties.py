@@ -1,0 +1,65 @@
+"""Oracle pins: the reference's own known-answer properties, checked on the CPU
+restatements (no GPU).
+
+* P_N == SP_N zeroth moment for isotropic data (starmap_2d_ex_boxes.m:7-16:
+  "identical (up to machine accuracy)").
+* Mass of the zeroth moment is conserved with sigma_a = 0, no source and
+  periodic boundaries (the staggered differences telescope).
+* The line source stays symmetric under x <-> y on a square grid.
+* The numpy and C restatements agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import c_oracle
+from oracle import solver_np as O
+from starmap_b200 import configs, starmap_init
+
+
+def boxes_prob(closure, N, n=40, tfinal=1.0):
+    def src(x, y):
+        return (((1.75 < x) & (x <= 2.25) & (1.75 < y) & (y <= 2.25)) |
+                ((2.75 < x) & (x <= 3.25) & (1.5 < y) & (y <= 2.5))).astype(float) * 2.0
+    return dict(closure=closure, n_mom=N, ax=[0, 5, 0, 5], n=[n, n], bc=[1, 1],
+                sigma_a=lambda x, y: 0.9, sigma_s0=lambda x, y: 0.1, source=src,
+                tfinal=tfinal, t_plot=[0, tfinal], quiet=True)
+
+
+@pytest.mark.parametrize("N", [3, 5, 9])
+def test_pn_equals_spn_for_isotropic_data(N):
+    rP = O.starmap_solver(starmap_init(boxes_prob("P", N)))
+    rS = O.starmap_solver(starmap_init(boxes_prob("SP", N)))
+    a, b = rP.output[0]["U"], rS.output[0]["U"]
+    assert rP.step_count == rS.step_count
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
+
+def test_mass_conservation_void_periodic():
+    par = starmap_init(configs.linesource(n=30, n_mom=7, tfinal=1.0))
+    r = O.starmap_solver(par)
+    X, Y = np.meshgrid(r.output[0]["x"], r.output[0]["y"], indexing="ij")
+    m0 = (np.exp(-(X ** 2 + Y ** 2) / (2 * 0.03 ** 2)) / (2 * np.pi * 0.03 ** 2)).sum()
+    assert abs(r.output[0]["U"].sum() - m0) <= 1e-13 * m0
+
+
+def test_linesource_xy_symmetry():
+    r = O.starmap_solver(starmap_init(configs.linesource(n=30, n_mom=5, tfinal=1.0)))
+    U = r.output[0]["U"]
+    assert np.abs(U - U.T).max() <= 1e-13 * np.abs(U).max()
+
+
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "box3d_bc1_p2_full", "td_sigma", "spn_3d"])
+def test_numpy_and_c_restatements_agree(name):
+    par = starmap_init(cases.ALL[name]())
+    a = O.starmap_solver(par)
+    b = c_oracle.run(par, nthreads=2)
+    for u, v in zip(a.output, b.output):
+        np.testing.assert_array_equal(u["U"], v["U"])
+
+
+def test_step_count_overshoot_quirk():
+    # dt fixed after the first step; the last step overshoots tfinal (starmap_solver.m:165-208)
+    par = starmap_init(configs.linesource(n=100, n_mom=7, tfinal=1.0))
+    r = O.starmap_solver(par, max_steps=None)
+    assert r.step_count == 67 and r.t > 1.0

@@ -32,7 +32,7 @@ def compare(out_gpu, out_ref):
     return worst, mism
 
 
-VARIANTS = {"auto": 0, "generic": 1, "strip": 2}
+VARIANTS = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -125,7 +125,7 @@ def test_variants_agree_on_c1_linesource():
     from starmap_b200.solver import setup_gpu
     par = starmap_init(configs.linesource())
     outs = []
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3, 4):
         S, fs, solver, T = setup_gpu(par)
         try:
             solver.set_variant(v)
@@ -138,3 +138,26 @@ def test_variants_agree_on_c1_linesource():
     for j in outs[0]:
         np.testing.assert_array_equal(outs[0][j], outs[1][j])
         np.testing.assert_array_equal(outs[0][j], outs[2][j])
+        np.testing.assert_array_equal(outs[0][j], outs[3][j])
+        np.testing.assert_array_equal(outs[0][j], outs[4][j])
+
+
+def test_gpu_pn_equals_spn_boxes():
+    from test_cpu_oracle_properties import boxes_prob
+    outP = starmap_solver(starmap_init(boxes_prob("P", 9)))
+    outS = starmap_solver(starmap_init(boxes_prob("SP", 9)))
+    a, b = outP[0]["U"], outS[0]["U"]
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
+
+def test_full_size_linesource_properties():
+    """2D P7 line source at full size (100x100, t=1, 67 steps): mass of the
+    zeroth moment conserved, x<->y symmetric, all moments finite."""
+    from starmap_b200 import configs
+    out = starmap_solver(starmap_init(configs.linesource()))
+    U = out[0]["U"]
+    X, Y = np.meshgrid(out[0]["x"], out[0]["y"], indexing="ij")
+    m0 = (np.exp(-(X ** 2 + Y ** 2) / (2 * 0.03 ** 2)) / (2 * np.pi * 0.03 ** 2)).sum()
+    assert abs(U.sum() - m0) <= 1e-12 * m0
+    assert np.abs(U - U.T).max() <= 1e-12 * np.abs(U).max()
+    assert all(np.isfinite(o["U"]).all() for o in out)
