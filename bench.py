@@ -167,6 +167,49 @@ def cpu_sample(par, budget_s: float, nthreads: int, max_steps: int | None = None
     return len(secs), sum(secs)
 
 
+def bench_batch(steps: int = 200):
+    """Batched sweep: 256 seeded 2D instances (edge 64..256, N in {3,5,7,11,15},
+    8x8-block log-uniform materials, own CFL dt), `steps` steps each, batched
+    (autotuned) vs a loop of plain per-instance runs."""
+    from starmap_b200 import configs, starmap_init
+    from starmap_b200.batch import _tables, setup_batch
+    from starmap_b200.solver import GpuSolver, handle_tables
+    pars = [starmap_init(p) for p in configs.batched_sweep()]
+    setups, batch = setup_batch(pars)
+    mc = sum(S.n_sys * int(np.prod(S.n)) for S, _ in setups)
+    U0 = [S.U0 for S, _ in setups]
+    batch.set_states(U0)
+    batch.set_dt([fs["dt"] for _, fs in setups])
+    batch.autotune(4)
+    batch.set_states(U0)
+    batch.run(steps)
+    ms, launches = batch.last_run_stats()
+    cfg = batch.config()
+    batch.close()
+    solvers = []
+    for S, fs in setups:
+        T = _tables(S, fs)
+        sv = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
+        sv.set_state(S.U0)
+        sv.set_dt(fs["dt"])
+        solvers.append(sv)
+    t0 = time.perf_counter()
+    dev = 0.0
+    for sv in solvers:
+        sv.run(steps)
+        sv.sync()
+        dev += sv.last_run_stats()[0]
+    wall = time.perf_counter() - t0
+    for sv in solvers:
+        sv.close()
+    batched = mc * steps / (ms / 1e3)
+    loop = mc * steps / wall
+    return {"value": batched, "unit": UNIT, "instances": len(pars), "moment_cells": mc, "steps": steps,
+            "ms": ms, "launches": launches, "config": cfg,
+            "plain_loop_value": loop, "plain_loop_device_value": mc * steps / (dev / 1e3),
+            "batched_over_plain_loop": batched / loop}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -210,6 +253,7 @@ def main():
                     help="kernel family (all give identical results)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline stepping")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of reference-arm stepping")
     args = ap.parse_args()
@@ -296,6 +340,8 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
+    if world == 1 and not args.no_batch:
+        line["batched"] = bench_batch()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         steps, secs = cpu_sample(par, budget_s=args.cpu_budget, nthreads=threads, warm=0)

@@ -172,6 +172,43 @@ int smg_check_finite(smg_handle* h);
 int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz,
                  int32_t* gt_out);
 
+/* ---------------------------------------------------------------------------
+ * Batched solver: many problems (uneven grid sizes and moment orders, each
+ * with its own dt) advanced together by one persistent cooperative launch per
+ * block of steps, the launch sequence replayed from a CUDA graph.  No
+ * reference counterpart: the reference solves one problem per call; a batch
+ * replaces a host loop of starmap_solver calls.  Each instance is an ordinary
+ * handle (state I/O through smg_batch_instance + smg_set_state/smg_get_state).
+ * --------------------------------------------------------------------------- */
+typedef struct smg_batch smg_batch;
+
+#define SMG_BATCH_BLOCK            1  /* threads per CTA (32..256, multiple of 32) */
+#define SMG_BATCH_GROUP            2  /* destinations per work item (1..256) */
+#define SMG_BATCH_STEPS_PER_LAUNCH 3  /* Strang steps per persistent launch */
+#define SMG_BATCH_SPIN_LIMIT       4  /* polls before a grid-barrier wait gives up (SMG_ETIMEOUT) */
+#define SMG_BATCH_BARRIER_EXTRA    5  /* test hook: barrier expects one CTA more than launched (0/1) */
+#define SMG_BATCH_USE_GRAPH        6  /* 1: replay the launch sequence from a CUDA graph */
+#define SMG_BATCH_PERSISTENT       7  /* 1: one cooperative launch per block of steps; 0: one launch per phase */
+
+int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch** out);
+void smg_batch_destroy(smg_batch* b);
+const char* smg_batch_last_error(const smg_batch* b);
+/* Handle of instance i (owned by the batch; do not destroy). */
+smg_handle* smg_batch_instance(smg_batch* b, int32_t i);
+/* dt[i] for every instance (decay factors recomputed as by smg_set_dt). */
+int smg_batch_set_dt(smg_batch* b, const double* dt);
+/* Advance every instance by nsteps Strang steps; SMG_ETIMEOUT if a grid
+ * barrier wait ran out of its spin limit (the state is then undefined). */
+int smg_batch_run(smg_batch* b, int64_t nsteps);
+int smg_batch_last_run_stats(smg_batch* b, double* ms, int64_t* launches);
+int smg_batch_tune(smg_batch* b, int32_t key, int64_t value);
+/* Current block, group, steps per launch and persistent grid size (0 when
+ * the batch runs one launch per phase). */
+int smg_batch_config(const smg_batch* b, int64_t out[4]);
+/* Time probe_steps steps for each candidate configuration (block x group x
+ * steps per launch), keep the fastest; every instance's state is restored. */
+int smg_batch_autotune(smg_batch* b, int64_t probe_steps, double* best_ms);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -73,6 +73,16 @@ SIGNATURES = {
     "smg_check_finite": (C.c_int, [C.c_void_p]),
     "smg_classify": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
+    "smg_batch_destroy": (None, [C.c_void_p]),
+    "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "smg_batch_instance": (C.c_void_p, [C.c_void_p, C.c_int32]),
+    "smg_batch_set_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "smg_batch_run": (C.c_int, [C.c_void_p, C.c_int64]),
+    "smg_batch_last_run_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "smg_batch_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
+    "smg_batch_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "smg_batch_autotune": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
 }
 
 
@@ -94,6 +104,13 @@ def lib():
 def check(code: int, handle=None):
     if code < 0:
         msg = lib().smg_last_error(handle)
+        raise SmgError(code, msg.decode() if msg else "")
+    return code
+
+
+def check_batch(code: int, batch=None):
+    if code < 0:
+        msg = lib().smg_batch_last_error(batch)
         raise SmgError(code, msg.decode() if msg else "")
     return code
 

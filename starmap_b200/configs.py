@@ -102,3 +102,39 @@ def pointsource3d(n=128, n_mom=9, tfinal=0.75, std=0.05, filter_order=4, f_eff=1
     if f_position:
         prob.update(filterfunction=exp_filter(filter_order, f_eff), f_position=f_position)
     return prob
+
+
+def batched_sweep(n_inst=256, seed=20261203, edges=tuple(range(64, 257, 32)), orders=(3, 5, 7, 11, 15)):
+    """Seeded batch of 2D P_N problems of uneven size and order.
+
+    Grid edge uniform over ``edges``, N uniform over ``orders``; sigma_a and
+    sigma_s0 piecewise constant on 8x8 blocks of [-1.5,1.5]^2 drawn
+    log-uniformly in [0.01, 10]; Gaussian initial condition with a random
+    centre in the inner 60% of the domain and standard deviation in
+    [0.02, 0.1]; periodic; the reference's default CFL number (cn = 0.99).
+    Returns a list of ``prob`` dicts (tfinal large: the batch is stepped a
+    fixed number of steps)."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for _ in range(n_inst):
+        edge = int(rng.choice(edges))
+        N = int(rng.choice(orders))
+        sa = 10 ** rng.uniform(-2, 1, size=(8, 8))
+        ss = 10 ** rng.uniform(-2, 1, size=(8, 8))
+        cx, cy = rng.uniform(-0.9, 0.9, size=2)
+        std = rng.uniform(0.02, 0.1)
+
+        def block_field(tab):
+            def f(x, y):
+                i = np.clip(np.floor((x + 1.5) / 3.0 * 8).astype(int), 0, 7)
+                j = np.clip(np.floor((y + 1.5) / 3.0 * 8).astype(int), 0, 7)
+                return tab[i, j]
+            return f
+
+        def gaussian(cx, cy, std):
+            return lambda x, y: np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * std ** 2)) / (2 * np.pi * std ** 2)
+
+        probs.append(dict(name="batch", closure="P", n_mom=N, ax=[-1.5, 1.5, -1.5, 1.5], n=[edge, edge],
+                          bc=[0, 0], ic=gaussian(cx, cy, std), sigma_a=block_field(sa), sigma_s0=block_field(ss),
+                          t_plot=[0.0, 1e9], tfinal=1e9, quiet=True))
+    return probs

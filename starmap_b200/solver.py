@@ -77,56 +77,23 @@ class GpuSolver:
                  decay_t=None, decay_a=-1, filter_mode=FILTER_NONE, filter1=None, filter2=None):
         L = _lib.lib()
         self._L = L
-        n_sys = int(np.asarray(Mz).shape[0])
-        self.n_sys = n_sys
-        self.n = [int(v) for v in n]
-        self.bc = [int(v) for v in bc]
-        self.gt = np.ascontiguousarray(np.asarray(gt, dtype=np.int32).reshape(n_sys, 3))
-        self._keep = []
-
-        def i32(a):
-            arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
-            self._keep.append(arr)
-            return arr
-
-        mats = [np.asfortranarray(np.asarray(M, dtype=np.float64)) for M in (Mx, My, Mz)]
-        self._keep += mats
-        fa = (_lib.smg_field * max(len(fields), 1))()
-        for k, (val, grid) in enumerate(fields):
-            fa[k].grid[:] = [int(g) for g in grid]
-            if np.ndim(val) == 0:
-                fa[k].data = None
-                fa[k].scalar = float(val)
-            else:
-                arr = np.asfortranarray(np.asarray(val, dtype=np.float64)).ravel(order="F")
-                arr = np.ascontiguousarray(arr)
-                self._keep.append(arr)
-                fa[k].data = dptr(arr)
-                fa[k].scalar = 0.0
-        self._fields = fa
-        self.field_grids = [tuple(int(g) for g in grid) for _, grid in fields]
-        p = _lib.smg_problem()
-        p.n_sys = n_sys
-        p.n[:] = self.n
-        p.bc[:] = self.bc
-        p.h[:] = [float(v) for v in h]
-        gtf = i32(self.gt.ravel())
-        p.gt = iptr(gtf)
-        p.Mx, p.My, p.Mz = (dptr(m) for m in mats)
-        p.n_fields = len(fields)
-        p.fields = C_cast_fields(fa)
-        p.sigma_t = iptr(i32(sigma_t))
-        p.decay_t = iptr(i32(decay_t)) if decay_t is not None else None
-        p.sigma_a = int(sigma_a)
-        p.decay_a = int(decay_a)
-        p.source = iptr(i32(source))
-        p.filter_mode = int(filter_mode)
-        p.filter1 = iptr(i32(filter1)) if filter1 is not None else None
-        p.filter2 = iptr(i32(filter2)) if filter2 is not None else None
+        p, keep, info = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
+                                      decay_t, decay_a, filter_mode, filter1, filter2)
+        self.n_sys, self.n, self.bc, self.gt, self.field_grids = info
         handle = _lib.C.c_void_p()
         check(L.smg_create(_lib.C.byref(p), _lib.C.byref(handle)))
         self.h = handle
-        self._keep = []
+        self.owned = True
+
+    @classmethod
+    def borrow(cls, handle, info):
+        """Wrap a handle owned by someone else (a batch instance)."""
+        self = cls.__new__(cls)
+        self._L = _lib.lib()
+        self.n_sys, self.n, self.bc, self.gt, self.field_grids = info
+        self.h = handle
+        self.owned = False
+        return self
 
     # ------------------------------------------------------------------
     def extents(self, j):
@@ -196,7 +163,8 @@ class GpuSolver:
 
     def close(self):
         if getattr(self, "h", None):
-            self._L.smg_destroy(self.h)
+            if getattr(self, "owned", True):
+                self._L.smg_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -208,6 +176,56 @@ class GpuSolver:
 
 def C_cast_fields(fa):
     return _lib.C.cast(fa, _lib.C.POINTER(_lib.smg_field))
+
+
+def build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
+                  decay_t=None, decay_a=-1, filter_mode=FILTER_NONE, filter1=None, filter2=None):
+    """``smg_problem`` for the C ABI plus the arrays it points to (keep them
+    alive until ``smg_create`` returns) and shape info for state transfers."""
+    n_sys = int(np.asarray(Mz).shape[0])
+    n = [int(v) for v in n]
+    bc = [int(v) for v in bc]
+    gt = np.ascontiguousarray(np.asarray(gt, dtype=np.int32).reshape(n_sys, 3))
+    keep = []
+
+    def i32(a):
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+        keep.append(arr)
+        return arr
+
+    mats = [np.asfortranarray(np.asarray(M, dtype=np.float64)) for M in (Mx, My, Mz)]
+    keep += mats
+    fa = (_lib.smg_field * max(len(fields), 1))()
+    keep.append(fa)
+    for k, (val, grid) in enumerate(fields):
+        fa[k].grid[:] = [int(g) for g in grid]
+        if np.ndim(val) == 0:
+            fa[k].data = None
+            fa[k].scalar = float(val)
+        else:
+            arr = np.ascontiguousarray(np.asfortranarray(np.asarray(val, dtype=np.float64)).ravel(order="F"))
+            keep.append(arr)
+            fa[k].data = dptr(arr)
+            fa[k].scalar = 0.0
+    p = _lib.smg_problem()
+    p.n_sys = n_sys
+    p.n[:] = n
+    p.bc[:] = bc
+    p.h[:] = [float(v) for v in h]
+    p.gt = iptr(i32(gt.ravel()))
+    p.Mx, p.My, p.Mz = (dptr(m) for m in mats)
+    p.n_fields = len(fields)
+    p.fields = C_cast_fields(fa)
+    p.sigma_t = iptr(i32(sigma_t))
+    p.decay_t = iptr(i32(decay_t)) if decay_t is not None else None
+    p.sigma_a = int(sigma_a)
+    p.decay_a = int(decay_a)
+    p.source = iptr(i32(source))
+    p.filter_mode = int(filter_mode)
+    p.filter1 = iptr(i32(filter1)) if filter1 is not None else None
+    p.filter2 = iptr(i32(filter2)) if filter2 is not None else None
+    info = (n_sys, n, bc, gt, [tuple(int(g) for g in grid) for _, grid in fields])
+    return p, keep, info
 
 
 # ----------------------------------------------------------------------
