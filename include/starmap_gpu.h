@@ -166,6 +166,11 @@ int smg_layout(const smg_handle* h, int64_t* bytes, int64_t dims_out[4]);
 /* Scan the state for NaN/Inf on the GPU; returns SMG_ENONFINITE if any. */
 int smg_check_finite(smg_handle* h);
 
+/* Sum of squares of every component of the state, sumsq[n_sys] (host):
+ * the squared discrete L2 norms monitored by starmap_2d_ex_l2norm.m:93-99
+ * (which applies staggered trapezoid weights on top).  Deterministic order. */
+int smg_state_sumsq(smg_handle* h, double* sumsq);
+
 /* Grid-type classification of starmap_solver.m:76-98 from the sparsity of
  * par.Mx/My/Mz (column-major n_sys x n_sys): writes gt_out[3*j+d] in {1,2}.
  * Host-only helper for callers that do not classify themselves. */

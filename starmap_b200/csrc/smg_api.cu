@@ -72,6 +72,8 @@ void free_device(smg_handle* h) {
     cudaFree(h->dFieldTab);
     cudaFree(h->dDest);
     cudaFree(h->dFlag);
+    cudaFree(h->dSumsq);
+    h->dSumsq = nullptr;
     for (auto& sc : h->sched) {
         cudaFree(sc.dmem);
         sc.dmem = nullptr;
@@ -641,7 +643,8 @@ int smg_create(const smg_problem* p, smg_handle** out) {
         (e = alloc((void**)&h->dCoups, sizeof(DevCoup) * std::max<size_t>(h->coups.size(), 1))) != cudaSuccess ||
         (e = alloc((void**)&h->dFieldTab, sizeof(DevField) * nfields)) != cudaSuccess ||
         (e = alloc((void**)&h->dDest, sizeof(int) * ns)) != cudaSuccess ||
-        (e = alloc((void**)&h->dFlag, sizeof(int))) != cudaSuccess) {
+        (e = alloc((void**)&h->dFlag, sizeof(int))) != cudaSuccess ||
+        (e = alloc((void**)&h->dSumsq, sizeof(double) * (size_t)ns * (smg::kSumsqBlocks + 1))) != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "cudaMalloc");
         free_device(h);
         delete h;

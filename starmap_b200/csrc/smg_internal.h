@@ -32,6 +32,7 @@ struct smg_handle {
     smg::DevField* dFieldTab = nullptr;
     int* dDest = nullptr;            // destA followed by destB
     int* dFlag = nullptr;            // device status word (finite check)
+    double* dSumsq = nullptr;        // reduction scratch: n_sys*kSumsqBlocks partials + n_sys results
     size_t bytes = 0;
     int nslots = 0;
     // run state
@@ -89,6 +90,10 @@ cudaError_t launch_pair(const smg_handle* h, int mode, int kfilter, cudaStream_t
 int strip_smem_bytes(const smg_handle* h, int phase);
 cudaError_t strip_init(const smg_handle* h);
 constexpr int kStripWarps = 8;
+constexpr int kSumsqBlocks = 32;     // CTAs per component in the sum-of-squares reduction
+constexpr int kSumsqThreads = 256;
+cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
+                         cudaStream_t s);
 constexpr int kMaxStripSmem = 200 * 1024;
 constexpr int kJobCap = 48;          // slot jobs per stage; larger stages are split
 constexpr int kMaxFieldRows = 64;    // coefficient rows cached per strip

@@ -158,6 +158,11 @@ class GpuSolver:
         check(self._L.smg_layout(self.h, _lib.C.byref(b), d), self.h)
         return b.value, list(d)
 
+    def state_sumsq(self):
+        out = np.zeros(self.n_sys)
+        check(self._L.smg_state_sumsq(self.h, dptr(out)), self.h)
+        return out
+
     def check_finite(self):
         return self._L.smg_check_finite(self.h)
 

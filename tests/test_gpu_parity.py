@@ -161,3 +161,25 @@ def test_full_size_linesource_properties():
     assert abs(U.sum() - m0) <= 1e-12 * m0
     assert np.abs(U - U.T).max() <= 1e-12 * np.abs(U).max()
     assert all(np.isfinite(o["U"]).all() for o in out)
+
+
+def test_state_sumsq_reduction():
+    """Per-component sums of squares of the state (deterministic two-pass
+    reduction through the handle's scratch) against the host sum."""
+    from starmap_b200.solver import GpuSolver, prepare
+    par = starmap_init(cases.box3d_bc1_p2_full())
+    S = prepare(par)
+    rng = np.random.default_rng(11)
+    fields = [(0.3, (1, 1, 1)), (1.0, (1, 1, 1))]
+    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, fields, [0] * S.n_sys, 0, [-1] * S.n_sys,
+                       decay_t=[1] * S.n_sys, decay_a=1)
+    try:
+        U = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
+        solver.set_state(U)
+        a = solver.state_sumsq()
+        b = solver.state_sumsq()
+        np.testing.assert_array_equal(a, b)
+        ref = np.array([np.sum(u * u) for u in U])
+        assert np.max(np.abs(a - ref) / ref) <= 1e-13
+    finally:
+        solver.close()
