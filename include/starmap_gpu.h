@@ -171,6 +171,21 @@ int smg_check_finite(smg_handle* h);
  * (which applies staggered trapezoid weights on top).  Deterministic order. */
 int smg_state_sumsq(smg_handle* h, double* sumsq);
 
+/* Sums of squares of ncomp device vectors without allocating any GPU memory.
+ * No counterpart in the reference: it serves hosts that must not allocate on
+ * the device themselves (a MEX gateway that only holds MATLAB-owned gpuArray
+ * buffers, a caller under a fixed device-memory budget).  Vector c holds len
+ * doubles at d_x + c*stride; d_out (device) receives ncomp sums; stream is a
+ * cudaStream_t (NULL: the default stream).  The partial sums live in a fixed
+ * 256 KB array inside the library, resident on every GPU that loads it, so
+ * ncomp is limited to 1024 (larger requests return SMG_EINVAL).  The first
+ * call on a device looks up that array's device address, so make it before
+ * any stream capture on that device.  All calls share the array: calls whose
+ * GPU work overlaps (different streams or threads) race on it.  The message
+ * of a failed call is smg_last_error(NULL). */
+int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t len, double* d_out,
+                      void* stream);
+
 /* Grid-type classification of starmap_solver.m:76-98 from the sparsity of
  * par.Mx/My/Mz (column-major n_sys x n_sys): writes gt_out[3*j+d] in {1,2}.
  * Host-only helper for callers that do not classify themselves. */

@@ -72,6 +72,7 @@ SIGNATURES = {
     "smg_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_check_finite": (C.c_int, [C.c_void_p]),
     "smg_state_sumsq": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "smg_sumsq_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "smg_classify": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),

@@ -414,6 +414,8 @@ bool strip_usable(const smg_handle* h) {
 
 }  // namespace
 
+void smg::set_global_error(const std::string& msg) { fail(nullptr, 0, msg); }
+
 extern "C" {
 
 const char* smg_version(void) { return "starmap_b200 0.1 (sm_100a, fp64)"; }

@@ -92,6 +92,7 @@ cudaError_t strip_init(const smg_handle* h);
 constexpr int kStripWarps = 8;
 constexpr int kSumsqBlocks = 32;     // CTAs per component in the sum-of-squares reduction
 constexpr int kSumsqThreads = 256;
+void set_global_error(const std::string& msg);   // message of smg_last_error(NULL)
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);
 constexpr int kMaxStripSmem = 200 * 1024;

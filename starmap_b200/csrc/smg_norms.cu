@@ -12,6 +12,9 @@
 // Padding points of a slot hold zeros, so the whole slot is summed.
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
+
 #include "../../include/starmap_gpu.h"
 #include "smg_internal.h"
 
@@ -71,5 +74,66 @@ extern "C" int smg_state_sumsq(smg_handle* h, double* sumsq) {
         h->err = std::string("smg_state_sumsq: ") + cudaGetErrorString(e);
         return SMG_ECUDA;
     }
+    return SMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the reduction above.
+//
+// Some hosts of this library must not allocate GPU memory themselves: a MEX
+// gateway running inside MATLAB works with gpuArray buffers that MATLAB's own
+// allocator owns and may not want a second allocator on the device; callers
+// that work under a fixed memory budget cannot afford an allocation (or the
+// synchronisation a cudaMalloc/cudaFree implies) per reduction.  For them the
+// partial sums go to a fixed array that is part of the library image: every
+// GPU that loads the library holds it (256 KB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long long kNoAllocScratch = 32768;   // doubles: 1024 components x 32 partials
+static __device__ __align__(256) double g_sumsq_scratch[kNoAllocScratch];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_addr[kMaxDevices] = {nullptr};
+
+int noalloc_fail(int code, const std::string& m) {
+    smg::set_global_error(m);   // read back with smg_last_error(NULL)
+    return code;
+}
+
+}  // namespace
+
+extern "C" int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t len, double* d_out,
+                                 void* stream) {
+    if (!d_x || !d_out) return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: NULL device pointer");
+    if (ncomp < 1 || len < 1 || stride < len)
+        return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: need ncomp >= 1, len >= 1 and stride >= len");
+    if ((long long)ncomp * smg::kSumsqBlocks > kNoAllocScratch)
+        return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: " + std::to_string(ncomp) +
+                                            " components exceed the fixed scratch (at most " +
+                                            std::to_string(kNoAllocScratch / smg::kSumsqBlocks) + ")");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(SMG_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: device index too large");
+    double* scratch;
+    {
+        // first call on this device (with it current): look up the device
+        // address of the static array; host code cannot use the symbol itself
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        if (!g_scratch_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_sumsq_scratch);
+            if (e != cudaSuccess)
+                return noalloc_fail(SMG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_scratch_addr[dev] = static_cast<double*>(p);
+        }
+        scratch = g_scratch_addr[dev];
+    }
+    // every partial a launch reads is written by the same launch first, so the
+    // contents left by an earlier call need no clearing
+    e = smg::launch_sumsq(d_x, ncomp, stride, len, scratch, d_out, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return noalloc_fail(SMG_ECUDA, std::string("smg_sumsq_noalloc: ") + cudaGetErrorString(e));
     return SMG_OK;
 }
