@@ -193,6 +193,31 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
                  int32_t* gt_out);
 
 /* ---------------------------------------------------------------------------
+ * Discrete adjoint.  No reference counterpart (the reference has no
+ * derivatives); it differentiates exactly the loop smg_run performs.
+ * smg_forward(h, nsteps, K) advances nsteps steps from the current state and
+ * keeps a checkpoint every K steps; smg_misfit(h, obs, &J) evaluates
+ * J = 1/2 sum (U_1(T) - obs)^2 on the zeroth moment (obs: host, component-0
+ * extents) and seeds the adjoint with U_1(T) - obs (smg_adjoint_seed seeds
+ * any adjoint state instead); smg_backward recomputes each segment from its
+ * checkpoint and runs the transposed phases back to t = 0, returning
+ * dJ/dU(0) per component and dJ/d(field) for every sigma and source field:
+ * an array of the field's extents, or one number for a scalar field (the sum
+ * over the points it acts on).  Decay fields are treated as
+ * expm1div(-sigma*dt/2) of their sigma field (their derivative enters the
+ * sigma gradient); filter fields are constants.  Requires f_position '' or
+ * 'substep' and fields that stay fixed between smg_forward and smg_backward.
+ * --------------------------------------------------------------------------- */
+int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every);
+int smg_misfit(smg_handle* h, const double* obs, double* J);
+int smg_adjoint_seed(smg_handle* h, const double* const* lam);
+/* grad_U0[j]: host array (component extents) or NULL; grad_fields[f]: host
+ * array (array field) / one double (scalar field) / NULL, f < n_fields. */
+int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fields);
+/* Device bytes held for checkpoints and adjoint buffers. */
+int smg_adjoint_bytes(const smg_handle* h, int64_t* bytes);
+
+/* ---------------------------------------------------------------------------
  * Batched solver: many problems (uneven grid sizes and moment orders, each
  * with its own dt) advanced together by one persistent cooperative launch per
  * block of steps, the launch sequence replayed from a CUDA graph.  No

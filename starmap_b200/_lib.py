@@ -75,6 +75,11 @@ SIGNATURES = {
     "smg_sumsq_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "smg_classify": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "smg_forward": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
+    "smg_misfit": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "smg_adjoint_seed": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double))]),
+    "smg_backward": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double))]),
+    "smg_adjoint_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
     "smg_batch_destroy": (None, [C.c_void_p]),
     "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),

@@ -1,0 +1,613 @@
+// smg_adjoint.cu -- discrete adjoint of the time loop.
+//
+// Forward: smg_forward runs the Strang loop from the current state and keeps
+// a copy of the state every `ckpt_every` steps.  Backward: for each segment,
+// last to first, the state is recomputed from its checkpoint with one launch
+// per phase (A k=1, B, A k=2 -- the fused A-A form of smg_run computes the
+// same numbers but does not expose the state between the two A phases),
+// recording the state before every phase and every destination's coupling sum
+//   W_j = -sum_c M_d(j,i_c) * D_c U_{i_c}.
+// Then the phases are walked backwards.  A phase updates each destination j
+// pointwise, U'_j = f(U_j, W_j; s_j, E_j, Q_j, F) (one or two dt/2 substeps of
+// starmap_solver.m:352-357, 401-411), where E = expm1div(-s*dt/2).  With
+// lambda' the adjoint after the phase:
+//   k_adj_point  (per destination point)
+//       lambda_j  = (dU'/dU)  lambda'_j
+//       v_j       = (dU'/dW)  lambda'_j
+//       grad_s   += (dU'/ds)  lambda'_j     (through E as well)
+//       grad_Q   += (dU'/dQ)  lambda'_j
+//   k_adj_transpose  (per source point)
+//       lambda_i += - sum_{j,c: i_c = i} M_d(j,i) (D_c^T v_j)
+// i.e. the transposed stencil and coupling.  The seed is the misfit
+// J = 1/2 sum (U_1(T) - obs)^2 on the zeroth moment (smg_misfit) or any
+// adjoint state (smg_adjoint_seed); after all phases lambda = dJ/dU(0).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/starmap_gpu.h"
+#include "smg_internal.h"
+#include "smg_pair.cuh"
+
+namespace smg {
+
+struct AdjCoef {       // resolved coefficient of one destination in one phase
+    const double* p;   // array slot, or nullptr -> scalar s
+    double s;
+};
+
+struct AdjDest {
+    int comp;          // component index
+    int ext[3];
+    AdjCoef sg, E, dE, Q, F1, F2;   // sigma, decay, d(decay)/d(sigma), source, substep filters
+    double* gs;        // gradient slot of sigma's field (nullptr: not tracked)
+    double* gq;        // gradient slot of the source field (nullptr: none)
+};
+
+struct TCoup {         // transposed coupling: source i <- destination slot v
+    int vslot;         // index of the destination in the phase's destination list
+    int code;          // axis*2 + (grid type of source i along axis == 2)
+    double w;          // M_d(j,i)
+};
+
+struct AdjSrc {
+    int comp;
+    int ext[3];
+    int tbeg, tend;
+};
+
+struct AdjData {
+    int64_t nsteps = 0, K = 0, nseg = 0;
+    std::vector<double*> ckpt;
+    double* work = nullptr;
+    double* lam = nullptr;
+    double* V = nullptr;
+    double* rec_state = nullptr;   // [3K][n_sys*cs]
+    double* rec_w = nullptr;       // [3K][maxdest*cs]
+    int maxdest = 0;
+    std::vector<double*> gfield;   // per user field: gradient slot (cs) or nullptr
+    std::vector<double*> dEslot;   // per sigma field: d(decay)/d(sigma) slot (arrays)
+    std::vector<double> dEscalar;  // per sigma field: scalar derivative
+    // per phase (0 = A, 1 = B): destination and source tables, host and device
+    std::vector<AdjDest> dests[2];
+    std::vector<AdjSrc> srcs[2];
+    std::vector<TCoup> tcoup[2];
+    AdjDest* d_dests[2] = {nullptr, nullptr};
+    AdjSrc* d_srcs[2] = {nullptr, nullptr};
+    TCoup* d_tcoup[2] = {nullptr, nullptr};
+    bool ready = false, seeded = false;
+    size_t bytes = 0;
+};
+
+// phi'(x) for phi(x) = (exp(x)-1)/x with the reference's Taylor branch
+// (starmap_solver.m:531-535): the derivative of 1 + x/2 + x^2/6 where that
+// branch is taken, the series sum_k k x^(k-1)/(k+1)! for moderate |x| (the
+// closed form cancels there), and (exp(x)*(x-1) + 1)/x^2 otherwise.
+__host__ __device__ inline double dphi(double x) {
+    if (fabs(x) <= 2e-4) return 0.5 + x / 3.0;
+    if (fabs(x) < 0.25) {
+        double term = 0.5, sum = 0.5;   // k = 1: 1/2!
+        double f = 2.0;                  // (k+1)!
+        double xp = 1.0;
+        for (int k = 2; k <= 16; ++k) {
+            xp *= x;
+            f *= (k + 1);
+            term = k * xp / f;
+            sum += term;
+        }
+        return sum;
+    }
+    return (exp(x) * (x - 1.0) + 1.0) / (x * x);
+}
+
+__global__ void k_dphi(double* out, const double* sigma, long long n, double hdt) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // E = phi(-sigma*dt/2)  ->  dE/dsigma = -dt/2 * phi'(-sigma*dt/2)
+    const double x = -sigma[i] * hdt;
+    out[i] = -hdt * dphi(x);
+}
+
+__device__ __forceinline__ double cval(const AdjCoef& c, long long pt) { return c.p ? c.p[pt] : c.s; }
+
+// MODE 0: phase A, one substep with filter F1 (= filter k of that A phase);
+// MODE 1: phase B, two substeps (filters F1 then F2).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_adj_point(DevGrid g, const AdjDest* dests, const double* __restrict__ pre,
+                                                   const double* __restrict__ W, double* lam, double* V, double hdt) {
+    const long long npts = g.s2 * g.B[2];
+    const long long pt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int di = blockIdx.y;
+    if (pt >= npts) return;
+    const AdjDest d = dests[di];
+    const int x = (int)(pt % g.s1);
+    const int y = (int)((pt / g.s1) % g.B[1]);
+    const int z = (int)(pt / g.s2);
+    if (x >= d.ext[0] || y >= d.ext[1] || z >= d.ext[2]) return;
+    const long long jo = (long long)d.comp * g.cs + pt;
+    const double lp = lam[jo];
+    const double u = pre[jo];
+    const double w = W[(long long)di * g.cs + pt];
+    const double s = cval(d.sg, pt), E = cval(d.E, pt), dE = cval(d.dE, pt), q = cval(d.Q, pt);
+    const double F1 = cval(d.F1, pt);
+    const double r = 1.0 - hdt * s * E;          // d(substep)/dU before the filter
+    double dU, dW, ds;
+    if (MODE == 0) {
+        const double G = w + q - s * u;
+        dU = F1 * r;
+        dW = F1 * hdt * E;
+        ds = F1 * hdt * (-u * E + G * dE);
+    } else {
+        const double F2 = cval(d.F2, pt);
+        const double G0 = w + q - s * u;
+        const double V1 = F1 * (u + hdt * G0 * E);
+        const double G1 = w + q - s * V1;
+        dU = F2 * r * F1 * r;
+        dW = F2 * (r * F1 * hdt * E + hdt * E);
+        ds = F2 * (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE));
+    }
+    lam[jo] = dU * lp;
+    V[(long long)di * g.cs + pt] = dW * lp;
+    if (d.gs) atomicAdd(d.gs + pt, ds * lp);
+    if (d.gq) atomicAdd(d.gq + pt, dW * lp);   // dU'/dQ = dU'/dW
+}
+
+// lambda_i += -sum M_d(j,i) (D^T v_j): D^T of the staggered difference of a
+// source on grid type g2 along one axis (preimages of hi and lo under the
+// stencil of starmap_solver.m:127-132).
+__device__ __forceinline__ double dT(const double* v, int q, int n, int bc, int g2, long long st) {
+    // v points at the destination slot at this source point's linear index
+    if (!g2) {
+        if (bc) {
+            double a = v[0];
+            if (q == n - 1) a += v[st];           // hi(p=n) = n-1
+            double b = v[st];                      // lo(p=q+1) = q
+            if (q == 0) b += v[0];                 // lo(p=0) = 0
+            return a - b;
+        }
+        const long long om = (q == 0) ? (long long)(n - 1) * st : -st;   // p = (q-1) mod n
+        return v[om] - v[0];
+    }
+    if (bc) {
+        const double a = q >= 1 ? v[-st] : 0.0;    // hi(p=q-1) = q
+        const double b = q <= n - 1 ? v[0] : 0.0;  // lo(p=q) = q
+        return a - b;
+    }
+    const long long op = (q == n - 1) ? -(long long)(n - 1) * st : st;    // p = (q+1) mod n
+    return v[0] - v[op];
+}
+
+__global__ void __launch_bounds__(256) k_adj_transpose(DevGrid g, const AdjSrc* srcs, const TCoup* tc,
+                                                       const double* __restrict__ V, double* lam) {
+    const long long npts = g.s2 * g.B[2];
+    const long long pt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int si = blockIdx.y;
+    if (pt >= npts) return;
+    const AdjSrc S = srcs[si];
+    const int x = (int)(pt % g.s1);
+    const int y = (int)((pt / g.s1) % g.B[1]);
+    const int z = (int)(pt / g.s2);
+    if (x >= S.ext[0] || y >= S.ext[1] || z >= S.ext[2]) return;
+    double acc = 0.0;
+    for (int c = S.tbeg; c < S.tend; ++c) {
+        const TCoup t = tc[c];
+        const int ax = t.code >> 1;
+        const int q = ax == 0 ? x : (ax == 1 ? y : z);
+        const long long st = ax == 0 ? 1 : (ax == 1 ? g.s1 : g.s2);
+        const double* v = V + (long long)t.vslot * g.cs + pt;
+        acc += t.w * dT(v, q, g.n[ax], g.bc[ax], t.code & 1, st) / g.h[ax];
+    }
+    lam[(long long)S.comp * g.cs + pt] -= acc;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 4) k_pair_rec(PairArgs a, int kf) {
+    const int bid = blockIdx.x;
+    pair_item<MODE, false, 1, true>(a, kf, bid % a.ngroups, (bid / a.ngroups) % a.nchunks,
+                                    bid / a.ngroups / a.nchunks, threadIdx.x, blockDim.x);
+}
+
+}  // namespace smg
+
+using smg::AdjData;
+
+namespace {
+
+int afail(smg_handle* h, int code, const std::string& m) {
+    h->err = m;
+    return code;
+}
+
+int acuda(smg_handle* h, cudaError_t e, const char* what) {
+    return afail(h, e == cudaErrorMemoryAllocation ? SMG_ENOMEM : SMG_ECUDA,
+                 std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define A_CUDA(h, expr)                                         \
+    do {                                                        \
+        cudaError_t e_ = (expr);                                \
+        if (e_ != cudaSuccess) return acuda((h), e_, #expr);    \
+    } while (0)
+
+size_t state_bytes(const smg_handle* h) { return (size_t)h->g.cs * h->n_sys * sizeof(double); }
+
+// pair-kernel arguments of one phase on an arbitrary state buffer
+smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec) {
+    smg::PairArgs a{};
+    const auto& P = h->pair[phase];
+    a.g = h->g;
+    a.U = U;
+    a.dests = P.d_dests;
+    a.coff = P.d_coff;
+    a.cw = P.d_cw;
+    a.ndest = P.ndest;
+    a.group = 8;
+    a.ngroups = (P.ndest + a.group - 1) / a.group;
+    const int tpr = (h->g.B[0] + 1) / 2;
+    a.nchunks = (tpr + 63) / 64;
+    a.hdt = h->hdt;
+    for (int k = 0; k < 3; ++k) {
+        a.rh[k] = h->rh[k];
+        a.exact_recip[k] = h->exact_recip[k];
+    }
+    a.filter_substep = h->filter_mode == SMG_FILTER_SUBSTEP;
+    a.wrec = wrec;
+    return a;
+}
+
+cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec) {
+    const int phase = mode == 1 ? 1 : 0;
+    const smg::PairArgs a = rec_args(h, phase, U, wrec);
+    if (a.ndest == 0) return cudaSuccess;
+    const unsigned nb = (unsigned)((long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2]);
+    if (mode == 1) smg::k_pair_rec<1><<<nb, 64, 0, h->stream>>>(a, kf);
+    else smg::k_pair_rec<0><<<nb, 64, 0, h->stream>>>(a, kf);
+    return cudaGetLastError();
+}
+
+void free_adj(smg_handle* h) {
+    AdjData* A = h->adj;
+    if (!A) return;
+    for (double* p : A->ckpt) cudaFree(p);
+    cudaFree(A->work);
+    cudaFree(A->lam);
+    cudaFree(A->V);
+    cudaFree(A->rec_state);
+    cudaFree(A->rec_w);
+    for (double* p : A->gfield) cudaFree(p);
+    for (double* p : A->dEslot) cudaFree(p);
+    for (int l = 0; l < 2; ++l) {
+        cudaFree(A->d_dests[l]);
+        cudaFree(A->d_srcs[l]);
+        cudaFree(A->d_tcoup[l]);
+    }
+    delete A;
+    h->adj = nullptr;
+}
+
+smg::AdjCoef coef_of(const smg_handle* h, int f) {
+    const smg::DevField& F = h->fields_host[f];
+    return smg::AdjCoef{F.p, F.p ? 0.0 : F.s};
+}
+
+// Destination/source tables of both phases (call after dE slots exist).
+int build_tables(smg_handle* h) {
+    AdjData* A = h->adj;
+    const int one = h->field_one;
+    for (int l = 0; l < 2; ++l) {
+        // destinations in the pair table's order: the recorded W and the
+        // scratch V use that index as their slot
+        std::vector<int> D;
+        for (const auto& pd : h->pair[l].dests) D.push_back((int)((long long)pd.off / h->g.cs));
+        const std::vector<int>& Sset = l == 0 ? h->destB : h->destA;   // sources of the phase
+        A->dests[l].clear();
+        A->srcs[l].clear();
+        A->tcoup[l].clear();
+        std::map<int, int> slot_of;
+        // phase A has two tables: filter k=1 and filter k=2 as the single filter
+        for (int rep = 0; rep < (l == 0 ? 2 : 1); ++rep)
+            for (int k = 0; k < (int)D.size(); ++k) {
+                const int j = D[k];
+                slot_of[j] = k;
+                const smg::DevComp& c = h->comps[j];
+                smg::AdjDest d{};
+                d.comp = j;
+                for (int a = 0; a < 3; ++a) d.ext[a] = c.ext[a];
+                int fs, fe;
+                if (l == 1 && j == 0) {
+                    fs = h->sigma_a;
+                    fe = h->decay_a >= 0 ? h->decay_a : h->derived_decay_a;
+                    d.F1 = d.F2 = coef_of(h, one);
+                } else {
+                    fs = c.sT;
+                    fe = c.ET;
+                    d.F1 = coef_of(h, rep == 0 ? c.F1 : c.F2);
+                    d.F2 = coef_of(h, c.F2);
+                }
+                d.sg = coef_of(h, fs);
+                d.E = coef_of(h, fe);
+                d.dE = smg::AdjCoef{A->dEslot[fs], A->dEslot[fs] ? 0.0 : A->dEscalar[fs]};
+                d.Q = coef_of(h, c.Q);
+                d.gs = fs < (int)A->gfield.size() ? A->gfield[fs] : nullptr;
+                d.gq = c.Q < (int)A->gfield.size() ? A->gfield[c.Q] : nullptr;
+                A->dests[l].push_back(d);
+            }
+        // transposed couplings: for each source, every (destination, code, w) naming it
+        std::map<int, std::vector<smg::TCoup>> bysrc;
+        for (int j : D)
+            for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q)
+                bysrc[h->coups[q].src].push_back(smg::TCoup{slot_of[j], h->coups[q].code, h->coups[q].w});
+        for (int i : Sset) {
+            smg::AdjSrc s{};
+            s.comp = i;
+            for (int a = 0; a < 3; ++a) s.ext[a] = h->comps[i].ext[a];
+            s.tbeg = (int)A->tcoup[l].size();
+            for (const auto& t : bysrc[i]) A->tcoup[l].push_back(t);
+            s.tend = (int)A->tcoup[l].size();
+            A->srcs[l].push_back(s);
+        }
+        cudaFree(A->d_dests[l]);
+        cudaFree(A->d_srcs[l]);
+        cudaFree(A->d_tcoup[l]);
+        A->d_dests[l] = nullptr;
+        A->d_srcs[l] = nullptr;
+        A->d_tcoup[l] = nullptr;
+        A_CUDA(h, cudaMalloc(&A->d_dests[l], sizeof(smg::AdjDest) * std::max<size_t>(1, A->dests[l].size())));
+        A_CUDA(h, cudaMalloc(&A->d_srcs[l], sizeof(smg::AdjSrc) * std::max<size_t>(1, A->srcs[l].size())));
+        A_CUDA(h, cudaMalloc(&A->d_tcoup[l], sizeof(smg::TCoup) * std::max<size_t>(1, A->tcoup[l].size())));
+        if (!A->dests[l].empty())
+            A_CUDA(h, cudaMemcpyAsync(A->d_dests[l], A->dests[l].data(), sizeof(smg::AdjDest) * A->dests[l].size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+        if (!A->srcs[l].empty())
+            A_CUDA(h, cudaMemcpyAsync(A->d_srcs[l], A->srcs[l].data(), sizeof(smg::AdjSrc) * A->srcs[l].size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+        if (!A->tcoup[l].empty())
+            A_CUDA(h, cudaMemcpyAsync(A->d_tcoup[l], A->tcoup[l].data(), sizeof(smg::TCoup) * A->tcoup[l].size(),
+                                      cudaMemcpyHostToDevice, h->stream));
+    }
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
+void grid_ext(const smg_handle* h, int f, int e[3]) {
+    const int gt = h->field_grid[f];
+    for (int a = 0; a < 3; ++a) {
+        const int d = h->sd[a];
+        const int g = 1 + ((gt >> d) & 1);
+        e[a] = (g == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+    }
+}
+
+}  // namespace
+
+void smg_adjoint_free(smg_handle* h) { free_adj(h); }
+
+extern "C" {
+
+int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
+    if (!h) return SMG_EINVAL;
+    if (nsteps < 1 || ckpt_every < 1) return afail(h, SMG_EINVAL, "smg_forward: nsteps and ckpt_every must be >= 1");
+    if (!h->dt_set || !h->state_set) return afail(h, SMG_ESTATE, "smg_forward: set the state and dt first");
+    if (h->filter_mode == SMG_FILTER_FULL)
+        return afail(h, SMG_EINVAL, "smg_forward: the adjoint supports f_position '' and 'substep'");
+    if (!(h->pair[0].ok && h->pair[1].ok)) return afail(h, SMG_EINVAL, "smg_forward: pair tables unavailable");
+    free_adj(h);
+    AdjData* A = new AdjData();
+    h->adj = A;
+    A->nsteps = nsteps;
+    A->K = std::min<int64_t>(ckpt_every, nsteps);
+    A->nseg = (nsteps + A->K - 1) / A->K;
+    A->maxdest = (int)std::max(h->destA.size(), h->destB.size());
+    const size_t sb = state_bytes(h);
+    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
+    A->ckpt.assign(A->nseg, nullptr);
+    for (auto& p : A->ckpt) A_CUDA(h, cudaMalloc(&p, sb));
+    A_CUDA(h, cudaMalloc(&A->work, sb));
+    A_CUDA(h, cudaMalloc(&A->lam, sb));
+    A_CUDA(h, cudaMalloc(&A->V, vb));
+    A_CUDA(h, cudaMalloc(&A->rec_state, sb * 3 * A->K));
+    A_CUDA(h, cudaMalloc(&A->rec_w, vb * 3 * A->K));
+    A_CUDA(h, cudaMemsetAsync(A->V, 0, vb, h->stream));
+    A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * 3 * A->K, h->stream));
+    A->bytes = sb * (A->nseg + 2 + 3 * A->K) + vb * (1 + 3 * A->K);
+    // gradient slots for sigma and source fields; d(decay)/d(sigma) per sigma field
+    const int nf = (int)h->field_grid.size();
+    A->gfield.assign(nf, nullptr);
+    A->dEslot.assign(nf, nullptr);
+    A->dEscalar.assign(nf, 0.0);
+    std::vector<char> is_sigma(nf, 0), is_q(nf, 0);
+    for (int j = 1; j < h->n_sys; ++j) is_sigma[h->comps[j].sT] = 1;
+    is_sigma[h->sigma_a] = 1;
+    for (int j = 0; j < h->n_sys; ++j)
+        if (h->comps[j].Q != h->field_zero) is_q[h->comps[j].Q] = 1;
+    for (int f = 0; f < nf; ++f) {
+        if (!(is_sigma[f] || is_q[f])) continue;
+        A_CUDA(h, cudaMalloc(&A->gfield[f], (size_t)h->g.cs * sizeof(double)));
+        A_CUDA(h, cudaMemsetAsync(A->gfield[f], 0, (size_t)h->g.cs * sizeof(double), h->stream));
+        A->bytes += (size_t)h->g.cs * sizeof(double);
+        if (!is_sigma[f]) continue;
+        const smg::DevField& F = h->fields_host[f];
+        if (F.p) {
+            A_CUDA(h, cudaMalloc(&A->dEslot[f], (size_t)h->g.cs * sizeof(double)));
+            A->bytes += (size_t)h->g.cs * sizeof(double);
+            smg::k_dphi<<<(unsigned)((h->g.cs + 255) / 256), 256, 0, h->stream>>>(A->dEslot[f], F.p, h->g.cs, h->hdt);
+            A_CUDA(h, cudaGetLastError());
+        } else {
+            A->dEscalar[f] = -h->hdt * smg::dphi(-F.s * h->hdt);
+        }
+    }
+    int rc = build_tables(h);
+    if (rc != SMG_OK) return rc;
+    // forward: checkpoint at the start of every segment, the segment itself as smg_run
+    for (int64_t s = 0; s < A->nseg; ++s) {
+        A_CUDA(h, cudaMemcpyAsync(A->ckpt[s], h->dU, sb, cudaMemcpyDeviceToDevice, h->stream));
+        const int64_t ks = std::min<int64_t>(A->K, nsteps - s * A->K);
+        rc = smg_run(h, ks);
+        if (rc != SMG_OK) return rc;
+    }
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    A->ready = true;
+    A->seeded = false;
+    return SMG_OK;
+}
+
+int smg_misfit(smg_handle* h, const double* obs, double* J) {
+    if (!h || !obs) return SMG_EINVAL;
+    AdjData* A = h->adj;
+    if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_misfit: call smg_forward first");
+    const int* e = h->comps[0].ext;
+    const size_t n = (size_t)e[0] * e[1] * e[2];
+    std::vector<double> u(n), lam0(n);
+    std::vector<double*> all(h->n_sys, nullptr);
+    all[0] = u.data();
+    int rc = smg_get_state(h, all.data());
+    if (rc != SMG_OK) return rc;
+    double sum = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        lam0[i] = u[i] - obs[i];
+        sum += lam0[i] * lam0[i];
+    }
+    if (J) *J = 0.5 * sum;
+    const size_t sb = state_bytes(h);
+    A_CUDA(h, cudaMemsetAsync(A->lam, 0, sb, h->stream));
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(lam0.data(), (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+    p.dstPtr = make_cudaPitchedPtr(A->lam, (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
+    p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+    p.kind = cudaMemcpyHostToDevice;
+    A_CUDA(h, cudaMemcpy3DAsync(&p, h->stream));
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    A->seeded = true;
+    return SMG_OK;
+}
+
+int smg_adjoint_seed(smg_handle* h, const double* const* lam) {
+    if (!h || !lam) return SMG_EINVAL;
+    AdjData* A = h->adj;
+    if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_adjoint_seed: call smg_forward first");
+    A_CUDA(h, cudaMemsetAsync(A->lam, 0, state_bytes(h), h->stream));
+    for (int j = 0; j < h->n_sys; ++j) {
+        if (!lam[j]) continue;
+        const int* e = h->comps[j].ext;
+        cudaMemcpy3DParms p{};
+        p.srcPtr = make_cudaPitchedPtr((void*)lam[j], (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+        p.dstPtr = make_cudaPitchedPtr(A->lam + (size_t)j * h->g.cs, (size_t)h->g.s1 * 8, (size_t)h->g.s1,
+                                       (size_t)h->g.B[1]);
+        p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+        p.kind = cudaMemcpyHostToDevice;
+        A_CUDA(h, cudaMemcpy3DAsync(&p, h->stream));
+    }
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    A->seeded = true;
+    return SMG_OK;
+}
+
+int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fields) {
+    if (!h) return SMG_EINVAL;
+    AdjData* A = h->adj;
+    if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_backward: call smg_forward first");
+    if (!A->seeded) return afail(h, SMG_ESTATE, "smg_backward: seed the adjoint (smg_misfit or smg_adjoint_seed)");
+    const size_t sb = state_bytes(h);
+    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
+    for (double* g : A->gfield)
+        if (g) A_CUDA(h, cudaMemsetAsync(g, 0, (size_t)h->g.cs * sizeof(double), h->stream));
+    const long long npts = h->g.s2 * h->g.B[2];
+    const unsigned nbx = (unsigned)((npts + 255) / 256);
+    const int modes[3] = {0, 1, 0}, kfs[3] = {1, 0, 2};
+    for (int64_t s = A->nseg - 1; s >= 0; --s) {
+        const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
+        A_CUDA(h, cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream));
+        for (int64_t k = 0; k < ks; ++k)
+            for (int ph = 0; ph < 3; ++ph) {
+                const int64_t r = 3 * k + ph;
+                A_CUDA(h, cudaMemcpyAsync((char*)A->rec_state + sb * r, A->work, sb, cudaMemcpyDeviceToDevice,
+                                          h->stream));
+                A_CUDA(h, launch_rec(h, modes[ph], kfs[ph], A->work, (double*)((char*)A->rec_w + vb * r)));
+            }
+        for (int64_t k = ks - 1; k >= 0; --k)
+            for (int ph = 2; ph >= 0; --ph) {
+                const int64_t r = 3 * k + ph;
+                const int l = modes[ph] == 1 ? 1 : 0;
+                const double* pre = (const double*)((const char*)A->rec_state + sb * r);
+                const double* W = (const double*)((const char*)A->rec_w + vb * r);
+                // phase A with filter k=2 uses F2 as its (single) filter
+                if (!A->dests[l].empty()) {
+                    const dim3 g1(nbx, (unsigned)(l == 0 ? A->dests[0].size() / 2 : A->dests[1].size()));
+                    if (l == 1) {
+                        smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[1], pre, W, A->lam, A->V, h->hdt);
+                    } else if (kfs[ph] == 1) {
+                        smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0], pre, W, A->lam, A->V, h->hdt);
+                    } else {
+                        smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + A->dests[0].size() / 2,
+                                                                       pre, W, A->lam, A->V, h->hdt);
+                    }
+                    A_CUDA(h, cudaGetLastError());
+                }
+                if (!A->srcs[l].empty()) {
+                    const dim3 g2(nbx, (unsigned)A->srcs[l].size());
+                    smg::k_adj_transpose<<<g2, 256, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], A->V, A->lam);
+                    A_CUDA(h, cudaGetLastError());
+                }
+            }
+    }
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (grad_U0) {
+        for (int j = 0; j < h->n_sys; ++j) {
+            if (!grad_U0[j]) continue;
+            const int* e = h->comps[j].ext;
+            cudaMemcpy3DParms p{};
+            p.srcPtr = make_cudaPitchedPtr(A->lam + (size_t)j * h->g.cs, (size_t)h->g.s1 * 8, (size_t)h->g.s1,
+                                           (size_t)h->g.B[1]);
+            p.dstPtr = make_cudaPitchedPtr(grad_U0[j], (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+            p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+            p.kind = cudaMemcpyDeviceToHost;
+            A_CUDA(h, cudaMemcpy3DAsync(&p, h->stream));
+        }
+    }
+    if (grad_fields) {
+        const int nf = h->field_one;   // user fields only
+        std::vector<double> tmp((size_t)h->g.cs);
+        for (int f = 0; f < nf; ++f) {
+            if (!grad_fields[f]) continue;
+            if (!A->gfield[f]) {
+                int e[3];
+                grid_ext(h, f, e);
+                const size_t n = h->fields_host[f].p ? (size_t)e[0] * e[1] * e[2] : 1;
+                std::fill(grad_fields[f], grad_fields[f] + n, 0.0);
+                continue;
+            }
+            if (h->fields_host[f].p) {
+                int e[3];
+                grid_ext(h, f, e);
+                cudaMemcpy3DParms p{};
+                p.srcPtr = make_cudaPitchedPtr(A->gfield[f], (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
+                p.dstPtr = make_cudaPitchedPtr(grad_fields[f], (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
+                p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
+                p.kind = cudaMemcpyDeviceToHost;
+                A_CUDA(h, cudaMemcpy3DAsync(&p, h->stream));
+            } else {
+                // scalar coefficient: the derivative is the sum over every point it acts on
+                A_CUDA(h, cudaMemcpyAsync(tmp.data(), A->gfield[f], tmp.size() * sizeof(double),
+                                          cudaMemcpyDeviceToHost, h->stream));
+                A_CUDA(h, cudaStreamSynchronize(h->stream));
+                double sum = 0.0;
+                for (double v : tmp) sum += v;
+                grad_fields[f][0] = sum;
+            }
+        }
+    }
+    A_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
+int smg_adjoint_bytes(const smg_handle* h, int64_t* bytes) {
+    if (!h || !bytes) return SMG_EINVAL;
+    *bytes = h->adj ? (int64_t)h->adj->bytes : 0;
+    return SMG_OK;
+}
+
+}  // extern "C"

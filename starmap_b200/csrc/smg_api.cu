@@ -63,6 +63,7 @@ void resolve_pair(smg_handle* h, int phase);
 cudaError_t upload_pair(smg_handle* h, int phase, bool alloc);
 
 void free_device(smg_handle* h) {
+    smg_adjoint_free(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
     cudaFree(h->dU);

@@ -152,6 +152,7 @@ struct PairArgs {
     double rh[3];
     int exact_recip[3];
     int filter_substep;
+    double* wrec;      // adjoint recording: W of destination di stored at wrec + di*cs (or nullptr)
 };
 
 // (a - b) / h correctly rounded.  When exact_recip is set the quotient is

@@ -9,6 +9,10 @@
 
 #include "smg_device.cuh"
 
+namespace smg {
+struct AdjData;
+}
+
 struct smg_handle {
     // problem
     int n_sys = 0;
@@ -79,7 +83,10 @@ struct smg_handle {
     int exact_recip[3] = {0, 0, 0};
     int nxs = 0;                     // 32-point strips per row
     bool strip_staged = false;       // stage slot-job loads with cp.async
+    smg::AdjData* adj = nullptr;     // adjoint checkpoints and buffers (smg_forward)
 };
+
+void smg_adjoint_free(smg_handle* h);   // smg_adjoint.cu
 
 namespace smg {
 // kernels (smg_phase.cu)

@@ -192,6 +192,11 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
             }
         }
         const double WA = -SA, WB = -SB;
+        if (a.wrec) {   // adjoint recording of the coupling sum (rare path)
+            double* wp = a.wrec + (long long)di * a.g.cs + pt;
+            wp[0] = WA;
+            if (v1) wp[1] = WB;
+        }
         if (MODE == 0) {
             u0 = upd(u0, WA, q0, s0, E0, a.hdt);
             u1 = upd(u1, WB, q1, s1, E1, a.hdt);

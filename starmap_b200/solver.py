@@ -158,6 +158,48 @@ class GpuSolver:
         check(self._L.smg_layout(self.h, _lib.C.byref(b), d), self.h)
         return b.value, list(d)
 
+    # -- discrete adjoint (smg_forward / smg_misfit / smg_backward) -----------
+    def forward(self, nsteps, ckpt_every):
+        check(self._L.smg_forward(self.h, int(nsteps), int(ckpt_every)), self.h)
+
+    def misfit(self, obs):
+        arr = np.ascontiguousarray(np.asfortranarray(
+            np.broadcast_to(np.asarray(obs, dtype=np.float64), self.extents(0))).ravel(order="F"))
+        J = _lib.C.c_double()
+        check(self._L.smg_misfit(self.h, dptr(arr), _lib.C.byref(J)), self.h)
+        return J.value
+
+    def adjoint_seed(self, lam):
+        arrs = []
+        ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
+        for j in range(self.n_sys):
+            if lam[j] is None:
+                continue
+            a = np.ascontiguousarray(np.asfortranarray(
+                np.broadcast_to(np.asarray(lam[j], dtype=np.float64), self.extents(j))).ravel(order="F"))
+            arrs.append(a)
+            ptrs[j] = dptr(a)
+        check(self._L.smg_adjoint_seed(self.h, ptrs), self.h)
+
+    def backward(self, fields=()):
+        """dJ/dU(0) per component and dJ/d(field) for the requested field indices."""
+        gu = {}
+        pu = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
+        for j in range(self.n_sys):
+            e = self.extents(j)
+            gu[j] = (np.empty(int(np.prod(e))), e)
+            pu[j] = dptr(gu[j][0])
+        nf = len(self.field_grids)
+        pf = (_lib.C.POINTER(_lib.C.c_double) * max(nf, 1))()
+        gf = {}
+        for k in fields:
+            gf[k] = np.empty(int(np.prod(self.grid_extents(self.field_grids[k]))))
+            pf[k] = dptr(gf[k])
+        check(self._L.smg_backward(self.h, pu, pf), self.h)
+        gradU = {j: b.reshape(e, order="F") for j, (b, e) in gu.items()}
+        gradF = {k: v.reshape(self.grid_extents(self.field_grids[k]), order="F") for k, v in gf.items()}
+        return gradU, gradF
+
     def state_sumsq(self):
         out = np.zeros(self.n_sys)
         check(self._L.smg_state_sumsq(self.h, dptr(out)), self.h)

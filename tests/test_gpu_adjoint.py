@@ -1,0 +1,145 @@
+"""Discrete adjoint: dot-product test (linear part), central finite
+differences for the sigma, source and initial-condition gradients, and the
+checkpoint length not changing the result."""
+import numpy as np
+import pytest
+
+from starmap_b200 import configs, starmap_init
+from starmap_b200.batch import _tables
+from starmap_b200.solver import GpuSolver, expm1div, first_step, handle_tables, prepare
+
+pytestmark = pytest.mark.gpu
+
+
+def adjoint_problem(n=12, N=3, bc=1, with_source=True, substep=True):
+    def sig_a(x, y):
+        return 0.3 + 0.2 * np.sin(2 * x) * np.cos(y)
+
+    prob = dict(name="adj", closure="P", n_mom=N, ax=[-1.0, 1.0, -1.0, 1.0], n=[n, n + 2], bc=[bc, bc],
+                ic=lambda x, y: np.exp(-8 * (x ** 2 + (y - 0.1) ** 2)), sigma_a=sig_a,
+                sigma_s0=lambda x, y: 0.8 + 0.1 * x, tfinal=1e9, t_plot=[0, 1e9], quiet=True)
+    if with_source:
+        prob["source"] = lambda x, y: np.exp(-6 * ((x - 0.3) ** 2 + y ** 2))
+    if substep:
+        prob.update(filterfunction=configs.exp_filter(2, 3.0), f_position="substep")
+    par = starmap_init(prob)
+    S = prepare(par)
+    fs = first_step(S)
+    return S, fs
+
+
+def make_solver(S, fs, T=None):
+    T = T or _tables(S, fs)
+    return GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T)), T
+
+
+def run_J(S, fs, T, U0, nsteps, obs):
+    solver, _ = make_solver(S, fs, T)
+    try:
+        solver.set_state(U0)
+        solver.set_dt(fs["dt"])
+        solver.run(nsteps)
+        u = solver.get_state([0])[0]
+    finally:
+        solver.close()
+    return 0.5 * np.sum((u - obs) ** 2)
+
+
+def with_sigma(T, S, fs, key, arr):
+    """Field table with sigma field `key` replaced by arr and its decay recomputed."""
+    import copy
+    T2 = copy.copy(T)
+    T2.fields = list(T.fields)
+    k = T.index[key]
+    T2.fields[k] = (arr, T.fields[k][1])
+    dkey = ("EA",) if key == ("sA",) else ("ET",) + key[1:]
+    kd = T.index[dkey]
+    T2.fields[kd] = (expm1div(-arr * fs["dt"] / 2), T.fields[kd][1])
+    return T2
+
+
+def test_dot_product():
+    S, fs = adjoint_problem(with_source=False)
+    rng = np.random.default_rng(0)
+    nsteps = 9
+    solver, T = make_solver(S, fs)
+    try:
+        delta = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
+        mu = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
+        solver.set_state(delta)
+        solver.set_dt(fs["dt"])
+        solver.forward(nsteps, 4)
+        Ad = solver.get_state()
+        solver.adjoint_seed(mu)
+        lam0, _ = solver.backward()
+    finally:
+        solver.close()
+    lhs = sum(np.sum(Ad[j] * mu[j]) for j in range(S.n_sys))
+    rhs = sum(np.sum(delta[j] * lam0[j]) for j in range(S.n_sys))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
+
+
+@pytest.mark.parametrize("bc,substep", [(1, True), (0, False)])
+def test_sigma_source_ic_gradients_vs_central_differences(bc, substep):
+    S, fs = adjoint_problem(bc=bc, substep=substep)
+    nsteps = 8
+    solver, T = make_solver(S, fs)
+    obs = None
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.forward(nsteps, 3)
+        u = solver.get_state([0])[0]
+        obs = 0.5 * u + 0.01
+        J0 = solver.misfit(obs)
+        keys = [k for k in T.index if k[0] in ("sT", "sA", "Q")]
+        gU, gF = solver.backward(fields=[T.index[k] for k in keys])
+    finally:
+        solver.close()
+    assert np.isclose(J0, run_J(S, fs, T, S.U0, nsteps, obs), rtol=1e-14)
+    rng = np.random.default_rng(1)
+    for key in keys:
+        k = T.index[key]
+        base = np.asarray(T.fields[k][0], dtype=np.float64)
+        d = rng.standard_normal(base.shape)
+        eps = 1e-6 * max(1.0, float(np.abs(base).max()))
+        if key[0] == "Q":
+            import copy
+            Tp, Tm = copy.copy(T), copy.copy(T)
+            Tp.fields, Tm.fields = list(T.fields), list(T.fields)
+            Tp.fields[k] = (base + eps * d, T.fields[k][1])
+            Tm.fields[k] = (base - eps * d, T.fields[k][1])
+        else:
+            Tp = with_sigma(T, S, fs, key, base + eps * d)
+            Tm = with_sigma(T, S, fs, key, base - eps * d)
+        fd = (run_J(S, fs, Tp, S.U0, nsteps, obs) - run_J(S, fs, Tm, S.U0, nsteps, obs)) / (2 * eps)
+        ad = float(np.sum(gF[k] * d))
+        assert abs(fd - ad) <= 1e-6 * max(abs(fd), 1e-3 * abs(J0)), (key, fd, ad)
+    # initial condition, all components
+    d = [rng.standard_normal(np.shape(S.U0[j])) for j in range(S.n_sys)]
+    eps = 1e-6
+    Up = [S.U0[j] + eps * d[j] for j in range(S.n_sys)]
+    Um = [S.U0[j] - eps * d[j] for j in range(S.n_sys)]
+    fd = (run_J(S, fs, T, Up, nsteps, obs) - run_J(S, fs, T, Um, nsteps, obs)) / (2 * eps)
+    ad = sum(float(np.sum(gU[j] * d[j].reshape(gU[j].shape))) for j in range(S.n_sys))
+    assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
+
+
+def test_checkpoint_interval_does_not_change_gradient():
+    S, fs = adjoint_problem(n=10, N=5)
+    res = []
+    for K in (1, 4, 11):
+        solver, T = make_solver(S, fs)
+        try:
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.forward(11, K)
+            u = solver.get_state([0])[0]
+            solver.misfit(0.9 * u)
+            gU, gF = solver.backward(fields=[T.index[("sA",)]])
+            res.append((gU, gF))
+        finally:
+            solver.close()
+    for gU, gF in res[1:]:
+        for j in gU:
+            np.testing.assert_allclose(gU[j], res[0][0][j], rtol=0, atol=1e-12 * np.abs(res[0][0][j]).max())
