@@ -210,6 +210,61 @@ def bench_batch(steps: int = 200):
             "batched_over_plain_loop": batched / loop}
 
 
+def bench_adjoint(nsteps: int = 400, ckpt: int = 20, n: int = 200):
+    """Misfit gradient w.r.t. sigma_a on the 2D P15 inverse problem: forward with
+    checkpoints, backward with recompute, their time ratio, and a central
+    finite-difference check of the sigma_a gradient along a random smooth
+    direction."""
+    from starmap_b200 import configs, starmap_init
+    from starmap_b200.adjoint import MisfitAdjoint
+    from starmap_b200.solver import setup_gpu
+
+    def run_u0(par, steps):
+        S, fs, sv, T = setup_gpu(par)
+        try:
+            sv.set_state(S.U0)
+            sv.set_dt(fs["dt"])
+            sv.run(steps)
+            sv.sync()
+            ms = sv.last_run_stats()[0]
+            return sv.get_state([0])[0], ms
+        finally:
+            sv.close()
+
+    obs, _ = run_u0(starmap_init(configs.adjoint_problem(n=n, sigma_a_field=configs.true_sigma_a)), nsteps)
+    par = starmap_init(configs.adjoint_problem(n=n))
+    _, plain_ms = run_u0(par, nsteps)
+    adj = MisfitAdjoint(par, ckpt_every=ckpt)
+    t0 = time.perf_counter()
+    J = adj.forward(obs, nsteps)
+    t1 = time.perf_counter()
+    g = adj.backward()
+    t2 = time.perf_counter()
+    adj_bytes = 0
+    adj.close()
+    # directional derivative along a smooth direction, sampled like sigma_a itself
+    def bump(x, y):
+        return np.sin(1.3 * x + 0.4) * np.cos(0.9 * y - 0.2)
+    eps = 1e-6
+
+    def J_of(scale):
+        p = starmap_init(configs.adjoint_problem(n=n, sigma_a_field=lambda x, y: 0.1 + scale * bump(x, y)))
+        u, _ = run_u0(p, nsteps)
+        return 0.5 * float(np.sum((u - obs) ** 2))
+    fd = (J_of(eps) - J_of(-eps)) / (2 * eps)
+    S = MisfitAdjoint.__new__(MisfitAdjoint)
+    from starmap_b200.solver import prepare
+    Sx = prepare(par)
+    ad = 0.0
+    for grid, gv in g["sigma_a"].items():
+        X, Y, Z = Sx.XYZ(grid)
+        ad += float(np.sum(gv * bump(Y, Z).reshape(np.shape(gv), order="F")))
+    return {"nsteps": nsteps, "ckpt_every": ckpt, "grid": [n, n], "n_sys": Sx.n_sys, "J": J,
+            "forward_s": t1 - t0, "backward_s": t2 - t1, "backward_over_forward": (t2 - t1) / (t1 - t0),
+            "plain_forward_s": plain_ms / 1e3, "backward_over_plain_forward": (t2 - t1) / (plain_ms / 1e3),
+            "fd_directional": fd, "adjoint_directional": ad, "fd_rel_err": abs(fd - ad) / abs(fd)}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -254,6 +309,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline stepping")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of reference-arm stepping")
     args = ap.parse_args()
@@ -342,6 +398,8 @@ def main():
         line["e2e"] = e2e
     if world == 1 and not args.no_batch:
         line["batched"] = bench_batch()
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = bench_adjoint()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         steps, secs = cpu_sample(par, budget_s=args.cpu_budget, nthreads=threads, warm=0)

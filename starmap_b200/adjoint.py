@@ -1,0 +1,78 @@
+"""Gradients of an L2 misfit on the zeroth moment through the GPU time loop.
+
+``MisfitAdjoint`` is a forward/backward pair in the shape of an autograd
+function, without a tensor framework (the reference's host is MATLAB/Octave):
+
+    adj = MisfitAdjoint(par, ckpt_every=20)
+    J = adj.forward(obs, nsteps)      # J = 1/2 sum (U_1(T) - obs)^2
+    g = adj.backward()                # dict of gradients
+    adj.close()
+
+``g["sigma_a"][grid]`` and ``g["sigma_s0"][grid]`` are the derivatives with
+respect to the coefficient samples on each staggered grid ``grid`` (the
+reference samples sigma_a and sigma_s0 separately on every grid type,
+starmap_solver.m:215-243; a user field defined on the domain gets its gradient
+by summing these through its own sampling), ``g["source"][j]`` for every
+component with a source, ``g["ic"][j]`` for every component, ``g["J"]`` the
+misfit.  Scalar coefficients get scalar derivatives.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .batch import _tables
+from .solver import GpuSolver, first_step, handle_tables, prepare
+
+__all__ = ["MisfitAdjoint"]
+
+
+class MisfitAdjoint:
+    def __init__(self, par: dict, ckpt_every: int = 20):
+        S = prepare(par)
+        if S.time_dependent.any() or S.src_td or S.filter_td:
+            raise NotImplementedError("the adjoint covers autonomous problems")
+        self.S = S
+        self.fs = first_step(S)
+        self.T = _tables(S, self.fs)
+        self.solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, self.T.fields,
+                                **handle_tables(S, self.T))
+        self.ckpt_every = int(ckpt_every)
+        self.J = None
+
+    def forward(self, obs, nsteps: int, U0=None) -> float:
+        s = self.solver
+        s.set_state(self.S.U0 if U0 is None else U0)
+        s.set_dt(self.fs["dt"])
+        s.forward(int(nsteps), self.ckpt_every)
+        self.J = s.misfit(obs)
+        return self.J
+
+    def backward(self) -> dict:
+        S, T = self.S, self.T
+        keys = [k for k in T.index if k[0] in ("sT", "sA", "Q")]
+        gU, gF = self.solver.backward(fields=[T.index[k] for k in keys])
+        sig_a, sig_s0 = {}, {}
+
+        def add(d, g, v):
+            d[g] = d[g] + v if g in d else np.array(v, dtype=np.float64)
+
+        for key in keys:
+            v = gF[T.index[key]]
+            if key[0] == "sT":   # sT{g,m} = sA{g} + sS0{g} - sSm{g,m}
+                g = key[1:4]
+                add(sig_a, g, v)
+                add(sig_s0, g, v)
+            elif key[0] == "sA":  # sA1 = sA{1,1,1} drives the zeroth moment
+                add(sig_a, (1, 1, 1), v)
+        src = {key[1]: gF[T.index[key]] for key in keys if key[0] == "Q"}
+        return {"J": self.J, "sigma_a": sig_a, "sigma_s0": sig_s0, "source": src,
+                "ic": [gU[j] for j in range(S.n_sys)]}
+
+    def close(self):
+        self.solver.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

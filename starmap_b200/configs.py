@@ -138,3 +138,25 @@ def batched_sweep(n_inst=256, seed=20261203, edges=tuple(range(64, 257, 32)), or
                           bc=[0, 0], ic=gaussian(cx, cy, std), sigma_a=block_field(sa), sigma_s0=block_field(ss),
                           t_plot=[0.0, 1e9], tfinal=1e9, quiet=True))
     return probs
+
+
+def adjoint_problem(n=200, n_mom=15, sigma_a_field=None):
+    """2D P15 inverse-problem setting: [-1.5,1.5]^2, periodic, sigma_s0 = 1,
+    normalised Gaussian initial condition with std 0.05, dt = 0.5 h.
+    ``sigma_a_field(x, y)`` defaults to the constant 0.1 returned as an array
+    (so that its gradient is a field); :func:`true_sigma_a` is the field that
+    generates the observations."""
+    ax = [-1.5, 1.5, -1.5, 1.5]
+    h = 3.0 / n
+    sa = sigma_a_field or (lambda x, y: 0.1 + 0.0 * x)
+    std = 0.05
+    return dict(name="Adjoint", closure="P", n_mom=n_mom, ax=ax, n=[n, n], bc=[0, 0],
+                ic=lambda x, y: np.exp(-(x ** 2 + y ** 2) / (2 * std ** 2)) / (2 * np.pi * std ** 2),
+                sigma_a=sa, sigma_s0=lambda x, y: 1.0, t_plot=[0.0, 1e9], tfinal=1e9,
+                cn=cn_for_dt("P", n_mom, 2, [h, h], 0.5 * h), quiet=True)
+
+
+def true_sigma_a(x, y):
+    """0.1 plus two Gaussian bumps of amplitude 1 and std 0.2 at (+-0.5, 0)."""
+    return 0.1 + np.exp(-((x - 0.5) ** 2 + y ** 2) / (2 * 0.2 ** 2)) + \
+        np.exp(-((x + 0.5) ** 2 + y ** 2) / (2 * 0.2 ** 2))

@@ -66,8 +66,8 @@ struct AdjData {
     double* work = nullptr;
     double* lam = nullptr;
     double* V = nullptr;
-    double* rec_state = nullptr;   // [3K][n_sys*cs]
-    double* rec_w = nullptr;       // [3K][maxdest*cs]
+    double* rec_state = nullptr;   // [2K+1][maxdest*cs]: destination values before each phase
+    double* rec_w = nullptr;       // [2K+1][maxdest*cs]: destination coupling sums
     int maxdest = 0;
     std::vector<double*> gfield;   // per user field: gradient slot (cs) or nullptr
     std::vector<double*> dEslot;   // per sigma field: d(decay)/d(sigma) slot (arrays)
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) k_adj_point(DevGrid g, const AdjDest* des
     if (x >= d.ext[0] || y >= d.ext[1] || z >= d.ext[2]) return;
     const long long jo = (long long)d.comp * g.cs + pt;
     const double lp = lam[jo];
-    const double u = pre[jo];
+    const double u = pre[(long long)di * g.cs + pt];
     const double w = W[(long long)di * g.cs + pt];
     const double s = cval(d.sg, pt), E = cval(d.E, pt), dE = cval(d.dE, pt), q = cval(d.Q, pt);
     const double F1 = cval(d.F1, pt);
@@ -204,6 +204,73 @@ __global__ void __launch_bounds__(256) k_adj_transpose(DevGrid g, const AdjSrc* 
     lam[(long long)S.comp * g.cs + pt] -= acc;
 }
 
+// Row form of dT for axes 1/2: both points of a pair share q, so every
+// preimage is a row offset and one 128-bit load serves both points.
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ double2 sub2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+__device__ __forceinline__ double2 dT_row(const double* v, int q, int n, int bc, int g2, long long st) {
+    const double2 z = make_double2(0.0, 0.0);
+    if (!g2) {
+        if (bc) {
+            double2 a = ld2(v);
+            if (q == n - 1) a = add2(a, ld2(v + st));
+            double2 b = ld2(v + st);
+            if (q == 0) b = add2(b, ld2(v));
+            return sub2(a, b);
+        }
+        const long long om = (q == 0) ? (long long)(n - 1) * st : -st;
+        return sub2(ld2(v + om), ld2(v));
+    }
+    if (bc) {
+        const double2 a = q >= 1 ? ld2(v - st) : z;
+        const double2 b = q <= n - 1 ? ld2(v) : z;
+        return sub2(a, b);
+    }
+    const long long op = (q == n - 1) ? -(long long)(n - 1) * st : st;
+    return sub2(ld2(v), ld2(v + op));
+}
+
+// Two adjacent points per thread (x = 2t, 2t+1): 128-bit loads for the y/z
+// preimages, per-point loads for x.
+__global__ void __launch_bounds__(128) k_adj_transpose2(DevGrid g, const AdjSrc* srcs, const TCoup* tc,
+                                                        const double* __restrict__ V, double* lam) {
+    const int tpr = (g.B[0] + 1) / 2;
+    const long long rows = (long long)g.B[1] * g.B[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int si = blockIdx.y;
+    if (t >= (long long)tpr * rows) return;
+    const int x0 = 2 * (int)(t % tpr);
+    const long long row = t / tpr;
+    const int y = (int)(row % g.B[1]);
+    const int z = (int)(row / g.B[1]);
+    const AdjSrc S = srcs[si];
+    if (x0 >= S.ext[0] || y >= S.ext[1] || z >= S.ext[2]) return;
+    const bool v1 = x0 + 1 < S.ext[0];
+    const long long pt = (long long)z * g.s2 + (long long)y * g.s1 + x0;
+    double a0 = 0.0, a1 = 0.0;
+    for (int c = S.tbeg; c < S.tend; ++c) {
+        const TCoup tcp = tc[c];
+        const int ax = tcp.code >> 1, g2 = tcp.code & 1;
+        const double* v = V + (long long)tcp.vslot * g.cs + pt;
+        const double f = tcp.w / g.h[ax];
+        if (ax == 0) {
+            a0 += f * dT(v, x0, g.n[0], g.bc[0], g2, 1);
+            if (v1) a1 += f * dT(v + 1, x0 + 1, g.n[0], g.bc[0], g2, 1);
+        } else {
+            const int q = ax == 1 ? y : z;
+            const long long st = ax == 1 ? g.s1 : g.s2;
+            const double2 d = dT_row(v, q, g.n[ax], g.bc[ax], g2, st);
+            a0 += f * d.x;
+            a1 += f * d.y;
+        }
+    }
+    double* L = lam + (long long)S.comp * g.cs + pt;
+    L[0] -= a0;
+    if (v1) L[1] -= a1;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256, 4) k_pair_rec(PairArgs a, int kf) {
     const int bid = blockIdx.x;
@@ -236,7 +303,7 @@ int acuda(smg_handle* h, cudaError_t e, const char* what) {
 size_t state_bytes(const smg_handle* h) { return (size_t)h->g.cs * h->n_sys * sizeof(double); }
 
 // pair-kernel arguments of one phase on an arbitrary state buffer
-smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec) {
+smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec, double* prec) {
     smg::PairArgs a{};
     const auto& P = h->pair[phase];
     a.g = h->g;
@@ -256,15 +323,17 @@ smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec) 
     }
     a.filter_substep = h->filter_mode == SMG_FILTER_SUBSTEP;
     a.wrec = wrec;
+    a.prec = prec;
     return a;
 }
 
-cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec) {
+cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec) {
     const int phase = mode == 1 ? 1 : 0;
-    const smg::PairArgs a = rec_args(h, phase, U, wrec);
+    const smg::PairArgs a = rec_args(h, phase, U, wrec, prec);
     if (a.ndest == 0) return cudaSuccess;
     const unsigned nb = (unsigned)((long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2]);
     if (mode == 1) smg::k_pair_rec<1><<<nb, 64, 0, h->stream>>>(a, kf);
+    else if (mode == 2) smg::k_pair_rec<2><<<nb, 64, 0, h->stream>>>(a, kf);
     else smg::k_pair_rec<0><<<nb, 64, 0, h->stream>>>(a, kf);
     return cudaGetLastError();
 }
@@ -308,8 +377,10 @@ int build_tables(smg_handle* h) {
         A->srcs[l].clear();
         A->tcoup[l].clear();
         std::map<int, int> slot_of;
-        // phase A has two tables: filter k=1 and filter k=2 as the single filter
-        for (int rep = 0; rep < (l == 0 ? 2 : 1); ++rep)
+        // phase A has three tables: single substep with filter k=1, single
+        // substep with filter k=2, and the fused pair A(k=2) A(k=1) as a
+        // two-substep phase (filters in that order)
+        for (int rep = 0; rep < (l == 0 ? 3 : 1); ++rep)
             for (int k = 0; k < (int)D.size(); ++k) {
                 const int j = D[k];
                 slot_of[j] = k;
@@ -326,7 +397,7 @@ int build_tables(smg_handle* h) {
                     fs = c.sT;
                     fe = c.ET;
                     d.F1 = coef_of(h, rep == 0 ? c.F1 : c.F2);
-                    d.F2 = coef_of(h, c.F2);
+                    d.F2 = coef_of(h, rep == 2 ? c.F1 : c.F2);
                 }
                 d.sg = coef_of(h, fs);
                 d.E = coef_of(h, fe);
@@ -395,25 +466,37 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     if (h->filter_mode == SMG_FILTER_FULL)
         return afail(h, SMG_EINVAL, "smg_forward: the adjoint supports f_position '' and 'substep'");
     if (!(h->pair[0].ok && h->pair[1].ok)) return afail(h, SMG_EINVAL, "smg_forward: pair tables unavailable");
-    free_adj(h);
-    AdjData* A = new AdjData();
-    h->adj = A;
-    A->nsteps = nsteps;
-    A->K = std::min<int64_t>(ckpt_every, nsteps);
-    A->nseg = (nsteps + A->K - 1) / A->K;
-    A->maxdest = (int)std::max(h->destA.size(), h->destB.size());
+    const int64_t K = std::min<int64_t>(ckpt_every, nsteps);
+    const int64_t nseg = (nsteps + K - 1) / K;
+    AdjData* A = h->adj;
     const size_t sb = state_bytes(h);
-    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
-    A->ckpt.assign(A->nseg, nullptr);
-    for (auto& p : A->ckpt) A_CUDA(h, cudaMalloc(&p, sb));
-    A_CUDA(h, cudaMalloc(&A->work, sb));
-    A_CUDA(h, cudaMalloc(&A->lam, sb));
-    A_CUDA(h, cudaMalloc(&A->V, vb));
-    A_CUDA(h, cudaMalloc(&A->rec_state, sb * 3 * A->K));
-    A_CUDA(h, cudaMalloc(&A->rec_w, vb * 3 * A->K));
-    A_CUDA(h, cudaMemsetAsync(A->V, 0, vb, h->stream));
-    A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * 3 * A->K, h->stream));
-    A->bytes = sb * (A->nseg + 2 + 3 * A->K) + vb * (1 + 3 * A->K);
+    const int maxdest = (int)std::max(h->destA.size(), h->destB.size());
+    const size_t vb = (size_t)h->g.cs * std::max(maxdest, 1) * sizeof(double);
+    if (!A || A->K != K || A->nseg != nseg) {
+        // (re)allocate: checkpoints, work/adjoint/scratch states and the
+        // recording of one segment (2K+1 phases); kept for later calls
+        free_adj(h);
+        A = new AdjData();
+        h->adj = A;
+        A->K = K;
+        A->nseg = nseg;
+        A->maxdest = maxdest;
+        A->ckpt.assign(nseg, nullptr);
+        for (auto& p : A->ckpt) A_CUDA(h, cudaMalloc(&p, sb));
+        A_CUDA(h, cudaMalloc(&A->work, sb));
+        A_CUDA(h, cudaMalloc(&A->lam, sb));
+        A_CUDA(h, cudaMalloc(&A->V, vb));
+        A_CUDA(h, cudaMalloc(&A->rec_state, vb * (2 * K + 1)));
+        A_CUDA(h, cudaMalloc(&A->rec_w, vb * (2 * K + 1)));
+        A_CUDA(h, cudaMemsetAsync(A->V, 0, vb, h->stream));
+        A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * (2 * K + 1), h->stream));
+        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
+    } else {
+        for (double* p : A->gfield) cudaFree(p);
+        for (double* p : A->dEslot) cudaFree(p);
+        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
+    }
+    A->nsteps = nsteps;
     // gradient slots for sigma and source fields; d(decay)/d(sigma) per sigma field
     const int nf = (int)h->field_grid.size();
     A->gfield.assign(nf, nullptr);
@@ -517,42 +600,51 @@ int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fiel
         if (g) A_CUDA(h, cudaMemsetAsync(g, 0, (size_t)h->g.cs * sizeof(double), h->stream));
     const long long npts = h->g.s2 * h->g.B[2];
     const unsigned nbx = (unsigned)((npts + 255) / 256);
-    const int modes[3] = {0, 1, 0}, kfs[3] = {1, 0, 2};
+    const int tpr = (h->g.B[0] + 1) / 2;
+    const unsigned nbp = (unsigned)(((long long)tpr * h->g.B[1] * h->g.B[2] + 127) / 128);
+    const size_t nA = A->dests[0].size() / 3;
     for (int64_t s = A->nseg - 1; s >= 0; --s) {
         const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
+        // the segment's phases as smg_run performs them: A(k=1), then per step
+        // B and the fused A(k=2)A(k=1) -- A(k=2) alone after the last step
+        std::vector<int> kind;   // 0: A k=1, 1: B, 2: fused A-A, 3: A k=2
+        kind.push_back(0);
+        for (int64_t k = 0; k < ks; ++k) {
+            kind.push_back(1);
+            kind.push_back(k + 1 < ks ? 2 : 3);
+        }
         A_CUDA(h, cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream));
-        for (int64_t k = 0; k < ks; ++k)
-            for (int ph = 0; ph < 3; ++ph) {
-                const int64_t r = 3 * k + ph;
-                A_CUDA(h, cudaMemcpyAsync((char*)A->rec_state + sb * r, A->work, sb, cudaMemcpyDeviceToDevice,
-                                          h->stream));
-                A_CUDA(h, launch_rec(h, modes[ph], kfs[ph], A->work, (double*)((char*)A->rec_w + vb * r)));
+        for (size_t r = 0; r < kind.size(); ++r) {
+            const int mode = kind[r] == 1 ? 1 : (kind[r] == 2 ? 2 : 0);
+            const int kf = kind[r] == 3 ? 2 : 1;
+            A_CUDA(h, launch_rec(h, mode, kf, A->work, (double*)((char*)A->rec_w + vb * r),
+                                 (double*)((char*)A->rec_state + vb * r)));
+        }
+        for (int64_t r = (int64_t)kind.size() - 1; r >= 0; --r) {
+            const int l = kind[r] == 1 ? 1 : 0;
+            const double* pre = (const double*)((const char*)A->rec_state + vb * r);
+            const double* W = (const double*)((const char*)A->rec_w + vb * r);
+            if (l == 1 && !A->dests[1].empty()) {
+                const dim3 g1(nbx, (unsigned)A->dests[1].size());
+                smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[1], pre, W, A->lam, A->V, h->hdt);
+            } else if (l == 0 && nA) {
+                const dim3 g1(nbx, (unsigned)nA);
+                if (kind[r] == 0)
+                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0], pre, W, A->lam, A->V, h->hdt);
+                else if (kind[r] == 3)
+                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + nA, pre, W, A->lam, A->V,
+                                                                   h->hdt);
+                else
+                    smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + 2 * nA, pre, W, A->lam, A->V,
+                                                                   h->hdt);
             }
-        for (int64_t k = ks - 1; k >= 0; --k)
-            for (int ph = 2; ph >= 0; --ph) {
-                const int64_t r = 3 * k + ph;
-                const int l = modes[ph] == 1 ? 1 : 0;
-                const double* pre = (const double*)((const char*)A->rec_state + sb * r);
-                const double* W = (const double*)((const char*)A->rec_w + vb * r);
-                // phase A with filter k=2 uses F2 as its (single) filter
-                if (!A->dests[l].empty()) {
-                    const dim3 g1(nbx, (unsigned)(l == 0 ? A->dests[0].size() / 2 : A->dests[1].size()));
-                    if (l == 1) {
-                        smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[1], pre, W, A->lam, A->V, h->hdt);
-                    } else if (kfs[ph] == 1) {
-                        smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0], pre, W, A->lam, A->V, h->hdt);
-                    } else {
-                        smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + A->dests[0].size() / 2,
-                                                                       pre, W, A->lam, A->V, h->hdt);
-                    }
-                    A_CUDA(h, cudaGetLastError());
-                }
-                if (!A->srcs[l].empty()) {
-                    const dim3 g2(nbx, (unsigned)A->srcs[l].size());
-                    smg::k_adj_transpose<<<g2, 256, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], A->V, A->lam);
-                    A_CUDA(h, cudaGetLastError());
-                }
+            A_CUDA(h, cudaGetLastError());
+            if (!A->srcs[l].empty()) {
+                const dim3 g2(nbp, (unsigned)A->srcs[l].size());
+                smg::k_adj_transpose2<<<g2, 128, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], A->V, A->lam);
+                A_CUDA(h, cudaGetLastError());
             }
+        }
     }
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     if (grad_U0) {

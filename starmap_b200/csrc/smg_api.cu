@@ -393,8 +393,8 @@ cudaError_t upload_pair(smg_handle* h, int phase, bool alloc) {
                            cudaMemcpyHostToDevice, h->stream);
 }
 
-// RN(1/h) and whether Markstein's correction from it is exact for every
-// dividend (|RN(1/h)*h - 1| < 2^-55 and normal numbers).
+// RN(1/h) per axis and the division mode of recip_div (smg_device.cuh):
+// 2 when |RN(1/h)*h - 1| < 2^-54, 1 for other normal h, 0 otherwise.
 void reciprocals(smg_handle* h) {
     bool used[3] = {false, false, false};
     for (const auto& c : h->coups) used[c.code >> 1] = true;
@@ -403,9 +403,10 @@ void reciprocals(smg_handle* h) {
         const double r = 1.0 / hv;
         const double e = std::fma(r, hv, -1.0);
         h->rh[a] = r;
+        int mode = 0;
+        if (std::isnormal(hv) && std::isnormal(r)) mode = std::fabs(e) < std::ldexp(1.0, -54) ? 2 : 1;
         // an axis without differences never divides; it does not restrict the kernels
-        h->exact_recip[a] = !used[a] ||
-                            (std::isnormal(hv) && std::isnormal(r) && std::fabs(e) < std::ldexp(1.0, -55));
+        h->exact_recip[a] = used[a] ? mode : 2;
     }
 }
 

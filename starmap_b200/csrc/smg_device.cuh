@@ -153,21 +153,33 @@ struct PairArgs {
     int exact_recip[3];
     int filter_substep;
     double* wrec;      // adjoint recording: W of destination di stored at wrec + di*cs (or nullptr)
+    double* prec;      // adjoint recording: destination values before the phase, same slots
 };
 
-// (a - b) / h correctly rounded.  When exact_recip is set the quotient is
-// formed from the precomputed reciprocal rh = RN(1/h) and one Markstein
-// correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al.,
-// Handbook of Floating-Point Arithmetic, "Markstein's theorem"): q = RN(d*rh)
-// is within one ulp of d/h whenever |rh*h - 1| < 2^-55 (checked on the host),
-// the residual r = d - q*h is exact in one FMA, and RN(q + r*rh) is the
-// correctly rounded quotient.  Otherwise the IEEE division is used.
-__device__ __forceinline__ double sdiv(double d, double h, double rh, int exact_recip) {
-    if (exact_recip) {
-        const double q = __dmul_rn(d, rh);
-        const double r = __fma_rn(-q, h, d);
-        return __fma_rn(r, rh, q);
+// (a - b) / h correctly rounded, from the precomputed reciprocal y = RN(1/h)
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al., Handbook of
+// Floating-Point Arithmetic, "Markstein's theorem": if y is within half an
+// ulp of 1/h and q within one ulp of d/h, then r = d - q*h is exact in one FMA
+// and RN(q + r*y) is the correctly rounded quotient).  exact_recip, set per
+// axis on the host:
+//   2: |y*h - 1| < 2^-54, so q = RN(d*y) is already within one ulp: one
+//      correction step (3 FP64 operations);
+//   1: h and y normal: a first correction brings q within one ulp (its error
+//      is ~|y*h-1| times the first error plus one rounding), the second is
+//      the Markstein step (5 operations);
+//   0: IEEE division.
+__device__ __forceinline__ double recip_div(double d, double h, double y, int mode) {
+    double q = __dmul_rn(d, y);
+    if (mode == 1) {
+        const double r0 = __fma_rn(-q, h, d);
+        q = __fma_rn(r0, y, q);
     }
+    const double r = __fma_rn(-q, h, d);
+    return __fma_rn(r, y, q);
+}
+
+__device__ __forceinline__ double sdiv(double d, double h, double rh, int exact_recip) {
+    if (exact_recip) return recip_div(d, h, rh, exact_recip);
     return __ddiv_rn(d, h);
 }
 

@@ -35,11 +35,7 @@ __device__ __forceinline__ double2 ldU2(const double* p) {
 
 template <bool EXACT>
 __device__ __forceinline__ double pdiv(double d, double h, double rh, int exact) {
-    if (EXACT) {
-        const double q = __dmul_rn(d, rh);
-        const double r = __fma_rn(-q, h, d);
-        return __fma_rn(r, rh, q);
-    }
+    if (EXACT) return recip_div(d, h, rh, exact);
     return sdiv(d, h, rh, exact);
 }
 
@@ -192,10 +188,15 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
             }
         }
         const double WA = -SA, WB = -SB;
-        if (a.wrec) {   // adjoint recording of the coupling sum (rare path)
+        if (a.wrec) {   // adjoint recording of the coupling sum and the values before the phase
             double* wp = a.wrec + (long long)di * a.g.cs + pt;
+            double* pp = a.prec + (long long)di * a.g.cs + pt;
             wp[0] = WA;
-            if (v1) wp[1] = WB;
+            pp[0] = u0;
+            if (v1) {
+                wp[1] = WB;
+                pp[1] = u1;
+            }
         }
         if (MODE == 0) {
             u0 = upd(u0, WA, q0, s0, E0, a.hdt);
