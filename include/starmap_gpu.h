@@ -153,6 +153,7 @@ int smg_set_variant(smg_handle* h, int32_t variant);
 #define SMG_TUNE_PAIR_BLOCK  2   /* threads per CTA of the pair kernel (32..256, multiple of 32) */
 #define SMG_TUNE_PAIR_UNROLL 3   /* couplings per inner iteration (1 or 2) */
 #define SMG_TUNE_PAIR_MINB   4   /* register budget: 3 or 4 resident CTAs of 256 threads (64/85 regs) */
+#define SMG_TUNE_ADJ_FUSED   5   /* smg_backward: 1 = one fused kernel per phase (default), 0 = pointwise + transpose kernels */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the
@@ -196,7 +197,10 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
  * Discrete adjoint.  No reference counterpart (the reference has no
  * derivatives); it differentiates exactly the loop smg_run performs.
  * smg_forward(h, nsteps, K) advances nsteps steps from the current state and
- * keeps a checkpoint every K steps; smg_misfit(h, obs, &J) evaluates
+ * keeps a checkpoint every K steps (K = 0: the largest K whose recording fits
+ * in 70% of the free device memory, normally K = nsteps, which records the
+ * whole run during the forward and recomputes nothing); the last segment is
+ * recorded during the forward itself.  smg_misfit(h, obs, &J) evaluates
  * J = 1/2 sum (U_1(T) - obs)^2 on the zeroth moment (obs: host, component-0
  * extents) and seeds the adjoint with U_1(T) - obs (smg_adjoint_seed seeds
  * any adjoint state instead); smg_backward recomputes each segment from its
@@ -207,6 +211,8 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
  * expm1div(-sigma*dt/2) of their sigma field (their derivative enters the
  * sigma gradient); filter fields are constants.  Requires f_position '' or
  * 'substep' and fields that stay fixed between smg_forward and smg_backward.
+ * smg_last_run_stats after smg_forward / smg_backward reports the device
+ * time of that call's GPU work (host copies of the results excluded).
  * --------------------------------------------------------------------------- */
 int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every);
 int smg_misfit(smg_handle* h, const double* obs, double* J);
@@ -216,6 +222,8 @@ int smg_adjoint_seed(smg_handle* h, const double* const* lam);
 int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fields);
 /* Device bytes held for checkpoints and adjoint buffers. */
 int smg_adjoint_bytes(const smg_handle* h, int64_t* bytes);
+/* Segment length K and segment count of the last smg_forward (0, 0 before one). */
+int smg_adjoint_info(const smg_handle* h, int64_t* K, int64_t* nseg);
 
 /* ---------------------------------------------------------------------------
  * Batched solver: many problems (uneven grid sizes and moment orders, each

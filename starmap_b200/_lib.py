@@ -20,6 +20,13 @@ SMG_ETIMEOUT = -3
 SMG_ENONFINITE = -4
 SMG_ENOMEM = -5
 SMG_ESTATE = -6
+
+# smg_tune keys
+SMG_TUNE_PAIR_GROUP = 1
+SMG_TUNE_PAIR_BLOCK = 2
+SMG_TUNE_PAIR_UNROLL = 3
+SMG_TUNE_PAIR_MINB = 4
+SMG_TUNE_ADJ_FUSED = 5
 _NAMES = {SMG_EINVAL: "SMG_EINVAL", SMG_ECUDA: "SMG_ECUDA", SMG_ETIMEOUT: "SMG_ETIMEOUT",
           SMG_ENONFINITE: "SMG_ENONFINITE", SMG_ENOMEM: "SMG_ENOMEM", SMG_ESTATE: "SMG_ESTATE"}
 
@@ -80,6 +87,7 @@ SIGNATURES = {
     "smg_adjoint_seed": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double))]),
     "smg_backward": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double))]),
     "smg_adjoint_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "smg_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
     "smg_batch_destroy": (None, [C.c_void_p]),
     "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),

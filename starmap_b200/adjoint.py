@@ -3,7 +3,7 @@
 ``MisfitAdjoint`` is a forward/backward pair in the shape of an autograd
 function, without a tensor framework (the reference's host is MATLAB/Octave):
 
-    adj = MisfitAdjoint(par, ckpt_every=20)
+    adj = MisfitAdjoint(par)             # ckpt_every=0: record as much as memory allows
     J = adj.forward(obs, nsteps)      # J = 1/2 sum (U_1(T) - obs)^2
     g = adj.backward()                # dict of gradients
     adj.close()
@@ -15,6 +15,12 @@ starmap_solver.m:215-243; a user field defined on the domain gets its gradient
 by summing these through its own sampling), ``g["source"][j]`` for every
 component with a source, ``g["ic"][j]`` for every component, ``g["J"]`` the
 misfit.  Scalar coefficients get scalar derivatives.
+
+``ckpt_every=K`` keeps a checkpoint every K steps and recomputes each segment
+during the backward sweep (memory: about K recorded steps); ``ckpt_every=0``
+picks the largest K that fits in device memory, normally the whole run, so
+that nothing is recomputed.  ``last_ms()`` is the device time of the last
+forward or backward call.
 """
 from __future__ import annotations
 
@@ -27,7 +33,7 @@ __all__ = ["MisfitAdjoint"]
 
 
 class MisfitAdjoint:
-    def __init__(self, par: dict, ckpt_every: int = 20):
+    def __init__(self, par: dict, ckpt_every: int = 0):
         S = prepare(par)
         if S.time_dependent.any() or S.src_td or S.filter_td:
             raise NotImplementedError("the adjoint covers autonomous problems")
@@ -67,6 +73,9 @@ class MisfitAdjoint:
         src = {key[1]: gF[T.index[key]] for key in keys if key[0] == "Q"}
         return {"J": self.J, "sigma_a": sig_a, "sigma_s0": sig_s0, "source": src,
                 "ic": [gU[j] for j in range(S.n_sys)]}
+
+    def last_ms(self) -> float:
+        return self.solver.last_run_stats()[0]
 
     def close(self):
         self.solver.close()

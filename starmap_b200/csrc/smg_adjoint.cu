@@ -51,6 +51,8 @@ struct AdjDest {
 struct TCoup {         // transposed coupling: source i <- destination slot v
     int vslot;         // index of the destination in the phase's destination list
     int code;          // axis*2 + (grid type of source i along axis == 2)
+    int vcomp;         // component index of that destination
+    int pad;
     double w;          // M_d(j,i)
 };
 
@@ -58,6 +60,7 @@ struct AdjSrc {
     int comp;
     int ext[3];
     int tbeg, tend;
+    int pslot;         // index of this component in the other phase type's destination list
 };
 
 struct AdjData {
@@ -80,6 +83,7 @@ struct AdjData {
     AdjSrc* d_srcs[2] = {nullptr, nullptr};
     TCoup* d_tcoup[2] = {nullptr, nullptr};
     bool ready = false, seeded = false;
+    bool tail_valid = false;       // the recording holds the last segment (written by smg_forward)
     size_t bytes = 0;
 };
 
@@ -271,10 +275,134 @@ __global__ void __launch_bounds__(128) k_adj_transpose2(DevGrid g, const AdjSrc*
     if (v1) L[1] -= a1;
 }
 
-template <int MODE>
+// ---------------------------------------------------------------------------
+// Fused backward phase.  The adjoint of destination j is kept scaled by the
+// derivative of its phase's update with respect to its coupling sum,
+//   Y_j = v_j = (dU'/dW)_j lambda'_j,
+// because that is what the transposed coupling of that phase consumes; its
+// own pointwise part lambda_j = (dU'/dU)_j lambda'_j is applied when j is
+// next a target, through rho = (dU'/dU)/(dU'/dW), in which the filter of the
+// last substep cancels and nothing is divided by zero: dU'/dW = F_2 (dt/2) E
+// (r F_1 + 1) with E = expm1div(-s dt/2) > 0 and r = 1 - (dt/2) s E =
+// exp(-s dt/2) > 0 (one substep: F_1 (dt/2) E).  With that, one launch per
+// phase r, over the sources i of the phase (the destinations of phases r-1
+// and r+1), does
+//   lambda_i  = rho_{r+1,i} Y_i           (phase r+1's pointwise part; PM)
+//   grads    += (d/ds, d/dQ of phase r+1 at i) lambda'_i
+//   lambda_i -= sum_j M_d(j,i) D^T Y_j     (phase r's transposed coupling)
+//   Y_i       = (dU'/dW)_{r-1,i} lambda_i  (scaled for phase r-1; NM)
+// and reads/writes disjoint components (sources i, destinations j).
+// PM / NM: 0 none, 1 one substep, 2 two substeps.
+// ---------------------------------------------------------------------------
+template <int M>
+__device__ __forceinline__ double dWdU_scale(const AdjDest& d, long long pt, double hdt) {
+    // dU'/dW of destination d at point pt (M = 1: one substep, 2: two)
+    const double s = cval(d.sg, pt), E = cval(d.E, pt), F1 = cval(d.F1, pt);
+    if (M == 1) return F1 * hdt * E;
+    const double F2 = cval(d.F2, pt);
+    const double r = 1.0 - hdt * s * E;
+    return F2 * hdt * E * (r * F1 + 1.0);
+}
+
+// phase's pointwise adjoint from Y = (dU'/dW) lambda' at one point, with the
+// gradient contributions; u, w: the destination value before the phase and
+// its coupling sum (recorded)
+template <int M>
+__device__ __forceinline__ double pend_point(const AdjDest& d, long long pt, double u, double w, double Y,
+                                             double hdt) {
+    const double s = cval(d.sg, pt), E = cval(d.E, pt), q = cval(d.Q, pt), F1 = cval(d.F1, pt);
+    const double r = 1.0 - hdt * s * E;
+    double rho, dsdw = 0.0;
+    if (M == 1) {
+        rho = r / (hdt * E);
+        if (d.gs) {
+            const double dE = cval(d.dE, pt);
+            const double G = w + q - s * u;
+            dsdw = (-u * E + G * dE) / E;
+        }
+    } else {
+        const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
+        rho = F1 * r * r * den;
+        if (d.gs) {
+            const double dE = cval(d.dE, pt);
+            const double G0 = w + q - s * u;
+            const double V1 = F1 * (u + hdt * G0 * E);
+            const double G1 = w + q - s * V1;
+            dsdw = (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
+        }
+    }
+    if (d.gs) atomicAdd(d.gs + pt, dsdw * Y);
+    if (d.gq) atomicAdd(d.gq + pt, Y);   // dU'/dQ = dU'/dW
+    return rho * Y;
+}
+
+template <int PM, int NM>
+__global__ void __launch_bounds__(128) k_adj_fused(DevGrid g, const AdjSrc* srcs, const TCoup* tc, int coup,
+                                                   const AdjDest* pend, const double* __restrict__ pre,
+                                                   const double* __restrict__ W, const AdjDest* next, double* Y,
+                                                   double hdt) {
+    const int tpr = (g.B[0] + 1) / 2;
+    const long long rows = (long long)g.B[1] * g.B[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int si = blockIdx.y;
+    if (t >= (long long)tpr * rows) return;
+    const int x0 = 2 * (int)(t % tpr);
+    const long long row = t / tpr;
+    const int y = (int)(row % g.B[1]);
+    const int z = (int)(row / g.B[1]);
+    const AdjSrc S = srcs[si];
+    if (x0 >= S.ext[0] || y >= S.ext[1] || z >= S.ext[2]) return;
+    const bool v1 = x0 + 1 < S.ext[0];
+    const long long pt = (long long)z * g.s2 + (long long)y * g.s1 + x0;
+    double* Yi = Y + (long long)S.comp * g.cs + pt;
+    double l0, l1 = 0.0;
+    if (v1) {
+        const double2 v = ld2(Yi);
+        l0 = v.x;
+        l1 = v.y;
+    } else {
+        l0 = Yi[0];
+    }
+    if (PM) {
+        const AdjDest& d = pend[S.pslot];
+        const long long rp = (long long)S.pslot * g.cs + pt;
+        l0 = pend_point<PM>(d, pt, pre[rp], W[rp], l0, hdt);
+        if (v1) l1 = pend_point<PM>(d, pt + 1, pre[rp + 1], W[rp + 1], l1, hdt);
+    }
+    if (coup) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int c = S.tbeg; c < S.tend; ++c) {
+            const TCoup tcp = tc[c];
+            const int ax = tcp.code >> 1, g2 = tcp.code & 1;
+            const double* v = Y + (long long)tcp.vcomp * g.cs + pt;
+            const double f = tcp.w / g.h[ax];
+            if (ax == 0) {
+                a0 += f * dT(v, x0, g.n[0], g.bc[0], g2, 1);
+                if (v1) a1 += f * dT(v + 1, x0 + 1, g.n[0], g.bc[0], g2, 1);
+            } else {
+                const int q = ax == 1 ? y : z;
+                const long long st = ax == 1 ? g.s1 : g.s2;
+                const double2 d = dT_row(v, q, g.n[ax], g.bc[ax], g2, st);
+                a0 += f * d.x;
+                a1 += f * d.y;
+            }
+        }
+        l0 -= a0;
+        l1 -= a1;
+    }
+    if (NM) {
+        const AdjDest& n = next[S.pslot];
+        l0 *= dWdU_scale<NM>(n, pt, hdt);
+        if (v1) l1 *= dWdU_scale<NM>(n, pt + 1, hdt);
+    }
+    if (v1) *reinterpret_cast<double2*>(Yi) = make_double2(l0, l1);
+    else Yi[0] = l0;
+}
+
+template <int MODE, int DIV>
 __global__ void __launch_bounds__(256, 4) k_pair_rec(PairArgs a, int kf) {
     const int bid = blockIdx.x;
-    pair_item<MODE, false, 1, true>(a, kf, bid % a.ngroups, (bid / a.ngroups) % a.nchunks,
+    pair_item<MODE, DIV, 1, true, true>(a, kf, bid % a.ngroups, (bid / a.ngroups) % a.nchunks,
                                     bid / a.ngroups / a.nchunks, threadIdx.x, blockDim.x);
 }
 
@@ -332,10 +460,33 @@ cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double*
     const smg::PairArgs a = rec_args(h, phase, U, wrec, prec);
     if (a.ndest == 0) return cudaSuccess;
     const unsigned nb = (unsigned)((long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2]);
-    if (mode == 1) smg::k_pair_rec<1><<<nb, 64, 0, h->stream>>>(a, kf);
-    else if (mode == 2) smg::k_pair_rec<2><<<nb, 64, 0, h->stream>>>(a, kf);
-    else smg::k_pair_rec<0><<<nb, 64, 0, h->stream>>>(a, kf);
+    const int div = std::min(a.exact_recip[0], std::min(a.exact_recip[1], a.exact_recip[2]));
+#define SMG_REC(D)                                                                          \
+    if (mode == 1) smg::k_pair_rec<1, D><<<nb, 64, 0, h->stream>>>(a, kf);                 \
+    else if (mode == 2) smg::k_pair_rec<2, D><<<nb, 64, 0, h->stream>>>(a, kf);            \
+    else smg::k_pair_rec<0, D><<<nb, 64, 0, h->stream>>>(a, kf);
+    if (div == 2) { SMG_REC(2) }
+    else if (div == 1) { SMG_REC(1) }
+    else { SMG_REC(0) }
+#undef SMG_REC
     return cudaGetLastError();
+}
+
+// One segment of ks steps from state U with recording, in smg_run's phase
+// order: A(k=1), then per step B and the fused A(k=2)A(k=1) -- A(k=2) alone
+// after the last step.  Phase r records into slot r (2ks+1 slots).
+cudaError_t record_segment(smg_handle* h, int64_t ks, double* U) {
+    const AdjData* A = h->adj;
+    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
+    for (int64_t r = 0; r <= 2 * ks; ++r) {
+        const int kind = r == 0 ? 0 : (r & 1 ? 1 : (r < 2 * ks ? 2 : 3));
+        const int mode = kind == 1 ? 1 : (kind == 2 ? 2 : 0);
+        const int kf = kind == 3 ? 2 : 1;
+        const cudaError_t e = launch_rec(h, mode, kf, U, (double*)((char*)A->rec_w + vb * r),
+                                         (double*)((char*)A->rec_state + vb * r));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 void free_adj(smg_handle* h) {
@@ -367,11 +518,18 @@ smg::AdjCoef coef_of(const smg_handle* h, int f) {
 int build_tables(smg_handle* h) {
     AdjData* A = h->adj;
     const int one = h->field_one;
+    // destinations of each phase type in the pair table's order: the recorded
+    // W / pre-values and the scratch V use that index as their slot
+    std::vector<int> Dl[2];
+    std::map<int, int> slot_in[2];
+    for (int l = 0; l < 2; ++l)
+        for (const auto& pd : h->pair[l].dests) {
+            const int j = (int)((long long)pd.off / h->g.cs);
+            slot_in[l][j] = (int)Dl[l].size();
+            Dl[l].push_back(j);
+        }
     for (int l = 0; l < 2; ++l) {
-        // destinations in the pair table's order: the recorded W and the
-        // scratch V use that index as their slot
-        std::vector<int> D;
-        for (const auto& pd : h->pair[l].dests) D.push_back((int)((long long)pd.off / h->g.cs));
+        const std::vector<int>& D = Dl[l];
         const std::vector<int>& Sset = l == 0 ? h->destB : h->destA;   // sources of the phase
         A->dests[l].clear();
         A->srcs[l].clear();
@@ -411,7 +569,7 @@ int build_tables(smg_handle* h) {
         std::map<int, std::vector<smg::TCoup>> bysrc;
         for (int j : D)
             for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q)
-                bysrc[h->coups[q].src].push_back(smg::TCoup{slot_of[j], h->coups[q].code, h->coups[q].w});
+                bysrc[h->coups[q].src].push_back(smg::TCoup{slot_of[j], h->coups[q].code, j, 0, h->coups[q].w});
         for (int i : Sset) {
             smg::AdjSrc s{};
             s.comp = i;
@@ -419,6 +577,8 @@ int build_tables(smg_handle* h) {
             s.tbeg = (int)A->tcoup[l].size();
             for (const auto& t : bysrc[i]) A->tcoup[l].push_back(t);
             s.tend = (int)A->tcoup[l].size();
+            const auto it = slot_in[1 - l].find(i);
+            s.pslot = it == slot_in[1 - l].end() ? -1 : it->second;
             A->srcs[l].push_back(s);
         }
         cudaFree(A->d_dests[l]);
@@ -455,23 +615,168 @@ void grid_ext(const smg_handle* h, int f, int e[3]) {
 
 }  // namespace
 
+namespace {
+
+// Two kernels per phase: k_adj_point over the destinations, then
+// k_adj_transpose2 over the sources.  Segments are walked last to first,
+// each recomputed from its checkpoint (the last one is still recorded from
+// smg_forward).
+cudaError_t backward_split(smg_handle* h, int64_t* launches) {
+    AdjData* A = h->adj;
+    const size_t sb = state_bytes(h);
+    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
+    const long long npts = h->g.s2 * h->g.B[2];
+    const unsigned nbx = (unsigned)((npts + 255) / 256);
+    const int tpr = (h->g.B[0] + 1) / 2;
+    const unsigned nbp = (unsigned)(((long long)tpr * h->g.B[1] * h->g.B[2] + 127) / 128);
+    const size_t nA = A->dests[0].size() / 3;
+    for (int64_t s = A->nseg - 1; s >= 0; --s) {
+        const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
+        if (!(s == A->nseg - 1 && A->tail_valid)) {
+            cudaError_t e = cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream);
+            if (e != cudaSuccess) return e;
+            e = record_segment(h, ks, A->work);
+            if (e != cudaSuccess) return e;
+            *launches += 2 * ks + 1;
+        }
+        for (int64_t r = 2 * ks; r >= 0; --r) {
+            const int kind = r == 0 ? 0 : (r & 1 ? 1 : (r < 2 * ks ? 2 : 3));
+            const int l = kind == 1 ? 1 : 0;
+            const double* pre = (const double*)((const char*)A->rec_state + vb * r);
+            const double* W = (const double*)((const char*)A->rec_w + vb * r);
+            if (l == 1 && !A->dests[1].empty()) {
+                const dim3 g1(nbx, (unsigned)A->dests[1].size());
+                smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[1], pre, W, A->lam, A->V, h->hdt);
+                ++*launches;
+            } else if (l == 0 && nA) {
+                const dim3 g1(nbx, (unsigned)nA);
+                if (kind == 0)
+                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0], pre, W, A->lam, A->V, h->hdt);
+                else if (kind == 3)
+                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + nA, pre, W, A->lam, A->V,
+                                                                   h->hdt);
+                else
+                    smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + 2 * nA, pre, W, A->lam, A->V,
+                                                                   h->hdt);
+                ++*launches;
+            }
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (!A->srcs[l].empty()) {
+                const dim3 g2(nbp, (unsigned)A->srcs[l].size());
+                smg::k_adj_transpose2<<<g2, 128, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], A->V, A->lam);
+                ++*launches;
+                e = cudaGetLastError();
+                if (e != cudaSuccess) return e;
+            }
+        }
+    }
+    return cudaSuccess;
+}
+
+// One k_adj_fused launch per phase.  The backward sees the phases of one
+// smg_run over all steps: A(k=1), (B, A(k=2)A(k=1))*, B, A(k=2); the A(k=2)
+// ending a segment and the A(k=1) starting the next one form one fused A-A
+// phase (same sources, same W; its values before are those recorded before
+// the segment's A(k=2)), so destinations and sources alternate strictly.
+// Phase kinds: 0 A(k=1), 1 B, 2 fused A-A, 3 A(k=2).
+cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
+    AdjData* A = h->adj;
+    const size_t sb = state_bytes(h);
+    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
+    const int tpr = (h->g.B[0] + 1) / 2;
+    const unsigned nbp = (unsigned)(((long long)tpr * h->g.B[1] * h->g.B[2] + 127) / 128);
+    const size_t nA = A->dests[0].size() / 3;
+    auto table = [&](int kind) -> const smg::AdjDest* {
+        if (kind < 0) return nullptr;
+        if (kind == 1) return A->d_dests[1];
+        return A->d_dests[0] + (kind == 0 ? 0 : (kind == 3 ? nA : 2 * nA));
+    };
+    auto substeps = [](int kind) { return kind < 0 ? 0 : (kind == 1 || kind == 2 ? 2 : 1); };
+    // targets l: 0 = sources of an A phase (B destinations), 1 = sources of a B phase
+    auto launch = [&](int l, int coup, int pkind, const double* pre, const double* W, int nkind) -> cudaError_t {
+        if (A->srcs[l].empty()) return cudaSuccess;
+        const dim3 grid(nbp, (unsigned)A->srcs[l].size());
+        const int PM = substeps(pkind), NM = substeps(nkind);
+        const smg::AdjDest* pt = table(pkind);
+        const smg::AdjDest* nt = table(nkind);
+#define SMG_FUSED(P, N)                                                                                 \
+    if (PM == P && NM == N)                                                                             \
+        smg::k_adj_fused<P, N><<<grid, 128, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], coup, pt, pre, W, \
+                                                            nt, A->lam, h->hdt);
+        SMG_FUSED(0, 0) SMG_FUSED(0, 1) SMG_FUSED(0, 2) SMG_FUSED(1, 0) SMG_FUSED(1, 1) SMG_FUSED(1, 2)
+        SMG_FUSED(2, 0) SMG_FUSED(2, 1) SMG_FUSED(2, 2)
+#undef SMG_FUSED
+        ++*launches;
+        return cudaGetLastError();
+    };
+    auto slot = [&](const double* base, int64_t r) { return (const double*)((const char*)base + vb * r); };
+    // the adjoint seed of the last phase's (A(k=2)) destinations, scaled
+    cudaError_t e = launch(1, 0, -1, nullptr, nullptr, 3);
+    if (e != cudaSuccess) return e;
+    for (int64_t s = A->nseg - 1; s >= 0; --s) {
+        const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
+        const bool last = s == A->nseg - 1;
+        if (!(last && A->tail_valid)) {
+            e = cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream);
+            if (e != cudaSuccess) return e;
+            e = record_segment(h, ks, A->work);
+            if (e != cudaSuccess) return e;
+            *launches += 2 * ks + 1;
+        }
+        for (int64_t l = last ? 2 * ks : 2 * ks - 1; l >= 0; --l) {
+            const int64_t p = l + 1;   // the phase after l (its pointwise part is pending)
+            int pkind = -1;
+            if (p <= 2 * ks) pkind = (p & 1) ? 1 : (p < 2 * ks ? 2 : (last ? 3 : 2));
+            int nkind = -1;            // the phase before l (the targets' destination phase)
+            if (l >= 1) nkind = ((l - 1) & 1) ? 1 : (l - 1 >= 2 ? 2 : (s == 0 ? 0 : 2));
+            else if (s > 0) nkind = 1;
+            e = launch((l & 1) ? 1 : 0, 1, pkind, pkind < 0 ? nullptr : slot(A->rec_state, p),
+                       pkind < 0 ? nullptr : slot(A->rec_w, p), nkind);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    // the first phase's (A(k=1)) pointwise part on its destinations
+    return launch(1, 0, 0, slot(A->rec_state, 0), slot(A->rec_w, 0), -1);
+}
+
+}  // namespace
+
 void smg_adjoint_free(smg_handle* h) { free_adj(h); }
 
 extern "C" {
 
 int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     if (!h) return SMG_EINVAL;
-    if (nsteps < 1 || ckpt_every < 1) return afail(h, SMG_EINVAL, "smg_forward: nsteps and ckpt_every must be >= 1");
+    if (nsteps < 1 || ckpt_every < 0)
+        return afail(h, SMG_EINVAL, "smg_forward: nsteps must be >= 1 and ckpt_every >= 0");
     if (!h->dt_set || !h->state_set) return afail(h, SMG_ESTATE, "smg_forward: set the state and dt first");
     if (h->filter_mode == SMG_FILTER_FULL)
         return afail(h, SMG_EINVAL, "smg_forward: the adjoint supports f_position '' and 'substep'");
     if (!(h->pair[0].ok && h->pair[1].ok)) return afail(h, SMG_EINVAL, "smg_forward: pair tables unavailable");
-    const int64_t K = std::min<int64_t>(ckpt_every, nsteps);
-    const int64_t nseg = (nsteps + K - 1) / K;
-    AdjData* A = h->adj;
     const size_t sb = state_bytes(h);
     const int maxdest = (int)std::max(h->destA.size(), h->destB.size());
     const size_t vb = (size_t)h->g.cs * std::max(maxdest, 1) * sizeof(double);
+    int64_t K = std::min<int64_t>(ckpt_every, nsteps);
+    if (ckpt_every == 0) {
+        // the largest K (fewest recomputed steps) whose checkpoints and
+        // recording fit in 70% of the free memory (the buffers this handle
+        // already holds count as free)
+        size_t fr = 0, tot = 0;
+        A_CUDA(h, cudaMemGetInfo(&fr, &tot));
+        const double held = h->adj ? (double)h->adj->bytes : 0.0;
+        const double budget = 0.7 * ((double)fr + held) - 4.0 * (double)sb;
+        K = 1;
+        for (int64_t k = nsteps; k >= 1; --k) {
+            const int64_t ns = (nsteps + k - 1) / k;
+            if ((double)sb * (ns + 2) + 2.0 * (double)vb * (2 * k + 1) <= budget) {
+                K = k;
+                break;
+            }
+        }
+    }
+    const int64_t nseg = (nsteps + K - 1) / K;
+    AdjData* A = h->adj;
     if (!A || A->K != K || A->nseg != nseg) {
         // (re)allocate: checkpoints, work/adjoint/scratch states and the
         // recording of one segment (2K+1 phases); kept for later calls
@@ -490,6 +795,7 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
         A_CUDA(h, cudaMalloc(&A->rec_w, vb * (2 * K + 1)));
         A_CUDA(h, cudaMemsetAsync(A->V, 0, vb, h->stream));
         A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * (2 * K + 1), h->stream));
+        A_CUDA(h, cudaMemsetAsync(A->rec_state, 0, vb * (2 * K + 1), h->stream));
         A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
     } else {
         for (double* p : A->gfield) cudaFree(p);
@@ -497,6 +803,8 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
         A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
     }
     A->nsteps = nsteps;
+    A->ready = false;
+    A->tail_valid = false;
     // gradient slots for sigma and source fields; d(decay)/d(sigma) per sigma field
     const int nf = (int)h->field_grid.size();
     A->gfield.assign(nf, nullptr);
@@ -525,16 +833,29 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     }
     int rc = build_tables(h);
     if (rc != SMG_OK) return rc;
-    // forward: checkpoint at the start of every segment, the segment itself as smg_run
+    for (int l = 0; l < 2; ++l)
+        for (const auto& sr : A->srcs[l])
+            if (sr.pslot < 0) return afail(h, SMG_EINVAL, "smg_forward: a component is no phase's destination");
+    // forward: checkpoint at the start of every segment; every segment but the
+    // last as smg_run, the last one recorded for the backward sweep
+    A_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    h->last_launches = 0;
     for (int64_t s = 0; s < A->nseg; ++s) {
         A_CUDA(h, cudaMemcpyAsync(A->ckpt[s], h->dU, sb, cudaMemcpyDeviceToDevice, h->stream));
         const int64_t ks = std::min<int64_t>(A->K, nsteps - s * A->K);
-        rc = smg_run(h, ks);
-        if (rc != SMG_OK) return rc;
+        if (s + 1 < A->nseg) {
+            rc = smg::run_steps(h, ks, false);
+            if (rc != SMG_OK) return rc;
+        } else {
+            A_CUDA(h, record_segment(h, ks, h->dU));
+            h->last_launches += 2 * ks + 1;
+        }
     }
+    A_CUDA(h, cudaEventRecord(h->ev1, h->stream));
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     A->ready = true;
     A->seeded = false;
+    A->tail_valid = true;
     return SMG_OK;
 }
 
@@ -594,58 +915,16 @@ int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fiel
     AdjData* A = h->adj;
     if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_backward: call smg_forward first");
     if (!A->seeded) return afail(h, SMG_ESTATE, "smg_backward: seed the adjoint (smg_misfit or smg_adjoint_seed)");
-    const size_t sb = state_bytes(h);
-    const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
     for (double* g : A->gfield)
         if (g) A_CUDA(h, cudaMemsetAsync(g, 0, (size_t)h->g.cs * sizeof(double), h->stream));
-    const long long npts = h->g.s2 * h->g.B[2];
-    const unsigned nbx = (unsigned)((npts + 255) / 256);
-    const int tpr = (h->g.B[0] + 1) / 2;
-    const unsigned nbp = (unsigned)(((long long)tpr * h->g.B[1] * h->g.B[2] + 127) / 128);
-    const size_t nA = A->dests[0].size() / 3;
-    for (int64_t s = A->nseg - 1; s >= 0; --s) {
-        const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
-        // the segment's phases as smg_run performs them: A(k=1), then per step
-        // B and the fused A(k=2)A(k=1) -- A(k=2) alone after the last step
-        std::vector<int> kind;   // 0: A k=1, 1: B, 2: fused A-A, 3: A k=2
-        kind.push_back(0);
-        for (int64_t k = 0; k < ks; ++k) {
-            kind.push_back(1);
-            kind.push_back(k + 1 < ks ? 2 : 3);
-        }
-        A_CUDA(h, cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream));
-        for (size_t r = 0; r < kind.size(); ++r) {
-            const int mode = kind[r] == 1 ? 1 : (kind[r] == 2 ? 2 : 0);
-            const int kf = kind[r] == 3 ? 2 : 1;
-            A_CUDA(h, launch_rec(h, mode, kf, A->work, (double*)((char*)A->rec_w + vb * r),
-                                 (double*)((char*)A->rec_state + vb * r)));
-        }
-        for (int64_t r = (int64_t)kind.size() - 1; r >= 0; --r) {
-            const int l = kind[r] == 1 ? 1 : 0;
-            const double* pre = (const double*)((const char*)A->rec_state + vb * r);
-            const double* W = (const double*)((const char*)A->rec_w + vb * r);
-            if (l == 1 && !A->dests[1].empty()) {
-                const dim3 g1(nbx, (unsigned)A->dests[1].size());
-                smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[1], pre, W, A->lam, A->V, h->hdt);
-            } else if (l == 0 && nA) {
-                const dim3 g1(nbx, (unsigned)nA);
-                if (kind[r] == 0)
-                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0], pre, W, A->lam, A->V, h->hdt);
-                else if (kind[r] == 3)
-                    smg::k_adj_point<0><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + nA, pre, W, A->lam, A->V,
-                                                                   h->hdt);
-                else
-                    smg::k_adj_point<1><<<g1, 256, 0, h->stream>>>(h->g, A->d_dests[0] + 2 * nA, pre, W, A->lam, A->V,
-                                                                   h->hdt);
-            }
-            A_CUDA(h, cudaGetLastError());
-            if (!A->srcs[l].empty()) {
-                const dim3 g2(nbp, (unsigned)A->srcs[l].size());
-                smg::k_adj_transpose2<<<g2, 128, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], A->V, A->lam);
-                A_CUDA(h, cudaGetLastError());
-            }
-        }
-    }
+    A_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    int64_t launches = 0;
+    const cudaError_t e = h->adj_fused ? backward_fused(h, &launches) : backward_split(h, &launches);
+    if (e != cudaSuccess) return acuda(h, e, "smg_backward");
+    A_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    h->last_launches = launches;
+    A->seeded = false;               // lambda now holds dJ/dU(0)
+    A->tail_valid = A->nseg == 1;    // the recording now holds segment 0
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     if (grad_U0) {
         for (int j = 0; j < h->n_sys; ++j) {
@@ -699,6 +978,13 @@ int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fiel
 int smg_adjoint_bytes(const smg_handle* h, int64_t* bytes) {
     if (!h || !bytes) return SMG_EINVAL;
     *bytes = h->adj ? (int64_t)h->adj->bytes : 0;
+    return SMG_OK;
+}
+
+int smg_adjoint_info(const smg_handle* h, int64_t* K, int64_t* nseg) {
+    if (!h) return SMG_EINVAL;
+    if (K) *K = h->adj ? h->adj->K : 0;
+    if (nseg) *nseg = h->adj ? h->adj->nseg : 0;
     return SMG_OK;
 }
 

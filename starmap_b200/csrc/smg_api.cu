@@ -853,6 +853,14 @@ int smg_run(smg_handle* h, int64_t nsteps) {
     if (nsteps < 0) return fail(h, SMG_EINVAL, "smg_run: nsteps must be >= 0");
     if (!h->dt_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_dt has not been called");
     if (!h->state_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_state has not been called");
+    return smg::run_steps(h, nsteps, true);
+}
+
+}  // extern "C"
+
+// nsteps steps on the handle's stream; with `events`, bracketed by the
+// handle's timing events (smg_last_run_stats)
+int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
     const int64_t kBlock = 64;   // steps per captured graph
     int64_t left = nsteps;
     if (left >= kBlock) {
@@ -872,16 +880,18 @@ int smg_run(smg_handle* h, int64_t nsteps) {
         }
     }
     int64_t launches = 0, rem = 0;
-    SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
     for (; left >= kBlock; left -= kBlock) {
         SMG_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
         launches += h->graph_launches;
     }
     SMG_CUDA(h, enqueue_steps(h, left, h->stream, &rem));
-    SMG_CUDA(h, cudaEventRecord(h->ev1, h->stream));
-    h->last_launches = launches + rem;
+    if (events) SMG_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    h->last_launches = events ? launches + rem : h->last_launches + launches + rem;
     return SMG_OK;
 }
+
+extern "C" {
 
 int smg_tune(smg_handle* h, int32_t key, int32_t value) {
     if (!h) return fail(h, SMG_EINVAL, "smg_tune: NULL handle");
@@ -902,6 +912,10 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             if (value != 3 && value != 4) return fail(h, SMG_EINVAL, "smg_tune: minb must be 3 or 4");
             h->pair_minb = value;
             break;
+        case SMG_TUNE_ADJ_FUSED:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj_fused must be 0 or 1");
+            h->adj_fused = value;
+            return SMG_OK;
         default:
             return fail(h, SMG_EINVAL, "smg_tune: unknown key");
     }

@@ -84,9 +84,10 @@ __device__ bool grid_barrier(const BatchArgs& B, int* s_flag) {
 
 template <int MODE>
 __device__ __forceinline__ void run_item(const smg::PairArgs& a, int kf, const BatchItem& it) {
-    const bool exact = a.exact_recip[0] && a.exact_recip[1] && a.exact_recip[2];
-    if (exact) smg::pair_item<MODE, true, 1, false>(a, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
-    else smg::pair_item<MODE, false, 1, false>(a, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    const int div = min(a.exact_recip[0], min(a.exact_recip[1], a.exact_recip[2]));
+    if (div == 2) smg::pair_item<MODE, 2, 1, false>(a, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    else if (div == 1) smg::pair_item<MODE, 1, 1, false>(a, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    else smg::pair_item<MODE, 0, 1, false>(a, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
 }
 
 __global__ void __launch_bounds__(256, 4) k_batch(BatchArgs B) {
@@ -130,9 +131,10 @@ __global__ void __launch_bounds__(256, 4) k_batch_phase(const smg::PairArgs* arg
         for (int k = threadIdx.x; k < (int)(sizeof(smg::PairArgs) / 4); k += blockDim.x) dst[k] = src[k];
     }
     __syncthreads();
-    const bool exact = sa.exact_recip[0] && sa.exact_recip[1] && sa.exact_recip[2];
-    if (exact) smg::pair_item<MODE, true, 1, true>(sa, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
-    else smg::pair_item<MODE, false, 1, true>(sa, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    const int div = min(sa.exact_recip[0], min(sa.exact_recip[1], sa.exact_recip[2]));
+    if (div == 2) smg::pair_item<MODE, 2, 1, true>(sa, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    else if (div == 1) smg::pair_item<MODE, 1, 1, true>(sa, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
+    else smg::pair_item<MODE, 0, 1, true>(sa, kf, it.grp, it.chunk, it.row, threadIdx.x, blockDim.x);
 }
 
 }  // namespace

@@ -183,6 +183,26 @@ __device__ __forceinline__ double sdiv(double d, double h, double rh, int exact_
     return __ddiv_rn(d, h);
 }
 
+// Division with the mode fixed at compile time for every axis of a launch
+// (DIV = the smallest per-axis mode; the two-step form is exact wherever the
+// one-step form is).  DIV 0 keeps the per-axis choice at run time.
+template <int DIV>
+__device__ __forceinline__ double tdiv(double d, double h, double rh, int exact_recip) {
+    if (DIV == 2) {
+        const double q = __dmul_rn(d, rh);
+        const double r = __fma_rn(-q, h, d);
+        return __fma_rn(r, rh, q);
+    }
+    if (DIV == 1) {
+        double q = __dmul_rn(d, rh);
+        const double r0 = __fma_rn(-q, h, d);
+        q = __fma_rn(r0, rh, q);
+        const double r = __fma_rn(-q, h, d);
+        return __fma_rn(r, rh, q);
+    }
+    return sdiv(d, h, rh, exact_recip);
+}
+
 __device__ __forceinline__ double fld(const DevField* f, int i, long long pt) {
     const DevField F = f[i];
     return F.p ? __ldg(F.p + pt) : F.s;

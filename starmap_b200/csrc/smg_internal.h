@@ -84,6 +84,7 @@ struct smg_handle {
     int nxs = 0;                     // 32-point strips per row
     bool strip_staged = false;       // stage slot-job loads with cp.async
     smg::AdjData* adj = nullptr;     // adjoint checkpoints and buffers (smg_forward)
+    int adj_fused = 1;               // smg_backward kernel form (SMG_TUNE_ADJ_FUSED)
 };
 
 void smg_adjoint_free(smg_handle* h);   // smg_adjoint.cu
@@ -100,6 +101,7 @@ constexpr int kStripWarps = 8;
 constexpr int kSumsqBlocks = 32;     // CTAs per component in the sum-of-squares reduction
 constexpr int kSumsqThreads = 256;
 void set_global_error(const std::string& msg);   // message of smg_last_error(NULL)
+int run_steps(smg_handle* h, int64_t nsteps, bool events);   // smg_run without argument checks
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);
 constexpr int kMaxStripSmem = 200 * 1024;

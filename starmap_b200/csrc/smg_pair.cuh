@@ -15,7 +15,8 @@ namespace smg {
 // A destination's couplings come in at most three runs (its x-, y- and
 // z-lists); within a run the stencil offsets, h and the division are fixed,
 // so they are selected once per run.  No shared memory and no barriers.
-// EXACT: every axis admits the exact reciprocal division.
+// DIV: the division mode of the launch (tdiv); REC: adjoint recording of the
+// coupling sums and pre-phase values (wrec/prec).
 // ---------------------------------------------------------------------------
 // Loads of the state U.  NC: the read-only (non-coherent) path, valid when U
 // is not written during the launch by another CTA that this CTA could read
@@ -33,11 +34,6 @@ __device__ __forceinline__ double2 ldU2(const double* p) {
     return *reinterpret_cast<const double2*>(p);
 }
 
-template <bool EXACT>
-__device__ __forceinline__ double pdiv(double d, double h, double rh, int exact) {
-    if (EXACT) return recip_div(d, h, rh, exact);
-    return sdiv(d, h, rh, exact);
-}
 
 __device__ __forceinline__ void pair_coef(const PairDest& dj, int k, const double* Fbase_unused, long long pt,
                                           bool v1, double& c0, double& c1) {
@@ -59,7 +55,7 @@ __device__ __forceinline__ void pair_coef(const PairDest& dj, int k, const doubl
 // One work item of the pair kernel: destinations [grp*group, ...) of row `row`,
 // points of chunk `chunk` (bdim threads, two points each).  Shared by the
 // plain launch (one item per CTA) and the batched persistent kernel.
-template <int MODE, bool EXACT, int UNROLL, bool NC = true>
+template <int MODE, int DIV, int UNROLL, bool NC = true, bool REC = false>
 __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, int chunk, int row, int tid, int bdim) {
     const int y = row % a.g.B[1];
     const int z = row / a.g.B[1];
@@ -132,10 +128,10 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
                         const double c0 = ldU<NC>(Upt + (o0 + hb)), e0 = ldU<NC>(Upt + (o0 + lb));
                         const double a1 = ldU<NC>(Upt + (o1 + ha)), b1 = ldU<NC>(Upt + (o1 + la));
                         const double c1 = ldU<NC>(Upt + (o1 + hb)), e1 = ldU<NC>(Upt + (o1 + lb));
-                        const double tA0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(a0, b0), hh, rr, ee), w0);
-                        const double tB0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(c0, e0), hh, rr, ee), w0);
-                        const double tA1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(a1, b1), hh, rr, ee), w1);
-                        const double tB1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(c1, e1), hh, rr, ee), w1);
+                        const double tA0 = __dmul_rn(tdiv<DIV>(__dsub_rn(a0, b0), hh, rr, ee), w0);
+                        const double tB0 = __dmul_rn(tdiv<DIV>(__dsub_rn(c0, e0), hh, rr, ee), w0);
+                        const double tA1 = __dmul_rn(tdiv<DIV>(__dsub_rn(a1, b1), hh, rr, ee), w1);
+                        const double tB1 = __dmul_rn(tdiv<DIV>(__dsub_rn(c1, e1), hh, rr, ee), w1);
                         if (first) { SA = tA0; SB = tB0; first = false; }
                         else { SA = __dadd_rn(SA, tA0); SB = __dadd_rn(SB, tB0); }
                         SA = __dadd_rn(SA, tA1);
@@ -145,8 +141,8 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
                 for (; c < ce; ++c) {
                     const int o = a.coff[c];
                     const double w = a.cw[c];
-                    const double dA = pdiv<EXACT>(__dsub_rn(ldU<NC>(Upt + (o + ha)), ldU<NC>(Upt + (o + la))), hh, rr, ee);
-                    const double dB = pdiv<EXACT>(__dsub_rn(ldU<NC>(Upt + (o + hb)), ldU<NC>(Upt + (o + lb))), hh, rr, ee);
+                    const double dA = tdiv<DIV>(__dsub_rn(ldU<NC>(Upt + (o + ha)), ldU<NC>(Upt + (o + la))), hh, rr, ee);
+                    const double dB = tdiv<DIV>(__dsub_rn(ldU<NC>(Upt + (o + hb)), ldU<NC>(Upt + (o + lb))), hh, rr, ee);
                     const double tA = __dmul_rn(dA, w), tB = __dmul_rn(dB, w);
                     if (first) { SA = tA; SB = tB; first = false; }
                     else { SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB); }
@@ -165,10 +161,10 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
                         const double2 lv0 = ldU2<NC>(Upt + (o0 + ol));
                         const double2 hv1 = ldU2<NC>(Upt + (o1 + oh));
                         const double2 lv1 = ldU2<NC>(Upt + (o1 + ol));
-                        const double tA0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv0.x, lv0.x), hh, rr, ee), w0);
-                        const double tB0 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv0.y, lv0.y), hh, rr, ee), w0);
-                        const double tA1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv1.x, lv1.x), hh, rr, ee), w1);
-                        const double tB1 = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv1.y, lv1.y), hh, rr, ee), w1);
+                        const double tA0 = __dmul_rn(tdiv<DIV>(__dsub_rn(hv0.x, lv0.x), hh, rr, ee), w0);
+                        const double tB0 = __dmul_rn(tdiv<DIV>(__dsub_rn(hv0.y, lv0.y), hh, rr, ee), w0);
+                        const double tA1 = __dmul_rn(tdiv<DIV>(__dsub_rn(hv1.x, lv1.x), hh, rr, ee), w1);
+                        const double tB1 = __dmul_rn(tdiv<DIV>(__dsub_rn(hv1.y, lv1.y), hh, rr, ee), w1);
                         if (first) { SA = tA0; SB = tB0; first = false; }
                         else { SA = __dadd_rn(SA, tA0); SB = __dadd_rn(SB, tB0); }
                         SA = __dadd_rn(SA, tA1);
@@ -180,15 +176,15 @@ __device__ __forceinline__ void pair_item(const PairArgs& a, int kf, int grp, in
                     const double w = a.cw[c];
                     const double2 hv = ldU2<NC>(Upt + (o + oh));
                     const double2 lv = ldU2<NC>(Upt + (o + ol));
-                    const double tA = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv.x, lv.x), hh, rr, ee), w);
-                    const double tB = __dmul_rn(pdiv<EXACT>(__dsub_rn(hv.y, lv.y), hh, rr, ee), w);
+                    const double tA = __dmul_rn(tdiv<DIV>(__dsub_rn(hv.x, lv.x), hh, rr, ee), w);
+                    const double tB = __dmul_rn(tdiv<DIV>(__dsub_rn(hv.y, lv.y), hh, rr, ee), w);
                     if (first) { SA = tA; SB = tB; first = false; }
                     else { SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB); }
                 }
             }
         }
         const double WA = -SA, WB = -SB;
-        if (a.wrec) {   // adjoint recording of the coupling sum and the values before the phase
+        if (REC) {   // adjoint recording of the coupling sum and the values before the phase
             double* wp = a.wrec + (long long)di * a.g.cs + pt;
             double* pp = a.prec + (long long)di * a.g.cs + pt;
             wp[0] = WA;

@@ -289,12 +289,12 @@ __global__ void __launch_bounds__(32 * kStripWarps, 3) k_phase_strip(StripArgs a
     if (STAGED) cp_async_wait_all();
 }
 
-template <int MODE, bool EXACT, int UNROLL, int MINB>
+template <int MODE, int DIV, int UNROLL, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_phase_pair(PairArgs a, int kf) {
     const int bid = blockIdx.x;
     const int grp = bid % a.ngroups;
     const int rest = bid / a.ngroups;
-    pair_item<MODE, EXACT, UNROLL>(a, kf, grp, rest % a.nchunks, rest / a.nchunks, threadIdx.x, blockDim.x);
+    pair_item<MODE, DIV, UNROLL>(a, kf, grp, rest % a.nchunks, rest / a.nchunks, threadIdx.x, blockDim.x);
 }
 
 
@@ -443,18 +443,19 @@ cudaError_t launch_pair(const smg_handle* h, int mode, int kfilter, cudaStream_t
     }
     a.filter_substep = h->filter_mode == 1;
     const long long blocks = (long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2];
-    const bool exact = h->exact_recip[0] && h->exact_recip[1] && h->exact_recip[2];
+    const int div = std::min(h->exact_recip[0], std::min(h->exact_recip[1], h->exact_recip[2]));
     const unsigned nb = (unsigned)blocks;
-    const int cfg = (exact ? 1 : 0) | (h->pair_unroll >= 2 ? 2 : 0) | (h->pair_minb >= 4 ? 4 : 0);
-#define SMG_PAIR(E, U, M)                                                                \
-    case (E ? 1 : 0) | (U == 2 ? 2 : 0) | (M == 4 ? 4 : 0):                              \
-        if (mode == 0) k_phase_pair<0, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);          \
-        else if (mode == 1) k_phase_pair<1, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);     \
-        else k_phase_pair<2, E, U, M><<<nb, bs, 0, s>>>(a, kfilter);                    \
+    const int cfg = div | (h->pair_unroll >= 2 ? 4 : 0) | (h->pair_minb >= 4 ? 8 : 0);
+#define SMG_PAIR(D, U, M)                                                                \
+    case D | (U == 2 ? 4 : 0) | (M == 4 ? 8 : 0):                                        \
+        if (mode == 0) k_phase_pair<0, D, U, M><<<nb, bs, 0, s>>>(a, kfilter);          \
+        else if (mode == 1) k_phase_pair<1, D, U, M><<<nb, bs, 0, s>>>(a, kfilter);     \
+        else k_phase_pair<2, D, U, M><<<nb, bs, 0, s>>>(a, kfilter);                    \
         break;
     switch (cfg) {
-        SMG_PAIR(true, 1, 3) SMG_PAIR(true, 2, 3) SMG_PAIR(true, 1, 4) SMG_PAIR(true, 2, 4)
-        SMG_PAIR(false, 1, 3) SMG_PAIR(false, 2, 3) SMG_PAIR(false, 1, 4) SMG_PAIR(false, 2, 4)
+        SMG_PAIR(2, 1, 3) SMG_PAIR(2, 2, 3) SMG_PAIR(2, 1, 4) SMG_PAIR(2, 2, 4)
+        SMG_PAIR(1, 1, 3) SMG_PAIR(1, 2, 3) SMG_PAIR(1, 1, 4) SMG_PAIR(1, 2, 4)
+        SMG_PAIR(0, 1, 3) SMG_PAIR(0, 2, 3) SMG_PAIR(0, 1, 4) SMG_PAIR(0, 2, 4)
     }
 #undef SMG_PAIR
     return cudaGetLastError();

@@ -169,6 +169,17 @@ class GpuSolver:
         check(self._L.smg_misfit(self.h, dptr(arr), _lib.C.byref(J)), self.h)
         return J.value
 
+    def adjoint_bytes(self):
+        b = _lib.C.c_int64()
+        check(self._L.smg_adjoint_bytes(self.h, _lib.C.byref(b)), self.h)
+        return b.value
+
+    def adjoint_segment(self):
+        """Checkpoint segment length K of the last forward."""
+        k = _lib.C.c_int64()
+        check(self._L.smg_adjoint_info(self.h, _lib.C.byref(k), None), self.h)
+        return k.value
+
     def adjoint_seed(self, lam):
         arrs = []
         ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()

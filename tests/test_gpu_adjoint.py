@@ -1,10 +1,11 @@
 """Discrete adjoint: dot-product test (linear part), central finite
-differences for the sigma, source and initial-condition gradients, and the
-checkpoint length not changing the result."""
+differences for the sigma, source and initial-condition gradients, the
+checkpoint length not changing the result, and the fused and the two-kernel
+backward sweeps agreeing."""
 import numpy as np
 import pytest
 
-from starmap_b200 import configs, starmap_init
+from starmap_b200 import _lib, configs, starmap_init
 from starmap_b200.batch import _tables
 from starmap_b200.solver import GpuSolver, expm1div, first_step, handle_tables, prepare
 
@@ -28,9 +29,11 @@ def adjoint_problem(n=12, N=3, bc=1, with_source=True, substep=True):
     return S, fs
 
 
-def make_solver(S, fs, T=None):
+def make_solver(S, fs, T=None, fused=1):
     T = T or _tables(S, fs)
-    return GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T)), T
+    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
+    solver.tune(_lib.SMG_TUNE_ADJ_FUSED, fused)
+    return solver, T
 
 
 def run_J(S, fs, T, U0, nsteps, obs):
@@ -58,17 +61,18 @@ def with_sigma(T, S, fs, key, arr):
     return T2
 
 
-def test_dot_product():
+@pytest.mark.parametrize("fused,K", [(1, 4), (0, 4), (1, 9)])
+def test_dot_product(fused, K):
     S, fs = adjoint_problem(with_source=False)
     rng = np.random.default_rng(0)
     nsteps = 9
-    solver, T = make_solver(S, fs)
+    solver, T = make_solver(S, fs, fused=fused)
     try:
         delta = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
         mu = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
         solver.set_state(delta)
         solver.set_dt(fs["dt"])
-        solver.forward(nsteps, 4)
+        solver.forward(nsteps, K)
         Ad = solver.get_state()
         solver.adjoint_seed(mu)
         lam0, _ = solver.backward()
@@ -79,11 +83,11 @@ def test_dot_product():
     assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
 
 
-@pytest.mark.parametrize("bc,substep", [(1, True), (0, False)])
-def test_sigma_source_ic_gradients_vs_central_differences(bc, substep):
+@pytest.mark.parametrize("bc,substep,fused", [(1, True, 1), (0, False, 1), (1, True, 0)])
+def test_sigma_source_ic_gradients_vs_central_differences(bc, substep, fused):
     S, fs = adjoint_problem(bc=bc, substep=substep)
     nsteps = 8
-    solver, T = make_solver(S, fs)
+    solver, T = make_solver(S, fs, fused=fused)
     obs = None
     try:
         solver.set_state(S.U0)
@@ -128,7 +132,7 @@ def test_sigma_source_ic_gradients_vs_central_differences(bc, substep):
 def test_checkpoint_interval_does_not_change_gradient():
     S, fs = adjoint_problem(n=10, N=5)
     res = []
-    for K in (1, 4, 11):
+    for K in (1, 4, 11, 0):
         solver, T = make_solver(S, fs)
         try:
             solver.set_state(S.U0)
@@ -143,3 +147,50 @@ def test_checkpoint_interval_does_not_change_gradient():
     for gU, gF in res[1:]:
         for j in gU:
             np.testing.assert_allclose(gU[j], res[0][0][j], rtol=0, atol=1e-12 * np.abs(res[0][0][j]).max())
+
+
+@pytest.mark.parametrize("bc,substep", [(1, True), (0, True), (1, False)])
+def test_fused_and_split_sweeps_agree(bc, substep):
+    S, fs = adjoint_problem(n=11, N=4, bc=bc, substep=substep)
+    out = {}
+    for fused in (0, 1):
+        solver, T = make_solver(S, fs, fused=fused)
+        try:
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.forward(10, 3)
+            u = solver.get_state([0])[0]
+            solver.misfit(0.7 * u - 0.01)
+            keys = [k for k in T.index if k[0] in ("sT", "sA", "Q")]
+            out[fused] = solver.backward(fields=[T.index[k] for k in keys])
+        finally:
+            solver.close()
+    (gU0, gF0), (gU1, gF1) = out[0], out[1]
+    for j in gU0:
+        np.testing.assert_allclose(gU1[j], gU0[j], rtol=0, atol=1e-12 * max(np.abs(gU0[j]).max(), 1e-300))
+    for k in gF0:
+        a, b = np.asarray(gF0[k]), np.asarray(gF1[k])
+        np.testing.assert_allclose(b, a, rtol=0, atol=1e-12 * max(np.abs(a).max(), 1e-300))
+
+
+def test_backward_reports_device_time_and_repeats():
+    """smg_last_run_stats after forward/backward gives their device time; a
+    second misfit+backward on the same forward gives the same gradient."""
+    S, fs = adjoint_problem(n=10, N=3)
+    solver, T = make_solver(S, fs)
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.forward(6, 0)
+        ms_f, nl_f = solver.last_run_stats()
+        u = solver.get_state([0])[0]
+        solver.misfit(0.5 * u)
+        g1, _ = solver.backward()
+        ms_b, nl_b = solver.last_run_stats()
+        solver.misfit(0.5 * u)
+        g2, _ = solver.backward()
+    finally:
+        solver.close()
+    assert ms_f > 0 and ms_b > 0 and nl_f == 13 and nl_b > 0
+    for j in g1:
+        np.testing.assert_array_equal(g1[j], g2[j])
