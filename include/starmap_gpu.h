@@ -49,11 +49,12 @@ extern "C" {
 #define SMG_ENOMEM     -5   /* device allocation failed */
 #define SMG_ESTATE     -6   /* call out of order (e.g. run before the state is set) */
 
-#define SMG_VARIANT_AUTO    0  /* best available kernel family (pair, else strip); phase A fused (default) */
+#define SMG_VARIANT_AUTO    0  /* best available kernel family (JIT, else pair, else strip); phase A fused (default) */
 #define SMG_VARIANT_GENERIC 1  /* point-per-thread kernels, one launch per half step */
 #define SMG_VARIANT_STRIP   2  /* strip kernels, one launch per half step */
 #define SMG_VARIANT_STAGED  3  /* strip kernels, slot-job loads staged by cp.async; phase A fused */
 #define SMG_VARIANT_PAIR    4  /* two points per thread, destination-centric; phase A fused */
+#define SMG_VARIANT_JIT     5  /* pair layout, kernels generated for this problem and compiled at run time (NVRTC) */
 
 #define SMG_FILTER_NONE    0   /* par.f_position = ''          */
 #define SMG_FILTER_SUBSTEP 1   /* par.f_position = 'substep'   */
@@ -147,6 +148,18 @@ int smg_sync(smg_handle* h);
  * memory.  No reference counterpart (the reference has one CPU code path). */
 int smg_set_variant(smg_handle* h, int32_t variant);
 
+/* The kernel family the next smg_run uses (AUTO resolved; JIT only after it
+ * was compiled: by smg_set_variant(JIT) or by AUTO's first smg_run) and, in
+ * `why` (cap bytes, may be NULL), the reason AUTO could not use JIT. */
+int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
+
+/* The CUDA C++ source of the specialised kernels (SMG_VARIANT_JIT) of problem
+ * p with the given CTA size and destination group; *len receives its length,
+ * buf (cap bytes) a NUL-terminated copy.  compile != 0 also compiles it with
+ * NVRTC for sm_100a (no GPU needed).  No reference counterpart. */
+int smg_jit_source(const smg_problem* p, int32_t block, int32_t group, int32_t compile, char* buf, int64_t cap,
+                   int64_t* len);
+
 /* Tuning parameters of the kernels (no reference counterpart).  They change
  * performance only, never results.  Keys: */
 #define SMG_TUNE_PAIR_GROUP  1   /* destinations per CTA of the pair kernel (1..256) */
@@ -154,6 +167,9 @@ int smg_set_variant(smg_handle* h, int32_t variant);
 #define SMG_TUNE_PAIR_UNROLL 3   /* couplings per inner iteration (1 or 2) */
 #define SMG_TUNE_PAIR_MINB   4   /* register budget: 3 or 4 resident CTAs of 256 threads (64/85 regs) */
 #define SMG_TUNE_ADJ_FUSED   5   /* smg_backward: 1 = one fused kernel per phase (default), 0 = pointwise + transpose kernels */
+#define SMG_TUNE_JIT_BLOCK   6   /* threads per CTA of the generated kernels (32..256, multiple of 32) */
+#define SMG_TUNE_JIT_GROUP   7   /* destinations per CTA of the generated kernels (1..256) */
+#define SMG_TUNE_JIT_REGS    8   /* register limit per thread of the generated kernels (0: compiler's choice, else 32..255) */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the

@@ -27,6 +27,16 @@ SMG_TUNE_PAIR_BLOCK = 2
 SMG_TUNE_PAIR_UNROLL = 3
 SMG_TUNE_PAIR_MINB = 4
 SMG_TUNE_ADJ_FUSED = 5
+SMG_TUNE_JIT_BLOCK = 6
+SMG_TUNE_JIT_GROUP = 7
+SMG_TUNE_JIT_REGS = 8
+
+SMG_VARIANT_AUTO = 0
+SMG_VARIANT_GENERIC = 1
+SMG_VARIANT_STRIP = 2
+SMG_VARIANT_STAGED = 3
+SMG_VARIANT_PAIR = 4
+SMG_VARIANT_JIT = 5
 _NAMES = {SMG_EINVAL: "SMG_EINVAL", SMG_ECUDA: "SMG_ECUDA", SMG_ETIMEOUT: "SMG_ETIMEOUT",
           SMG_ENONFINITE: "SMG_ENONFINITE", SMG_ENOMEM: "SMG_ENOMEM", SMG_ESTATE: "SMG_ESTATE"}
 
@@ -88,6 +98,9 @@ SIGNATURES = {
     "smg_backward": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_double))]),
     "smg_adjoint_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "smg_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "smg_active_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_char_p, C.c_int64]),
+    "smg_jit_source": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int64,
+                                 C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
     "smg_batch_destroy": (None, [C.c_void_p]),
     "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstarmap_gpu.so")
-SOURCES = ["smg_api.cu", "smg_phase.cu", "smg_batch.cu", "smg_norms.cu", "smg_adjoint.cu"]
+SOURCES = ["smg_api.cu", "smg_phase.cu", "smg_batch.cu", "smg_norms.cu", "smg_adjoint.cu", "smg_jit.cu"]
 HEADERS = ["smg_device.cuh", "smg_internal.h", "smg_pair.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -47,7 +47,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
            "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp",
-           *[os.path.join(CSRC, s) for s in SOURCES], *extra]
+           *[os.path.join(CSRC, s) for s in SOURCES], "-ldl", *extra]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -61,9 +61,11 @@ int extent(int n, int bc, int g) { return (g == 2 && bc == 1) ? n + 1 : n; }
 
 void resolve_pair(smg_handle* h, int phase);
 cudaError_t upload_pair(smg_handle* h, int phase, bool alloc);
+int create_impl(const smg_problem* p, smg_handle** out, bool device);
 
 void free_device(smg_handle* h) {
     smg_adjoint_free(h);
+    smg::jit_free(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
     cudaFree(h->dU);
@@ -417,6 +419,7 @@ bool strip_usable(const smg_handle* h) {
 }  // namespace
 
 void smg::set_global_error(const std::string& msg) { fail(nullptr, 0, msg); }
+int smg::create_host(const smg_problem* p, smg_handle** out) { return create_impl(p, out, false); }
 
 extern "C" {
 
@@ -478,7 +481,34 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
     return SMG_OK;
 }
 
-int smg_create(const smg_problem* p, smg_handle** out) {
+int smg_create(const smg_problem* p, smg_handle** out) { return create_impl(p, out, true); }
+
+}  // extern "C"
+
+namespace {
+
+// Breadth-first level of every component in the coupling graph from
+// component 0 (unreached components after the last level).
+std::vector<int> coupling_levels(const smg_handle* h) {
+    const int ns = h->n_sys;
+    std::vector<int> level(ns, -1), queue(1, 0);
+    level[0] = 0;
+    for (size_t qi = 0; qi < queue.size(); ++qi) {
+        const int j = queue[qi];
+        for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
+            const int i = h->coups[q].src;
+            if (level[i] < 0) { level[i] = level[j] + 1; queue.push_back(i); }
+        }
+    }
+    int maxl = 0;
+    for (int j = 0; j < ns; ++j) maxl = std::max(maxl, level[j]);
+    for (int j = 0; j < ns; ++j) if (level[j] < 0) level[j] = maxl + 1;
+    return level;
+}
+
+// smg_create; with device == false only the host tables (no CUDA call), for
+// smg_jit_source on machines without a GPU
+int create_impl(const smg_problem* p, smg_handle** out, bool device) {
     if (!p || !out) return fail(nullptr, SMG_EINVAL, "smg_create: NULL argument");
     *out = nullptr;
     const int ns = p->n_sys;
@@ -603,7 +633,9 @@ int smg_create(const smg_problem* p, smg_handle** out) {
     // slots for array fields
     std::vector<int> slot(nfields, -1);
     int nslots = 0;
+    h->field_is_array.assign(nf, 0);
     for (int f = 0; f < nf; ++f) {
+        h->field_is_array[f] = p->fields[f].data != nullptr;
         h->field_grid[f] = (p->fields[f].grid[0] - 1) | ((p->fields[f].grid[1] - 1) << 1) | ((p->fields[f].grid[2] - 1) << 2);
         if (p->fields[f].data) slot[f] = nslots++;
         h->fields_host[f].s = p->fields[f].scalar;
@@ -627,6 +659,13 @@ int smg_create(const smg_problem* p, smg_handle** out) {
         c.F2 = (p->filter_mode == 1 && p->filter2[j] >= 0) ? p->filter2[j] : h->field_one;
     }
 
+    if (!device) {
+        const std::vector<int> level = coupling_levels(h);
+        reciprocals(h);
+        for (int ph = 0; ph < 2; ++ph) build_pair(h, ph, level);
+        *out = h;
+        return SMG_OK;
+    }
     // device allocations
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -683,18 +722,7 @@ int smg_create(const smg_problem* p, smg_handle** out) {
     CREATE_CUDA(cudaMemcpyAsync(h->dFieldTab, h->fields_host.data(), sizeof(DevField) * nfields, cudaMemcpyHostToDevice, h->stream));
     // strip-kernel schedules: stage = breadth-first level of the coupling graph
     {
-        std::vector<int> level(ns, -1), queue(1, 0);
-        level[0] = 0;
-        for (size_t qi = 0; qi < queue.size(); ++qi) {
-            const int j = queue[qi];
-            for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
-                const int i = h->coups[q].src;
-                if (level[i] < 0) { level[i] = level[j] + 1; queue.push_back(i); }
-            }
-        }
-        int maxl = 0;
-        for (int j = 0; j < ns; ++j) maxl = std::max(maxl, level[j]);
-        for (int j = 0; j < ns; ++j) if (level[j] < 0) level[j] = maxl + 1;
+        const std::vector<int> level = coupling_levels(h);
         build_schedule(h, 0, level);
         build_schedule(h, 1, level);
         for (int ph = 0; ph < 2; ++ph) {
@@ -721,6 +749,10 @@ int smg_create(const smg_problem* p, smg_handle** out) {
     *out = h;
     return SMG_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 void smg_destroy(smg_handle* h) {
     if (!h) return;
@@ -807,12 +839,17 @@ static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, 
     int64_t L = 0;
     // AUTO runs the pair kernel when its tables exist (measured fastest on the
     // 820-moment lattice workload), else the strip kernel, else the generic one
-    const bool pair = (h->variant == SMG_VARIANT_PAIR || h->variant == SMG_VARIANT_AUTO) && h->pair[0].ok && h->pair[1].ok;
-    const bool strip = !pair && strip_usable(h);
-    const bool fuse = ((strip && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_STAGED)) || pair) &&
+    const bool jit = h->jit && (h->variant == SMG_VARIANT_JIT || h->variant == SMG_VARIANT_AUTO);
+    const bool pair = !jit && (h->variant == SMG_VARIANT_PAIR || h->variant == SMG_VARIANT_AUTO) && h->pair[0].ok &&
+                      h->pair[1].ok;
+    const bool strip = !jit && !pair && strip_usable(h);
+    const bool fuse = ((strip && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_STAGED)) || pair || jit) &&
                       h->filter_mode != SMG_FILTER_FULL;
     const bool hasA = !h->destA.empty();
-    auto ph = [&](int mode, int kf) { return pair ? smg::launch_pair(h, mode, kf, s) : smg::launch_strip(h, mode, kf, s); };
+    auto ph = [&](int mode, int kf) {
+        if (jit) return smg::launch_jit(h, mode, kf, s);
+        return pair ? smg::launch_pair(h, mode, kf, s) : smg::launch_strip(h, mode, kf, s);
+    };
     if (fuse && nsteps >= 1) {
         if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; ++L; }
         for (int64_t k = 0; k < nsteps; ++k) {
@@ -828,7 +865,12 @@ static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, 
         return cudaSuccess;
     }
     for (int64_t k = 0; k < nsteps; ++k) {
-        if (strip) {
+        if (jit) {
+            if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; ++L; }
+            if ((e = ph(1, 0)) != cudaSuccess) return e;
+            ++L;
+            if (hasA) { if ((e = ph(0, 2)) != cudaSuccess) return e; ++L; }
+        } else if (strip) {
             if (hasA) { if ((e = smg::launch_strip(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
             if ((e = smg::launch_strip(h, 1, 0, s)) != cudaSuccess) return e;
             ++L;
@@ -862,6 +904,19 @@ int smg_run(smg_handle* h, int64_t nsteps) {
 // handle's timing events (smg_last_run_stats)
 int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
     const int64_t kBlock = 64;   // steps per captured graph
+    if (h->variant == SMG_VARIANT_AUTO && !h->jit && !h->jit_failed && nsteps > 0) {
+        // first run: generate and compile the specialised kernels; without
+        // NVRTC (or for tables beyond 32-bit offsets) AUTO keeps the pair kernel
+        std::string why;
+        if (smg::jit_build(h, why) != SMG_OK) {
+            h->jit_failed = true;
+            h->jit_err = why;
+        } else if (h->graph) {
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+            h->graph_steps = 0;
+        }
+    }
     int64_t left = nsteps;
     if (left >= kBlock) {
         if (!h->graph || h->graph_steps != kBlock) {
@@ -912,6 +967,24 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             if (value != 3 && value != 4) return fail(h, SMG_EINVAL, "smg_tune: minb must be 3 or 4");
             h->pair_minb = value;
             break;
+        case SMG_TUNE_JIT_BLOCK:
+            if (value < 32 || value > 256 || value % 32) return fail(h, SMG_EINVAL, "smg_tune: jit block must be 32..256, x32");
+            h->jit_block = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_GROUP:
+            if (value < 1 || value > 256) return fail(h, SMG_EINVAL, "smg_tune: jit group must be 1..256");
+            h->jit_group = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_REGS:
+            if (value != 0 && (value < 32 || value > 255)) return fail(h, SMG_EINVAL, "smg_tune: jit regs must be 0 or 32..255");
+            h->jit_regs = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
         case SMG_TUNE_ADJ_FUSED:
             if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj_fused must be 0 or 1");
             h->adj_fused = value;
@@ -927,10 +1000,32 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
     return SMG_OK;
 }
 
+int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap) {
+    if (!h || !variant) return fail(h, SMG_EINVAL, "smg_active_variant: NULL argument");
+    int v;
+    if (h->jit && (h->variant == SMG_VARIANT_JIT || h->variant == SMG_VARIANT_AUTO)) v = SMG_VARIANT_JIT;
+    else if ((h->variant == SMG_VARIANT_PAIR || h->variant == SMG_VARIANT_AUTO) && h->pair[0].ok && h->pair[1].ok)
+        v = SMG_VARIANT_PAIR;
+    else if (strip_usable(h)) v = h->strip_staged ? SMG_VARIANT_STAGED : SMG_VARIANT_STRIP;
+    else v = SMG_VARIANT_GENERIC;
+    *variant = v;
+    if (why && cap > 0) {
+        const size_t n = std::min<size_t>((size_t)cap - 1, h->jit_err.size());
+        std::memcpy(why, h->jit_err.data(), n);
+        why[n] = '\0';
+    }
+    return SMG_OK;
+}
+
 int smg_set_variant(smg_handle* h, int32_t variant) {
     if (!h) return fail(h, SMG_EINVAL, "smg_set_variant: NULL handle");
-    if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_PAIR)
+    if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_JIT)
         return fail(h, SMG_EINVAL, "smg_set_variant: unknown variant");
+    if (variant == SMG_VARIANT_JIT && !h->jit) {
+        std::string why;
+        const int rc = smg::jit_build(h, why);
+        if (rc != SMG_OK) return fail(h, rc, "smg_set_variant: specialised kernels unavailable: " + why);
+    }
     if ((variant == SMG_VARIANT_STRIP || variant == SMG_VARIANT_STAGED) && !(h->sched[0].ok && h->sched[1].ok))
         return fail(h, SMG_EINVAL, "smg_set_variant: strip schedule does not fit in shared memory");
     if (variant == SMG_VARIANT_PAIR && !(h->pair[0].ok && h->pair[1].ok))

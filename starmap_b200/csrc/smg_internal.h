@@ -9,8 +9,11 @@
 
 #include "smg_device.cuh"
 
+struct smg_problem;
+
 namespace smg {
 struct AdjData;
+struct JitState;
 }
 
 struct smg_handle {
@@ -23,6 +26,7 @@ struct smg_handle {
     std::vector<int> destA, destB;   // outer set (phase A), inner set (phase B)
     std::vector<smg::DevField> fields_host;  // device view of the field table
     std::vector<int> field_grid;     // packed grid type of each field (for uploads)
+    std::vector<char> field_is_array;  // per user field: array (1) or scalar (0), fixed at creation
     std::vector<int> sigma_t_field, decay_t_field;   // per component
     std::vector<int> derived_decay;  // field index -> decay field computed on device (or -1)
     int sigma_a = -1, decay_a = -1, derived_decay_a = -1;
@@ -85,6 +89,10 @@ struct smg_handle {
     bool strip_staged = false;       // stage slot-job loads with cp.async
     smg::AdjData* adj = nullptr;     // adjoint checkpoints and buffers (smg_forward)
     int adj_fused = 1;               // smg_backward kernel form (SMG_TUNE_ADJ_FUSED)
+    smg::JitState* jit = nullptr;    // problem-specialised kernels (SMG_VARIANT_JIT)
+    int jit_block = 64, jit_group = 4, jit_regs = 64;
+    bool jit_failed = false;         // AUTO tried the JIT and it was unavailable
+    std::string jit_err;
 };
 
 void smg_adjoint_free(smg_handle* h);   // smg_adjoint.cu
@@ -102,6 +110,12 @@ constexpr int kSumsqBlocks = 32;     // CTAs per component in the sum-of-squares
 constexpr int kSumsqThreads = 256;
 void set_global_error(const std::string& msg);   // message of smg_last_error(NULL)
 int run_steps(smg_handle* h, int64_t nsteps, bool events);   // smg_run without argument checks
+int jit_build(smg_handle* h, std::string& err);             // generate, compile, load (SMG_OK or error)
+void jit_free(smg_handle* h);
+cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
+std::string jit_source(const smg_handle* h, int block, int group);
+int jit_compile_link(const std::vector<std::string>& programs, int regs, std::vector<char>& cubin, std::string& err);
+int create_host(const smg_problem* p, smg_handle** out);   // host tables only (no CUDA call)
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);
 constexpr int kMaxStripSmem = 200 * 1024;

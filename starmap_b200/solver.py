@@ -134,6 +134,13 @@ class GpuSolver:
     def set_dt(self, dt):
         check(self._L.smg_set_dt(self.h, float(dt)), self.h)
 
+    def active_variant(self):
+        """(kernel family the next run uses, reason AUTO could not use JIT)."""
+        v = _lib.C.c_int32()
+        why = _lib.C.create_string_buffer(512)
+        check(self._L.smg_active_variant(self.h, _lib.C.byref(v), why, 512), self.h)
+        return v.value, why.value.decode()
+
     def set_variant(self, variant):
         check(self._L.smg_set_variant(self.h, int(variant)), self.h)
 
@@ -234,6 +241,21 @@ class GpuSolver:
 
 def C_cast_fields(fa):
     return _lib.C.cast(fa, _lib.C.POINTER(_lib.smg_field))
+
+
+def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay_t=None, decay_a=-1,
+               filter_mode=FILTER_NONE, filter1=None, filter2=None, block=64, group=8, compile=False):
+    """CUDA C++ source of the problem's specialised kernels (SMG_VARIANT_JIT);
+    with compile=True also compiled by NVRTC for sm_100a (no GPU needed)."""
+    L = _lib.lib()
+    p, keep, _ = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
+                               decay_t, decay_a, filter_mode, filter1, filter2)
+    ln = _lib.C.c_int64()
+    check(L.smg_jit_source(_lib.C.byref(p), int(block), int(group), 0, None, 0, _lib.C.byref(ln)))
+    buf = _lib.C.create_string_buffer(ln.value + 1)
+    check(L.smg_jit_source(_lib.C.byref(p), int(block), int(group), int(bool(compile)), buf, ln.value + 1,
+                           _lib.C.byref(ln)))
+    return buf.value.decode()
 
 
 def build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,

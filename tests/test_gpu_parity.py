@@ -32,7 +32,7 @@ def compare(out_gpu, out_ref):
     return worst, mism
 
 
-VARIANTS = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4}
+VARIANTS = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4, "jit": 5}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -125,7 +125,7 @@ def test_variants_agree_on_c1_linesource():
     from starmap_b200.solver import setup_gpu
     par = starmap_init(configs.linesource())
     outs = []
-    for v in (0, 1, 2, 3, 4):
+    for v in (0, 1, 2, 3, 4, 5):
         S, fs, solver, T = setup_gpu(par)
         try:
             solver.set_variant(v)
@@ -140,6 +140,48 @@ def test_variants_agree_on_c1_linesource():
         np.testing.assert_array_equal(outs[0][j], outs[2][j])
         np.testing.assert_array_equal(outs[0][j], outs[3][j])
         np.testing.assert_array_equal(outs[0][j], outs[4][j])
+        np.testing.assert_array_equal(outs[0][j], outs[5][j])
+
+
+def test_auto_runs_the_specialised_kernels():
+    """On a B200 with NVRTC, AUTO compiles and runs the generated kernels."""
+    from starmap_b200 import configs
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(configs.linesource())
+    S, fs, solver, T = setup_gpu(par)
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.run(3)
+        v, why = solver.active_variant()
+    finally:
+        solver.close()
+    assert v == 5, why
+
+
+@pytest.mark.parametrize("block,group", [(32, 1), (128, 3), (256, 64)])
+def test_jit_tuning_keeps_results(block, group):
+    from starmap_b200 import _lib
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(cases.odd_mixed_bc())
+    outs = []
+    for tune in (False, True):
+        S, fs, solver, T = setup_gpu(par)
+        try:
+            if tune:
+                solver.tune(_lib.SMG_TUNE_JIT_BLOCK, block)
+                solver.tune(_lib.SMG_TUNE_JIT_GROUP, group)
+                solver.set_variant(5)
+            else:
+                solver.set_variant(4)
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.run(7)
+            outs.append(solver.get_state())
+        finally:
+            solver.close()
+    for j in outs[0]:
+        np.testing.assert_array_equal(outs[0][j], outs[1][j])
 
 
 def test_gpu_pn_equals_spn_boxes():
