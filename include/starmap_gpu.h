@@ -154,11 +154,12 @@ int smg_set_variant(smg_handle* h, int32_t variant);
 int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
 
 /* The CUDA C++ source of the specialised kernels (SMG_VARIANT_JIT) of problem
- * p with the given CTA size and destination group; *len receives its length,
- * buf (cap bytes) a NUL-terminated copy.  compile != 0 also compiles it with
- * NVRTC for sm_100a (no GPU needed).  No reference counterpart. */
-int smg_jit_source(const smg_problem* p, int32_t block, int32_t group, int32_t compile, char* buf, int64_t cap,
-                   int64_t* len);
+ * p, generated with the SMG_TUNE_JIT_* settings keys[i] = values[i] (ntune of
+ * them; defaults otherwise); *len receives its length, buf (cap bytes) a
+ * NUL-terminated copy.  compile != 0 also compiles it with NVRTC for sm_100a
+ * (no GPU needed).  No reference counterpart. */
+int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune, int32_t compile,
+                   char* buf, int64_t cap, int64_t* len);
 
 /* Tuning parameters of the kernels (no reference counterpart).  They change
  * performance only, never results.  Keys: */
@@ -170,6 +171,10 @@ int smg_jit_source(const smg_problem* p, int32_t block, int32_t group, int32_t c
 #define SMG_TUNE_JIT_BLOCK   6   /* threads per CTA of the generated kernels (32..256, multiple of 32) */
 #define SMG_TUNE_JIT_GROUP   7   /* destinations per CTA of the generated kernels (1..256) */
 #define SMG_TUNE_JIT_REGS    8   /* register limit per thread of the generated kernels (0: compiler's choice, else 32..255) */
+#define SMG_TUNE_JIT_SPLIT   9   /* groups per separately compiled program (1..64; 0: one per phase) */
+#define SMG_TUNE_JIT_CALLS  10   /* 0: one kernel per program, the kernels of a phase run concurrently (default);
+                                    1: one kernel per phase calling the separately compiled groups */
+#define SMG_TUNE_JIT_XPAIR  11   /* x differences: 0 = four 64-bit loads per point pair, 1 = two aligned 128-bit loads */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the

@@ -30,6 +30,9 @@ SMG_TUNE_ADJ_FUSED = 5
 SMG_TUNE_JIT_BLOCK = 6
 SMG_TUNE_JIT_GROUP = 7
 SMG_TUNE_JIT_REGS = 8
+SMG_TUNE_JIT_SPLIT = 9
+SMG_TUNE_JIT_CALLS = 10
+SMG_TUNE_JIT_XPAIR = 11
 
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1
@@ -99,8 +102,8 @@ SIGNATURES = {
     "smg_adjoint_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "smg_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_active_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_char_p, C.c_int64]),
-    "smg_jit_source": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int64,
-                                 C.POINTER(C.c_int64)]),
+    "smg_jit_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32,
+                                 C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
     "smg_batch_destroy": (None, [C.c_void_p]),
     "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),

@@ -846,30 +846,32 @@ static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, 
     const bool fuse = ((strip && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_STAGED)) || pair || jit) &&
                       h->filter_mode != SMG_FILTER_FULL;
     const bool hasA = !h->destA.empty();
+    // one phase; L counts its kernels (the generated code may use several)
     auto ph = [&](int mode, int kf) {
-        if (jit) return smg::launch_jit(h, mode, kf, s);
+        if (jit) {
+            L += smg::jit_launches(h, mode == 1 ? 1 : 0);
+            return smg::launch_jit(h, mode, kf, s);
+        }
+        ++L;
         return pair ? smg::launch_pair(h, mode, kf, s) : smg::launch_strip(h, mode, kf, s);
     };
     if (fuse && nsteps >= 1) {
-        if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; ++L; }
+        if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; }
         for (int64_t k = 0; k < nsteps; ++k) {
             if ((e = ph(1, 0)) != cudaSuccess) return e;
-            ++L;
             if (!hasA) continue;
             if (k + 1 < nsteps) e = ph(2, 0);
             else e = ph(0, 2);
             if (e != cudaSuccess) return e;
-            ++L;
         }
         if (launches) *launches = L;
         return cudaSuccess;
     }
     for (int64_t k = 0; k < nsteps; ++k) {
         if (jit) {
-            if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; ++L; }
+            if (hasA) { if ((e = ph(0, 1)) != cudaSuccess) return e; }
             if ((e = ph(1, 0)) != cudaSuccess) return e;
-            ++L;
-            if (hasA) { if ((e = ph(0, 2)) != cudaSuccess) return e; ++L; }
+            if (hasA) { if ((e = ph(0, 2)) != cudaSuccess) return e; }
         } else if (strip) {
             if (hasA) { if ((e = smg::launch_strip(h, 0, 1, s)) != cudaSuccess) return e; ++L; }
             if ((e = smg::launch_strip(h, 1, 0, s)) != cudaSuccess) return e;
@@ -982,6 +984,24 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
         case SMG_TUNE_JIT_REGS:
             if (value != 0 && (value < 32 || value > 255)) return fail(h, SMG_EINVAL, "smg_tune: jit regs must be 0 or 32..255");
             h->jit_regs = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_SPLIT:
+            if (value < 0 || value > 64) return fail(h, SMG_EINVAL, "smg_tune: jit split must be 0..64");
+            h->jit_split = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_CALLS:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: jit calls must be 0 or 1");
+            h->jit_calls = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_XPAIR:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: jit xpair must be 0 or 1");
+            h->jit_xpair = value;
             smg::jit_free(h);
             h->jit_failed = false;
             break;

@@ -91,6 +91,9 @@ struct smg_handle {
     int adj_fused = 1;               // smg_backward kernel form (SMG_TUNE_ADJ_FUSED)
     smg::JitState* jit = nullptr;    // problem-specialised kernels (SMG_VARIANT_JIT)
     int jit_block = 64, jit_group = 4, jit_regs = 64;
+    int jit_split = 16;              // groups per NVRTC program (0: one program per phase)
+    int jit_calls = 0;               // 1: one kernel per phase calling separately compiled groups
+    int jit_xpair = 0;               // x differences from aligned 128-bit pairs (1) or 64-bit loads (0)
     bool jit_failed = false;         // AUTO tried the JIT and it was unavailable
     std::string jit_err;
 };
@@ -114,7 +117,8 @@ int jit_build(smg_handle* h, std::string& err);             // generate, compile
 void jit_free(smg_handle* h);
 cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
 std::string jit_source(const smg_handle* h, int block, int group);
-int jit_compile_link(const std::vector<std::string>& programs, int regs, std::vector<char>& cubin, std::string& err);
+int jit_compile(const smg_handle* h, int block, int group, std::string& err);   // compile only (no device)
+int jit_launches(const smg_handle* h, int phase);                                 // kernels per phase
 int create_host(const smg_problem* p, smg_handle** out);   // host tables only (no CUDA call)
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);

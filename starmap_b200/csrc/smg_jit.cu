@@ -255,6 +255,28 @@ std::string coef_decl(const smg_handle* h, int f, const char* n) {
 std::string cx(const smg_handle* h, int f, const char* n) { return is_array(h, f) ? std::string(n) + ".x" : n; }
 std::string cy(const smg_handle* h, int f, const char* n) { return is_array(h, f) ? std::string(n) + ".y" : n; }
 
+// Interior form of the x stencil for a source of grid type g2 (1 or 2 along
+// x): pattern A is (hi, lo) = (p, p-1), pattern B (p+1, p).
+bool xpattern_a(int g2, int bc) { return g2 == 0 ? bc == 1 : bc == 0; }
+
+// Thread condition under which both points of the pair follow the interior
+// form and the extra 128-bit load stays inside the padded row:
+//   g2=0 bc=1 (A): 1 <= p <= n-1 for both points, load at x0-2 >= 0
+//   g2=1 bc=0 (A): p >= 1, load at x0-2 >= 0
+//   g2=0 bc=0 (B): p+1 <= n-1 for both points, load up to x0+3 < s1
+//   g2=1 bc=1 (B): every p; load up to x0+3 < s1
+// (a second point outside the destination's extent is computed but unused)
+std::string xfast_cond(const smg_handle* h, int g2) {
+    const int n = h->g.n[0], bc = h->g.bc[0];
+    const long long s1 = h->g.s1;
+    char b[160];
+    if (g2 == 0 && bc == 1) std::snprintf(b, sizeof b, "(x0 >= 2 && x0 + 1 <= %d)", n - 1);
+    else if (g2 == 1 && bc == 0) std::snprintf(b, sizeof b, "(x0 >= 2)");
+    else if (g2 == 0 && bc == 0) std::snprintf(b, sizeof b, "(x0 + 2 <= %d && x0 + 3 < %lld)", n - 1, s1);
+    else std::snprintf(b, sizeof b, "(x0 + 3 < %lld)", s1);
+    return b;
+}
+
 // One destination's block.  Update modes: 0 one substep with filter kf;
 // 1 two substeps (phase B: F1 then F2); 2 fused A(k=2) A(k=1) (F2 then F1).
 // Phase A blocks carry modes 0 and 2 (chosen by `mode` at run time), phase B
@@ -280,7 +302,6 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
     o += b;
     // the x stencil of the second point is evaluated only inside the extent
     if (!v1_always) o += "        const bool v1 = x1 < " + std::to_string(c.ext[0]) + ";\n";
-    const std::string sel1 = v1_always ? "" : "v1 ? ", sel2 = v1_always ? "" : " : 0";
     const Coefs f = coefs_of(h, phase, j);
     const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
     o += "        " + coef_decl(h, f.q, "q") + coef_decl(h, f.s, "s") + coef_decl(h, f.E, "E") + "\n";
@@ -296,7 +317,8 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
         const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
         const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
         first = false;
-        if (a == 0) {
+        if (a == 0 && !h->jit_xpair) {
+            // four 64-bit loads at the thread's stencil offsets
             std::snprintf(b, sizeof b,
                           "        { const double* S = Up + %lld;\n"
                           "          const double a0 = ld1(S + hx0_%d), b0 = ld1(S + lx0_%d), a1 = ld1(S + (%shx1_%d%s)), "
@@ -304,8 +326,30 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
                           "          const double tA = __dmul_rn(%s(__dsub_rn(a0, b0), %s, %s), %s);\n"
                           "          const double tB = __dmul_rn(%s(__dsub_rn(a1, b1), %s, %s), %s);\n"
                           "          %s }\n",
-                          so, g2, g2, sel1.c_str(), g2, sel2.c_str(), sel1.c_str(), g2, sel2.c_str(), dv, H.c_str(),
-                          RH.c_str(), W.c_str(), dv, H.c_str(), RH.c_str(), W.c_str(), fold);
+                          so, g2, g2, v1_always ? "" : "v1 ? ", g2, v1_always ? "" : " : 0", v1_always ? "" : "v1 ? ",
+                          g2, v1_always ? "" : " : 0", dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(), RH.c_str(),
+                          W.c_str(), fold);
+        } else if (a == 0) {
+            // interior: the three values a point pair needs from two aligned
+            // 128-bit loads (pattern A: p-1, p, p+1 -> loads at x0-2 and x0;
+            // pattern B: x0, x0+1, x0+2 -> loads at x0 and x0+2); threads
+            // where the stencil is not the interior one (xf_g2 false) use it
+            const bool patA = xpattern_a(g2, g.bc[0]);
+            const std::string fast = patA
+                ? "const double2 P = ld2(S), Q = ld2(S - 2); a0 = P.x; b0 = Q.y; a1 = P.y; b1 = P.x;"
+                : "const double2 P = ld2(S), R = ld2(S + 2); a0 = P.y; b0 = P.x; a1 = R.x; b1 = P.y;";
+            std::snprintf(b, sizeof b,
+                          "        { const double* S = Up + %lld; double a0, b0, a1, b1;\n"
+                          "          if (xf_%d) { %s }\n"
+                          "          else { int hi, lo; stencil(x0, %d, %d, %d, hi, lo); a0 = ld1(S + (hi - x0)); "
+                          "b0 = ld1(S + (lo - x0));\n"
+                          "                 if (%s) { stencil(x1, %d, %d, %d, hi, lo); a1 = ld1(S + (hi - x0)); "
+                          "b1 = ld1(S + (lo - x0)); } else { a1 = b1 = 0.0; } }\n"
+                          "          const double tA = __dmul_rn(%s(__dsub_rn(a0, b0), %s, %s), %s);\n"
+                          "          const double tB = __dmul_rn(%s(__dsub_rn(a1, b1), %s, %s), %s);\n"
+                          "          %s }\n",
+                          so, g2, fast.c_str(), g.n[0], g.bc[0], g2, v1_always ? "true" : "v1", g.n[0], g.bc[0], g2,
+                          dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(), RH.c_str(), W.c_str(), fold);
         } else {
             const char* n = a == 1 ? "y" : "z";
             std::snprintf(b, sizeof b,
@@ -355,11 +399,14 @@ const char* kGroupArgs =
     "(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, int y, int z)";
 
 // device function of one group: the thread's stencil offsets, then the blocks
-void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group) {
+// (inl: a function inlined into the dispatch kernel of the same program;
+// otherwise an external function called from it)
+void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group, bool inl) {
     const smg::DevGrid& g = h->g;
     char b[1024];
     const int d0 = k * group, d1 = std::min<int>((k + 1) * group, (int)D.size());
-    o += "extern \"C\" __device__ __noinline__ void " + group_name(phase, k) + kGroupArgs + " {\n";
+    o += std::string(inl ? "static __device__ __forceinline__ void " : "extern \"C\" __device__ __noinline__ void ") +
+         group_name(phase, k) + kGroupArgs + " {\n";
     std::snprintf(b, sizeof b,
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
@@ -370,7 +417,9 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
     bool used[3] = {false, false, false};
     for (int i = d0; i < d1; ++i)
         for (int q = h->comps[D[i]].cbeg; q < h->comps[D[i]].cend; ++q) used[h->coups[q].code >> 1] = true;
-    if (used[0])
+    if (used[0] && h->jit_xpair)
+        for (int g2 = 0; g2 < 2; ++g2) o += "    const bool xf_" + std::to_string(g2) + " = " + xfast_cond(h, g2) + ";\n";
+    if (used[0] && !h->jit_xpair)
         for (int g2 = 0; g2 < 2; ++g2) {
             std::snprintf(b, sizeof b,
                           "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
@@ -397,28 +446,32 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
     o += "}\n";
 }
 
-// dispatch kernel of one phase type: CTA -> (group, row, chunk); calls the group
-void emit_dispatch(std::string& o, const smg_handle* h, int phase, int ngroups, int block) {
+// kernel over groups [k0, k1) of one phase type: CTA -> (group, row, chunk),
+// then the group's code (inlined, or a call when the groups are compiled
+// separately)
+void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k1, int block, bool inl,
+                   const std::string& name) {
     const smg::DevGrid& g = h->g;
     const int tpr = (g.B[0] + 1) / 2;
     const int nchunks = (tpr + block - 1) / block;
     const long long per = (long long)nchunks * g.B[1] * g.B[2];
     char b[1024];
-    for (int k = 0; k < ngroups; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + kGroupArgs + ";\n";
+    if (!inl)
+        for (int k = k0; k < k1; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + kGroupArgs + ";\n";
     std::snprintf(b, sizeof b,
-                  "extern \"C\" __global__ void __launch_bounds__(%d) smg_jit_p%d(double* __restrict__ U, "
+                  "extern \"C\" __global__ void __launch_bounds__(%d) %s(double* __restrict__ U, "
                   "const DevField* __restrict__ F, double hdt, int kf, int mode) {\n"
                   "    const int bid = blockIdx.x;\n"
-                  "    const int grp = bid / %lld;\n"
-                  "    const int rest = bid - grp * %lld;\n"
+                  "    const int grp = %d + bid / %lld;\n"
+                  "    const int rest = bid %% %lld;\n"
                   "    const int row = rest / %d, chunk = rest - row * %d;\n"
                   "    const int y = row %% %d, z = row / %d;\n"
                   "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
                   "    if (x0 >= %d) return;\n"
                   "    switch (grp) {\n",
-                  block, phase, per, per, nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
+                  block, name.c_str(), k0, per, per, nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
     o += b;
-    for (int k = 0; k < ngroups; ++k)
+    for (int k = k0; k < k1; ++k)
         o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z); break;\n";
     o += "    default: break;\n    }\n}\n";
 }
@@ -431,35 +484,68 @@ std::vector<int> phase_dests(const smg_handle* h, int phase) {
     return D;
 }
 
-// The programs of one handle: [0] the dispatch kernels, then the group
-// functions, `per` groups per program.
-std::vector<std::string> programs(const smg_handle* h, int block, int group, int per) {
-    std::vector<std::string> P;
-    std::string disp = kPrelude;
-    std::vector<std::string> fns;
+// One generated kernel: its program, phase type, name and CTA count.
+struct KernelSrc {
+    std::string src, name;
+    int phase;
+    long long grid;
+};
+
+// The generated code of one handle.
+//   calls: [0] one dispatch kernel per phase type, then the group functions,
+//          `per` groups per program, compiled as relocatable code and linked
+//          (one launch per phase; each group is entered by a call);
+//   inline (calls false): `per` groups per program (0: all of the phase),
+//          each program one kernel over its groups with their code inlined;
+//          the kernels of a phase run concurrently.
+std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int per, bool calls) {
+    const smg::DevGrid& g = h->g;
+    const int tpr = (g.B[0] + 1) / 2;
+    const long long cta_per_group = (long long)((tpr + block - 1) / block) * g.B[1] * g.B[2];
+    std::vector<KernelSrc> P;
+    if (calls) {
+        KernelSrc disp{kPrelude, "", -1, 0};
+        std::vector<std::string> fns;
+        for (int phase = 0; phase < 2; ++phase) {
+            const std::vector<int> D = phase_dests(h, phase);
+            if (D.empty()) continue;
+            const int ng = ((int)D.size() + group - 1) / group;
+            for (int k = 0; k < ng; ++k) {
+                std::string s;
+                emit_group(s, h, phase, k, D, group, false);
+                fns.push_back(std::move(s));
+            }
+            emit_dispatch(disp.src, h, phase, 0, ng, block, false, "smg_jit_p" + std::to_string(phase));
+        }
+        P.push_back(std::move(disp));
+        const size_t step = per > 0 ? (size_t)per : fns.size();
+        for (size_t i = 0; i < fns.size(); i += step) {
+            KernelSrc k{kPrelude, "", -1, 0};
+            for (size_t j = i; j < std::min(fns.size(), i + step); ++j) k.src += fns[j];
+            P.push_back(std::move(k));
+        }
+        return P;
+    }
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
         if (D.empty()) continue;
         const int ng = ((int)D.size() + group - 1) / group;
-        emit_dispatch(disp, h, phase, ng, block);
-        for (int k = 0; k < ng; ++k) {
-            std::string s;
-            emit_group(s, h, phase, k, D, group);
-            fns.push_back(std::move(s));
+        const int step = per > 0 ? per : ng;
+        for (int k0 = 0; k0 < ng; k0 += step) {
+            const int k1 = std::min(ng, k0 + step);
+            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
+                        (long long)(k1 - k0) * cta_per_group};
+            for (int j = k0; j < k1; ++j) emit_group(k.src, h, phase, j, D, group, true);
+            emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name);
+            P.push_back(std::move(k));
         }
-    }
-    P.push_back(std::move(disp));
-    for (size_t i = 0; i < fns.size(); i += per) {
-        std::string s = kPrelude;
-        for (size_t k = i; k < std::min(fns.size(), i + per); ++k) s += fns[k];
-        P.push_back(std::move(s));
     }
     return P;
 }
 
 // regs > 0: register limit per thread of every function (--maxrregcount);
 // the linked kernel's count is the maximum over its call graph
-int compile_one(const std::string& src, int regs, std::vector<char>& cubin, std::string& err) {
+int compile_one(const std::string& src, int regs, bool rdc, std::vector<char>& cubin, std::string& err) {
     Api& a = api();
     nvrtcProgram_t prog = nullptr;
     nvrtcResult_t r = a.CreateProgram(&prog, src.c_str(), "smg_jit.cu", 0, nullptr, nullptr);
@@ -468,8 +554,8 @@ int compile_one(const std::string& src, int regs, std::vector<char>& cubin, std:
         return SMG_ECUDA;
     }
     const std::string rr = "--maxrregcount=" + std::to_string(regs);
-    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false", "--relocatable-device-code=true",
-                          rr.c_str()};
+    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
+                          rdc ? "--relocatable-device-code=true" : "--relocatable-device-code=false", rr.c_str()};
     r = a.CompileProgram(prog, regs > 0 ? 5 : 4, opts);
     if (r != 0) {
         size_t n = 0;
@@ -488,37 +574,21 @@ int compile_one(const std::string& src, int regs, std::vector<char>& cubin, std:
     return SMG_OK;
 }
 
-std::map<std::string, std::vector<char>> g_cubins;   // joined sources -> linked cubin, process-wide
+std::map<std::string, std::vector<std::vector<char>>> g_cubins;   // sources -> cubins, process-wide
 std::mutex g_cubin_mu;
 
-}  // namespace
-
-namespace smg {
-
-struct JitState {
-    CUmodule_t mod = nullptr;
-    CUfunction_t fn[2] = {nullptr, nullptr};   // dispatch kernel per phase type
-    int block = 64, group = 8;
-    long long grid[2] = {0, 0};
-};
-
-std::string jit_source(const smg_handle* h, int block, int group) {
-    std::string o;
-    int i = 0;
-    for (const std::string& s : programs(h, block, group, 4)) o += "// ---- program " + std::to_string(i++) + "\n" + s;
-    return o;
-}
-
-// Compile the programs on all host threads and link them into one sm_100a
-// cubin (cached per process by source text).
-int jit_compile_link(const std::vector<std::string>& P, int regs, std::vector<char>& cubin, std::string& err) {
-    std::string key = "regs " + std::to_string(regs) + "\n";
-    for (const auto& s : P) key += s;
+// Compile the programs on all host threads; for the calls layout link them
+// into one cubin, for the inline layout keep one cubin per program.  Cached
+// per process by source text and options.
+int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std::vector<std::vector<char>>& out,
+                     std::string& err) {
+    std::string key = "regs " + std::to_string(regs) + (calls ? " calls\n" : " inline\n");
+    for (const auto& k : P) key += k.src;
     {
         std::lock_guard<std::mutex> lk(g_cubin_mu);
         auto it = g_cubins.find(key);
         if (it != g_cubins.end()) {
-            cubin = it->second;
+            out = it->second;
             return SMG_OK;
         }
     }
@@ -527,7 +597,8 @@ int jit_compile_link(const std::vector<std::string>& P, int regs, std::vector<ch
         err = a.why;
         return SMG_EINVAL;
     }
-    if (!a.link_ok) {
+    const bool link = calls && P.size() > 1;
+    if (link && !a.link_ok) {
         err = a.link_why;
         return SMG_EINVAL;
     }
@@ -537,7 +608,7 @@ int jit_compile_link(const std::vector<std::string>& P, int regs, std::vector<ch
     std::atomic<size_t> next(0);
     const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 64));
     auto work = [&]() {
-        for (size_t i = next++; i < P.size(); i = next++) rcs[i] = compile_one(P[i], regs, obj[i], errs[i]);
+        for (size_t i = next++; i < P.size(); i = next++) rcs[i] = compile_one(P[i].src, regs, link, obj[i], errs[i]);
     };
     std::vector<std::thread> th;
     for (unsigned t = 1; t < std::min<size_t>(nt, P.size()); ++t) th.emplace_back(work);
@@ -548,35 +619,82 @@ int jit_compile_link(const std::vector<std::string>& P, int regs, std::vector<ch
             err = errs[i];
             return rcs[i];
         }
-    nvJitLinkHandle_t L = nullptr;
-    const char* lopts[] = {"-arch=sm_100a"};
-    if (a.LinkCreate(&L, 1, lopts) != 0) {
-        err = "nvJitLinkCreate failed";
-        return SMG_ECUDA;
-    }
-    int rc = SMG_OK;
-    for (size_t i = 0; i < P.size() && rc == SMG_OK; ++i) {
-        const std::string name = "smg_jit_" + std::to_string(i) + ".cubin";
-        if (a.LinkAddData(L, kJitLinkInputCubin, obj[i].data(), obj[i].size(), name.c_str()) != 0) rc = SMG_ECUDA;
-    }
-    if (rc == SMG_OK && a.LinkComplete(L) != 0) rc = SMG_ECUDA;
-    if (rc != SMG_OK) {
+    if (!link) {
+        out = std::move(obj);
+    } else {
+        nvJitLinkHandle_t L = nullptr;
+        const char* lopts[] = {"-arch=sm_100a"};
+        if (a.LinkCreate(&L, 1, lopts) != 0) {
+            err = "nvJitLinkCreate failed";
+            return SMG_ECUDA;
+        }
+        int rc = SMG_OK;
+        for (size_t i = 0; i < P.size() && rc == SMG_OK; ++i) {
+            const std::string name = "smg_jit_" + std::to_string(i) + ".cubin";
+            if (a.LinkAddData(L, kJitLinkInputCubin, obj[i].data(), obj[i].size(), name.c_str()) != 0) rc = SMG_ECUDA;
+        }
+        if (rc == SMG_OK && a.LinkComplete(L) != 0) rc = SMG_ECUDA;
+        if (rc != SMG_OK) {
+            size_t n = 0;
+            a.LinkErrorLogSize(L, &n);
+            std::string log(n, '\0');
+            if (n) a.LinkErrorLog(L, &log[0]);
+            err = "nvJitLink: " + log.substr(0, 2000);
+            a.LinkDestroy(&L);
+            return rc;
+        }
         size_t n = 0;
-        a.LinkErrorLogSize(L, &n);
-        std::string log(n, '\0');
-        if (n) a.LinkErrorLog(L, &log[0]);
-        err = "nvJitLink: " + log.substr(0, 2000);
+        a.LinkedCubinSize(L, &n);
+        out.assign(1, std::vector<char>(n, 0));
+        a.LinkedCubin(L, out[0].data());
         a.LinkDestroy(&L);
-        return rc;
     }
-    size_t n = 0;
-    a.LinkedCubinSize(L, &n);
-    cubin.assign(n, 0);
-    a.LinkedCubin(L, cubin.data());
-    a.LinkDestroy(&L);
     std::lock_guard<std::mutex> lk(g_cubin_mu);
-    g_cubins[key] = cubin;
+    g_cubins[key] = out;
     return SMG_OK;
+}
+
+}  // namespace
+
+namespace smg {
+
+struct JitKernel {
+    CUfunction_t fn = nullptr;
+    long long grid = 0;
+};
+
+struct JitState {
+    std::vector<CUmodule_t> mods;
+    std::vector<JitKernel> k[2];           // kernels of each phase type
+    int block = 64;
+    std::vector<cudaStream_t> side;        // concurrent kernels of a phase (inline layout)
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+};
+
+std::string jit_source(const smg_handle* h, int block, int group) {
+    std::string o;
+    int i = 0;
+    for (const KernelSrc& k : programs(h, block, group, h->jit_split, h->jit_calls))
+        o += "// ---- program " + std::to_string(i++) + (k.name.empty() ? "" : " (" + k.name + ")") + "\n" + k.src;
+    return o;
+}
+
+int jit_compile(const smg_handle* h, int block, int group, std::string& err) {
+    std::vector<std::vector<char>> cubins;
+    return compile_programs(programs(h, block, group, h->jit_split, h->jit_calls), 64, h->jit_calls, cubins, err);
+}
+
+void jit_free(smg_handle* h) {
+    JitState* J = h->jit;
+    if (!J) return;
+    for (cudaStream_t st : J->side) cudaStreamDestroy(st);
+    if (J->fork) cudaEventDestroy(J->fork);
+    for (cudaEvent_t e : J->join) cudaEventDestroy(e);
+    if (api().cu_ok)
+        for (CUmodule_t m : J->mods) api().ModuleUnload(m);
+    delete J;
+    h->jit = nullptr;
 }
 
 int jit_build(smg_handle* h, std::string& err) {
@@ -591,75 +709,117 @@ int jit_build(smg_handle* h, std::string& err) {
         return SMG_EINVAL;
     }
     const int block = h->jit_block, group = h->jit_group;
-    std::vector<char> cubin;
-    int rc = jit_compile_link(programs(h, block, group, 4), h->jit_regs, cubin, err);
+    const bool calls = h->jit_calls != 0;
+    const std::vector<KernelSrc> P = programs(h, block, group, h->jit_split, calls);
+    std::vector<std::vector<char>> cubins;
+    int rc = compile_programs(P, h->jit_regs, calls, cubins, err);
     if (rc != SMG_OK) return rc;
     JitState* J = new JitState();
+    h->jit = J;
     J->block = block;
-    J->group = group;
-    if (a.ModuleLoadData(&J->mod, cubin.data()) != 0) {
-        err = "cuModuleLoadData failed";
-        delete J;
+    auto fail = [&](const std::string& m) {
+        err = m;
+        jit_free(h);
         return SMG_ECUDA;
+    };
+    for (const auto& c : cubins) {
+        CUmodule_t m = nullptr;
+        if (a.ModuleLoadData(&m, c.data()) != 0) return fail("cuModuleLoadData failed");
+        J->mods.push_back(m);
     }
-    const int tpr = (h->g.B[0] + 1) / 2;
-    const long long nchunks = (tpr + block - 1) / block;
-    const long long rows = (long long)h->g.B[1] * h->g.B[2];
-    for (int phase = 0; phase < 2; ++phase) {
-        const std::vector<int> D = phase_dests(h, phase);
-        J->grid[phase] = ((long long)D.size() + group - 1) / group * nchunks * rows;
-        if (D.empty()) continue;
-        const std::string name = "smg_jit_p" + std::to_string(phase);
-        if (a.ModuleGetFunction(&J->fn[phase], J->mod, name.c_str()) != 0) {
-            err = "cuModuleGetFunction " + name;
-            a.ModuleUnload(J->mod);
-            delete J;
-            return SMG_ECUDA;
+    if (calls) {
+        const int tpr = (h->g.B[0] + 1) / 2;
+        const long long per = (long long)((tpr + block - 1) / block) * h->g.B[1] * h->g.B[2];
+        for (int phase = 0; phase < 2; ++phase) {
+            const std::vector<int> D = phase_dests(h, phase);
+            if (D.empty()) continue;
+            JitKernel k;
+            k.grid = ((long long)D.size() + group - 1) / group * per;
+            const std::string name = "smg_jit_p" + std::to_string(phase);
+            if (a.ModuleGetFunction(&k.fn, J->mods[0], name.c_str()) != 0) return fail("cuModuleGetFunction " + name);
+            J->k[phase].push_back(k);
+        }
+    } else {
+        for (size_t i = 0; i < P.size(); ++i) {
+            JitKernel k;
+            k.grid = P[i].grid;
+            if (a.ModuleGetFunction(&k.fn, J->mods[i], P[i].name.c_str()) != 0)
+                return fail("cuModuleGetFunction " + P[i].name);
+            J->k[P[i].phase].push_back(k);
+        }
+        const size_t nk = std::max(J->k[0].size(), J->k[1].size());
+        if (nk > 1) {
+            if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+            for (size_t i = 0; i < nk; ++i) {
+                cudaStream_t st = nullptr;
+                cudaEvent_t ev = nullptr;
+                if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail("cudaStreamCreate");
+                J->side.push_back(st);
+                if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+                J->join.push_back(ev);
+            }
         }
     }
-    h->jit = J;
     return SMG_OK;
 }
 
-void jit_free(smg_handle* h) {
-    if (!h->jit) return;
-    if (h->jit->mod && api().cu_ok) api().ModuleUnload(h->jit->mod);
-    delete h->jit;
-    h->jit = nullptr;
-}
-
+// One phase: its kernel, or its kernels forked onto the side streams after
+// the work already queued on s and joined back into s (inside a stream
+// capture this becomes parallel branches of the graph).
 cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s) {
     const int phase = mode == 1 ? 1 : 0;
-    const JitState* J = h->jit;
-    CUfunction_t f = J->fn[phase];
-    if (!f || J->grid[phase] == 0) return cudaSuccess;
+    JitState* J = h->jit;
+    const std::vector<JitKernel>& K = J->k[phase];
+    if (K.empty()) return cudaSuccess;
     double* U = h->dU;
     const DevField* F = h->dFieldTab;
     double hdt = h->hdt;
     int kf = kfilter;
     int md = mode;
     void* args[] = {&U, &F, &hdt, &kf, &md};
-    const CUresult_t r =
-        api().LaunchKernel(f, (unsigned)J->grid[phase], 1, 1, (unsigned)J->block, 1, 1, 0, s, args, nullptr);
-    return r == 0 ? cudaSuccess : cudaErrorLaunchFailure;
+    auto go = [&](const JitKernel& k, cudaStream_t st) {
+        return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, (unsigned)J->block, 1, 1, 0, st, args, nullptr) == 0
+                   ? cudaSuccess
+                   : cudaErrorLaunchFailure;
+    };
+    if (K.size() == 1) return go(K[0], s);
+    cudaError_t e = cudaEventRecord(J->fork, s);
+    if (e != cudaSuccess) return e;
+    for (size_t i = 0; i < K.size(); ++i) {
+        if ((e = cudaStreamWaitEvent(J->side[i], J->fork, 0)) != cudaSuccess) return e;
+        if ((e = go(K[i], J->side[i])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(J->join[i], J->side[i])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, J->join[i], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
+
+int jit_launches(const smg_handle* h, int phase) { return h->jit ? (int)h->jit->k[phase].size() : 0; }
 
 }  // namespace smg
 
-extern "C" int smg_jit_source(const smg_problem* p, int32_t block, int32_t group, int32_t compile, char* buf,
-                              int64_t cap, int64_t* len) {
-    if (!p) return SMG_EINVAL;
-    if (block < 32 || block > 256 || block % 32 || group < 1 || group > 256) {
-        smg::set_global_error("smg_jit_source: block must be 32..256 (x32), group 1..256");
+extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune,
+                              int32_t compile, char* buf, int64_t cap, int64_t* len) {
+    if (!p || ntune < 0 || (ntune > 0 && (!keys || !values))) {
+        smg::set_global_error("smg_jit_source: bad arguments");
         return SMG_EINVAL;
     }
     smg_handle* h = nullptr;
     int rc = smg::create_host(p, &h);
     if (rc != SMG_OK) return rc;
-    const std::string s = smg::jit_source(h, block, group);
-    std::vector<std::string> P;
-    if (compile) P = programs(h, block, group, 4);
-    delete h;
+    for (int i = 0; i < ntune; ++i) {
+        if (keys[i] < SMG_TUNE_JIT_BLOCK) {
+            rc = SMG_EINVAL;
+            smg::set_global_error("smg_jit_source: only SMG_TUNE_JIT_* keys apply");
+        } else if ((rc = smg_tune(h, keys[i], values[i])) != SMG_OK) {
+            smg::set_global_error("smg_jit_source: " + h->err);
+        }
+        if (rc != SMG_OK) {
+            delete h;
+            return rc;
+        }
+    }
+    const std::string s = smg::jit_source(h, h->jit_block, h->jit_group);
     if (len) *len = (int64_t)s.size();
     if (buf && cap > 0) {
         const size_t n = std::min<size_t>((size_t)cap - 1, s.size());
@@ -667,11 +827,10 @@ extern "C" int smg_jit_source(const smg_problem* p, int32_t block, int32_t group
         buf[n] = '\0';
     }
     if (compile) {
-        std::vector<char> cubin;
         std::string err;
-        rc = smg::jit_compile_link(P, 64, cubin, err);
+        rc = smg::jit_compile(h, h->jit_block, h->jit_group, err);
         if (rc != SMG_OK) smg::set_global_error("smg_jit_source: " + err);
-        return rc;
     }
-    return SMG_OK;
+    delete h;
+    return rc;
 }

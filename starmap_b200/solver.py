@@ -244,16 +244,20 @@ def C_cast_fields(fa):
 
 
 def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay_t=None, decay_a=-1,
-               filter_mode=FILTER_NONE, filter1=None, filter2=None, block=64, group=8, compile=False):
-    """CUDA C++ source of the problem's specialised kernels (SMG_VARIANT_JIT);
-    with compile=True also compiled by NVRTC for sm_100a (no GPU needed)."""
+               filter_mode=FILTER_NONE, filter1=None, filter2=None, compile=False, tune=None):
+    """CUDA C++ source of the problem's specialised kernels (SMG_VARIANT_JIT)
+    for the SMG_TUNE_JIT_* settings in ``tune`` ({key: value}); with
+    compile=True also compiled by NVRTC for sm_100a (no GPU needed)."""
     L = _lib.lib()
     p, keep, _ = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
                                decay_t, decay_a, filter_mode, filter1, filter2)
+    tune = dict(tune or {})
+    keys = (_lib.C.c_int32 * max(len(tune), 1))(*[int(k) for k in tune])
+    vals = (_lib.C.c_int32 * max(len(tune), 1))(*[int(v) for v in tune.values()])
     ln = _lib.C.c_int64()
-    check(L.smg_jit_source(_lib.C.byref(p), int(block), int(group), 0, None, 0, _lib.C.byref(ln)))
+    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), 0, None, 0, _lib.C.byref(ln)))
     buf = _lib.C.create_string_buffer(ln.value + 1)
-    check(L.smg_jit_source(_lib.C.byref(p), int(block), int(group), int(bool(compile)), buf, ln.value + 1,
+    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), int(bool(compile)), buf, ln.value + 1,
                            _lib.C.byref(ln)))
     return buf.value.decode()
 

@@ -10,12 +10,14 @@ from starmap_b200.batch import _tables
 from starmap_b200.solver import first_step, handle_tables, jit_source, prepare
 
 
-def _source(name, compile=False, block=64, group=8):
+def _source(name, compile=False, block=64, group=8, **tune):
     S = prepare(starmap_init(cases.ALL[name]()))
     fs = first_step(S)
     T = _tables(S, fs)
+    settings = {_lib.SMG_TUNE_JIT_BLOCK: block, _lib.SMG_TUNE_JIT_GROUP: group}
+    settings.update({getattr(_lib, "SMG_TUNE_JIT_" + k.upper()): v for k, v in tune.items()})
     return S, jit_source(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T),
-                         block=block, group=group, compile=compile)
+                         compile=compile, tune=settings)
 
 
 def _nvrtc_available():
@@ -30,22 +32,25 @@ def _nvrtc_available():
 
 @pytest.mark.parametrize("name", sorted(cases.ALL))
 def test_generated_source_structure(name):
-    S, src = _source(name)
+    S, src = _source(name, split=4, calls=0)
     n_a = sum(1 for j in range(S.n_sys) if int(np.sum(np.asarray(S.gt[j]) == 2)) % 2 == 1)
-    assert "smg_jit_p1(" in src
-    assert ("smg_jit_p0(" in src) == (n_a > 0)
+    assert "smg_jit_p1_0(" in src
+    assert ("smg_jit_p0_0(" in src) == (n_a > 0)
     # one block per destination: every component is updated once per phase
     assert src.count("double* Uj = U + pt + ") == S.n_sys
-    # one device function per group of 8 destinations, called from the dispatch kernels
-    ngroups = (n_a + 7) // 8 + (S.n_sys - n_a + 7) // 8
-    assert src.count("__noinline__ void smg_g") == ngroups
+    # one inlined function per group of 8 destinations, 4 groups per kernel
+    ga, gb = (n_a + 7) // 8, (S.n_sys - n_a + 7) // 8
+    assert src.count("__forceinline__ void smg_g") == ga + gb
+    assert src.count("__global__") == (ga + 3) // 4 + (gb + 3) // 4
 
 
 @pytest.mark.parametrize("name", ["lin_p7_periodic", "odd_mixed_bc", "pt3d_p3", "lattice_p4_full", "spn_3d"])
-def test_generated_source_compiles(name):
+@pytest.mark.parametrize("layout", [dict(calls=0, split=4, xpair=0), dict(calls=1, split=2, xpair=1),
+                                    dict(calls=0, split=0, xpair=1)])
+def test_generated_source_compiles(name, layout):
     if not _nvrtc_available():
         pytest.skip("NVRTC library not present")
-    _source(name, compile=True, block=128, group=3)
+    _source(name, compile=True, block=128, group=3, **layout)
 
 
 def test_bad_tuning_rejected():

@@ -159,8 +159,9 @@ def test_auto_runs_the_specialised_kernels():
     assert v == 5, why
 
 
-@pytest.mark.parametrize("block,group", [(32, 1), (128, 3), (256, 64)])
-def test_jit_tuning_keeps_results(block, group):
+@pytest.mark.parametrize("block,group,split,calls,xpair", [(32, 1, 4, 0, 0), (128, 3, 1, 1, 0), (256, 64, 4, 0, 1),
+                                                         (64, 4, 0, 0, 1), (64, 2, 3, 1, 1)])
+def test_jit_tuning_keeps_results(block, group, split, calls, xpair):
     from starmap_b200 import _lib
     from starmap_b200.solver import setup_gpu
     par = starmap_init(cases.odd_mixed_bc())
@@ -171,6 +172,9 @@ def test_jit_tuning_keeps_results(block, group):
             if tune:
                 solver.tune(_lib.SMG_TUNE_JIT_BLOCK, block)
                 solver.tune(_lib.SMG_TUNE_JIT_GROUP, group)
+                solver.tune(_lib.SMG_TUNE_JIT_SPLIT, split)
+                solver.tune(_lib.SMG_TUNE_JIT_CALLS, calls)
+                solver.tune(_lib.SMG_TUNE_JIT_XPAIR, xpair)
                 solver.set_variant(5)
             else:
                 solver.set_variant(4)
