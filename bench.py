@@ -132,9 +132,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per step of the phase kernels from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "phase_kernels_lattice_p39_350.txt")
+def ncu_traffic(family="jit"):
+    """DRAM bytes per step of the phase kernels of `family` from the committed ncu summary (or None)."""
+    name = "phase_kernels_jit_lattice_p39.txt" if family == "jit" else "phase_kernels_lattice_p39_350.txt"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_step:"):
@@ -324,7 +325,7 @@ def main():
     ap.add_argument("--steps", type=int, default=321)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--variant", choices=["auto", "generic", "strip", "staged", "pair"], default="auto",
+    ap.add_argument("--variant", choices=["auto", "generic", "strip", "staged", "pair", "jit"], default="auto",
                     help="kernel family (all give identical results)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -350,13 +351,14 @@ def main():
     n_sys = S.n_sys
     cells = int(np.prod(S.n))
     upd_step = n_sys * cells
-    variant = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4}[args.variant]
+    variant = {"auto": 0, "generic": 1, "strip": 2, "staged": 3, "pair": 4, "jit": 5}[args.variant]
     solver.set_variant(variant)
-    alg = algorithmic_bytes_per_step(S, T, fused=(variant in (0, 3, 4)))
+    alg = algorithmic_bytes_per_step(S, T, fused=(variant in (0, 3, 4, 5)))
     solver.set_state(S.U0)
     solver.set_dt(fs["dt"])
     solver.run(args.warmup)
     solver.sync()
+    family = {1: "generic", 2: "strip", 3: "staged", 4: "pair", 5: "jit"}[solver.active_variant()[0]]
 
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -396,7 +398,7 @@ def main():
     peak, peak_kind = measured_peak()
     t_step = ms_max / 1e3 / args.steps
     achieved = alg["step"] / t_step / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(family)
     line = {
         "metric": METRIC, "value": upd_step * args.steps * world / (ms_max / 1e3), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -405,11 +407,13 @@ def main():
         "config": {"workload": WORKLOAD_NAME, "n_sys": n_sys, "cells": cells,
                    "updates_per_step": upd_step, "state_gb": alg["state_bytes"] / 1e9,
                    "l2": "inputs larger than L2 (state %.2f GB > 126 MB), no flush" % (alg["state_bytes"] / 1e9),
-                   "parallelism": "replicas" if world > 1 else "single GPU", "variant": args.variant},
+                   "parallelism": "replicas" if world > 1 else "single GPU", "variant": args.variant,
+                   "kernel_family": family},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_step": alg["step"],
-                     "kernel": "fused staggered half-step kernels (phase A/B), avg over the timed steps"},
+                     "kernel": "phase kernels of the step (A, then B and the fused A-A), "
+                               "averaged over the timed steps"},
         "gpu_launches": int(launches),
         "clocks": clk,
         "finite": finite,
