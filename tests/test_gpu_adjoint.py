@@ -194,3 +194,44 @@ def test_backward_reports_device_time_and_repeats():
     assert ms_f > 0 and ms_b > 0 and nl_f == 13 and nl_b > 0
     for j in g1:
         np.testing.assert_array_equal(g1[j], g2[j])
+
+
+@pytest.mark.parametrize("bc,substep,fused,K", [(1, True, 1, 3), (0, False, 1, 0), (1, True, 0, 4)])
+def test_gradients_match_cpu_adjoint(bc, substep, fused, K):
+    """GPU dJ/dU(0), dJ/dsigma_t, dJ/dsigma_a and dJ/dq against the oracle's
+    CPU adjoint of the same loop (oracle/adjoint_np.py), relative 1e-11 per
+    output array."""
+    from oracle import adjoint_np as A
+    S, fs = adjoint_problem(bc=bc, substep=substep)
+    nsteps = 7
+    solver, T = make_solver(S, fs, fused=fused)
+    try:
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.forward(nsteps, K)
+        u = solver.get_state([0])[0]
+        obs = 0.5 * u + 0.01
+        J = solver.misfit(obs)
+        keys = [k for k in T.index if k[0] in ("sT", "sA", "Q")]
+        gU, gF = solver.backward(fields=[T.index[k] for k in keys])
+    finally:
+        solver.close()
+    ref = A.adjoint(S.par, nsteps, A.misfit_seed(obs))
+    assert np.isclose(J, ref["J"], rtol=1e-13)
+
+    def close(got, want, what):
+        got = np.asarray(got, dtype=np.float64).ravel(order="F")
+        want = np.asarray(want, dtype=np.float64).ravel(order="F")
+        err = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-300)
+        assert err <= 1e-11, (what, err)
+
+    for j in range(S.n_sys):
+        close(gU[j], ref["lam0"][j], ("U0", j))
+    for key in keys:
+        k = T.index[key]
+        if key[0] == "sT":
+            close(gF[k], ref["g_sT"][key[1:]], key)
+        elif key[0] == "sA":
+            close(gF[k], ref["g_sA"], key)
+        else:
+            close(gF[k], ref["g_Q"][key[1]], key)
