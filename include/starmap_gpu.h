@@ -156,8 +156,9 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
 /* The CUDA C++ source of the specialised kernels (SMG_VARIANT_JIT) of problem
  * p, generated with the SMG_TUNE_JIT_* settings keys[i] = values[i] (ntune of
  * them; defaults otherwise); *len receives its length, buf (cap bytes) a
- * NUL-terminated copy.  compile != 0 also compiles it with NVRTC for sm_100a
- * (no GPU needed).  No reference counterpart. */
+ * NUL-terminated copy.  compile = 1 also compiles it with NVRTC for sm_100a
+ * (no GPU needed); compile = 2 adds (to the source and the compilation) the
+ * adjoint's recording and backward-phase kernels.  No reference counterpart. */
 int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune, int32_t compile,
                    char* buf, int64_t cap, int64_t* len);
 

@@ -84,6 +84,8 @@ struct AdjData {
     TCoup* d_tcoup[2] = {nullptr, nullptr};
     bool ready = false, seeded = false;
     bool tail_valid = false;       // the recording holds the last segment (written by smg_forward)
+    DevField* dDE = nullptr;       // per field: d(decay)/d(sigma) (array slot or scalar), generated kernels
+    double** dG = nullptr;         // per field: gradient slot or nullptr, generated kernels
     size_t bytes = 0;
 };
 
@@ -456,6 +458,7 @@ smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec, 
 }
 
 cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec) {
+    if (h->jit_rec) return smg::launch_jit_rec(h, mode, kf, U, wrec, prec, h->stream);
     const int phase = mode == 1 ? 1 : 0;
     const smg::PairArgs a = rec_args(h, phase, U, wrec, prec);
     if (a.ndest == 0) return cudaSuccess;
@@ -500,6 +503,8 @@ void free_adj(smg_handle* h) {
     cudaFree(A->rec_w);
     for (double* p : A->gfield) cudaFree(p);
     for (double* p : A->dEslot) cudaFree(p);
+    cudaFree(A->dDE);
+    cudaFree(A->dG);
     for (int l = 0; l < 2; ++l) {
         cudaFree(A->d_dests[l]);
         cudaFree(A->d_srcs[l]);
@@ -696,6 +701,13 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
     // targets l: 0 = sources of an A phase (B destinations), 1 = sources of a B phase
     auto launch = [&](int l, int coup, int pkind, const double* pre, const double* W, int nkind) -> cudaError_t {
         if (A->srcs[l].empty()) return cudaSuccess;
+        if (h->jit_adj && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_JIT)) {
+            // kind -> (substeps, filters in k=2, k=1 order)
+            auto swap = [](int kind) { return kind == 2 || kind == 3 ? 1 : 0; };
+            *launches += smg::jit_adj_launches(h, l);
+            return smg::launch_jit_adj(h, l, coup, substeps(pkind), swap(pkind), substeps(nkind), swap(nkind), A->lam,
+                                       A->dDE, A->dG, pre, W, h->stream);
+        }
         const dim3 grid(nbp, (unsigned)A->srcs[l].size());
         const int PM = substeps(pkind), NM = substeps(nkind);
         const smg::AdjDest* pt = table(pkind);
@@ -833,6 +845,33 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     }
     int rc = build_tables(h);
     if (rc != SMG_OK) return rc;
+    {   // per-field tables of the generated backward kernels
+        const int nft = (int)h->fields_host.size();
+        std::vector<smg::DevField> de(nft, smg::DevField{nullptr, 0.0});
+        std::vector<double*> gt(nft, nullptr);
+        for (int f = 0; f < nf; ++f) {
+            de[f] = smg::DevField{A->dEslot[f], A->dEscalar[f]};
+            gt[f] = A->gfield[f];
+        }
+        cudaFree(A->dDE);
+        cudaFree(A->dG);
+        A->dDE = nullptr;
+        A->dG = nullptr;
+        A_CUDA(h, cudaMalloc(&A->dDE, sizeof(smg::DevField) * nft));
+        A_CUDA(h, cudaMalloc(&A->dG, sizeof(double*) * nft));
+        A_CUDA(h, cudaMemcpyAsync(A->dDE, de.data(), sizeof(smg::DevField) * nft, cudaMemcpyHostToDevice, h->stream));
+        A_CUDA(h, cudaMemcpyAsync(A->dG, gt.data(), sizeof(double*) * nft, cudaMemcpyHostToDevice, h->stream));
+        A_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    // recording and backward kernels: the generated ones where the handle runs
+    // the generated kernels (AUTO or JIT), else the precompiled ones
+    if ((h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_JIT) && !h->jit_failed) {
+        std::string why;
+        if (smg::jit_build_rec(h, why) != SMG_OK || smg::jit_build_adj(h, why) != SMG_OK) {
+            h->jit_failed = true;
+            h->jit_err = why;
+        }
+    }
     for (int l = 0; l < 2; ++l)
         for (const auto& sr : A->srcs[l])
             if (sr.pslot < 0) return afail(h, SMG_EINVAL, "smg_forward: a component is no phase's destination");

@@ -90,6 +90,8 @@ struct smg_handle {
     smg::AdjData* adj = nullptr;     // adjoint checkpoints and buffers (smg_forward)
     int adj_fused = 1;               // smg_backward kernel form (SMG_TUNE_ADJ_FUSED)
     smg::JitState* jit = nullptr;    // problem-specialised kernels (SMG_VARIANT_JIT)
+    smg::JitState* jit_rec = nullptr;  // the same with adjoint recording (smg_forward / smg_backward)
+    smg::JitState* jit_adj = nullptr;  // generated backward-phase kernels (smg_backward)
     int jit_block = 64, jit_group = 4, jit_regs = 64;
     int jit_split = 16;              // groups per NVRTC program (0: one program per phase)
     int jit_calls = 0;               // 1: one kernel per phase calling separately compiled groups
@@ -116,6 +118,13 @@ int run_steps(smg_handle* h, int64_t nsteps, bool events);   // smg_run without 
 int jit_build(smg_handle* h, std::string& err);             // generate, compile, load (SMG_OK or error)
 void jit_free(smg_handle* h);
 cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s);
+int jit_build_rec(smg_handle* h, std::string& err);
+int jit_build_adj(smg_handle* h, std::string& err);
+cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_swap, int nm, int nm_swap, double* Y,
+                           const DevField* DE, double* const* Gt, const double* pre, const double* W, cudaStream_t s);
+int jit_adj_launches(const smg_handle* h, int l);
+cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U, double* wrec, double* prec,
+                           cudaStream_t s);
 std::string jit_source(const smg_handle* h, int block, int group);
 int jit_compile(const smg_handle* h, int block, int group, std::string& err);   // compile only (no device)
 int jit_launches(const smg_handle* h, int phase);                                 // kernels per phase

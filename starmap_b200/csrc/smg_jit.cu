@@ -203,6 +203,86 @@ static __device__ __forceinline__ const double* fp(const DevField* F, int i) {
 static __device__ __forceinline__ double fs(const DevField* F, int i) { return __ldg(&F[i].s); }
 )";
 
+// Helpers of the generated adjoint kernels: D^T of a staggered difference
+// (preimages of hi and lo under the stencil of starmap_solver.m:127-132), per
+// point (x) and for a row pair (y/z, one 128-bit load serves both points).
+const char* kAdjPrelude = R"(
+static __device__ __forceinline__ double dT(const double* v, int q, int n, int bc, int g2, long long st) {
+    if (!g2) {
+        if (bc) {
+            double a = v[0];
+            if (q == n - 1) a += v[st];
+            double b = v[st];
+            if (q == 0) b += v[0];
+            return a - b;
+        }
+        const long long om = (q == 0) ? (long long)(n - 1) * st : -st;
+        return v[om] - v[0];
+    }
+    if (bc) {
+        const double a = q >= 1 ? v[-st] : 0.0;
+        const double b = q <= n - 1 ? v[0] : 0.0;
+        return a - b;
+    }
+    const long long op = (q == n - 1) ? -(long long)(n - 1) * st : st;
+    return v[0] - v[op];
+}
+static __device__ __forceinline__ double2 L2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+static __device__ __forceinline__ double2 S2(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+static __device__ __forceinline__ double2 A2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+static __device__ __forceinline__ double2 dT_row(const double* v, int q, int n, int bc, int g2, long long st) {
+    const double2 z = make_double2(0.0, 0.0);
+    if (!g2) {
+        if (bc) {
+            double2 a = L2(v);
+            if (q == n - 1) a = A2(a, L2(v + st));
+            double2 b = L2(v + st);
+            if (q == 0) b = A2(b, L2(v));
+            return S2(a, b);
+        }
+        const long long om = (q == 0) ? (long long)(n - 1) * st : -st;
+        return S2(L2(v + om), L2(v));
+    }
+    if (bc) {
+        const double2 a = q >= 1 ? L2(v - st) : z;
+        const double2 b = q <= n - 1 ? L2(v) : z;
+        return S2(a, b);
+    }
+    const long long op = (q == n - 1) ? -(long long)(n - 1) * st : st;
+    return S2(L2(v), L2(v + op));
+}
+// phase's pointwise adjoint from Y = (dU'/dW) lambda' (one substep: M = 1,
+// two: M = 2; F1 the first substep's filter), with its gradient
+// contributions; returns lambda = (dU'/dU) lambda'
+static __device__ __forceinline__ double pend(int M, double u, double w, double Y, double s, double E, double q,
+                                              double F1, double dE, double* gs, double* gq, int pt, double hdt) {
+    const double r = 1.0 - hdt * s * E;
+    double rho, dsdw = 0.0;
+    if (M == 1) {
+        rho = r / (hdt * E);
+        if (gs) dsdw = (-u * E + (w + q - s * u) * dE) / E;
+    } else {
+        const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
+        rho = F1 * r * r * den;
+        if (gs) {
+            const double G0 = w + q - s * u;
+            const double V1 = F1 * (u + hdt * G0 * E);
+            const double G1 = w + q - s * V1;
+            dsdw = (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
+        }
+    }
+    if (gs) atomicAdd(gs + pt, dsdw * Y);
+    if (gq) atomicAdd(gq + pt, Y);
+    return rho * Y;
+}
+// dU'/dW of a destination (F1 first, F2 last substep filter)
+static __device__ __forceinline__ double dwdu(int M, double s, double E, double F1, double F2, double hdt) {
+    if (M == 1) return F1 * hdt * E;
+    const double r = 1.0 - hdt * s * E;
+    return F2 * hdt * E * (r * F1 + 1.0);
+}
+)";
+
 std::string lit(double v) {
     // exact value as a C++17 hexadecimal floating literal
     char buf[64];
@@ -283,7 +363,9 @@ std::string xfast_cond(const smg_handle* h, int g2) {
 // blocks mode 1.  Loads of the second point are unconditional: the row pitch
 // is a multiple of 8 doubles, so x0+1 lies inside the padded row even where
 // the component's extent ends at x0 (that value is unused and not stored).
-void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
+// rec: also store the coupling sum W and the values before the update into
+// slot di of the recording buffers WR / PR (adjoint recording, smg_forward)
+void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bool rec) {
     const smg::DevComp& c = h->comps[j];
     const smg::DevGrid& g = h->g;
     char b[4096];
@@ -376,6 +458,15 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
         return filt ? " u0 = __dmul_rn(u0, " + a0 + "); u1 = __dmul_rn(u1, " + a1 + ");" : std::string();
     };
     o += "        double u0 = u.x, u1 = u.y;\n";
+    if (rec) {
+        const long long so = (long long)di * g.cs;
+        std::snprintf(b, sizeof b,
+                      "        { double* wp = WR + pt + %lld; double* pp = PR + pt + %lld;\n"
+                      "          if (%s) { *reinterpret_cast<double2*>(wp) = make_double2(-SA, -SB); "
+                      "*reinterpret_cast<double2*>(pp) = u; } else { wp[0] = -SA; pp[0] = u.x; } }\n",
+                      so, so, v1_always ? "true" : "v1");
+        o += b;
+    }
     if (phase == 0) {
         const std::string one = "        " + substep() +
                                 (filt ? " u0 = __dmul_rn(u0, kf == 1 ? " + k10 + " : " + k20 +
@@ -395,18 +486,22 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j) {
 }
 
 std::string group_name(int phase, int k) { return "smg_g" + std::to_string(phase) + "_" + std::to_string(k); }
-const char* kGroupArgs =
-    "(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, int y, int z)";
+std::string group_args(bool rec) {
+    return std::string("(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, "
+                       "int y, int z") +
+           (rec ? ", double* __restrict__ WR, double* __restrict__ PR)" : ")");
+}
 
 // device function of one group: the thread's stencil offsets, then the blocks
 // (inl: a function inlined into the dispatch kernel of the same program;
 // otherwise an external function called from it)
-void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group, bool inl) {
+void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group, bool inl,
+                bool rec) {
     const smg::DevGrid& g = h->g;
     char b[1024];
     const int d0 = k * group, d1 = std::min<int>((k + 1) * group, (int)D.size());
     o += std::string(inl ? "static __device__ __forceinline__ void " : "extern \"C\" __device__ __noinline__ void ") +
-         group_name(phase, k) + kGroupArgs + " {\n";
+         group_name(phase, k) + group_args(rec) + " {\n";
     std::snprintf(b, sizeof b,
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
@@ -442,7 +537,7 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
             o += b;
         }
     }
-    for (int i = d0; i < d1; ++i) emit_dest(o, h, phase, D[i]);
+    for (int i = d0; i < d1; ++i) emit_dest(o, h, phase, D[i], i, rec);
     o += "}\n";
 }
 
@@ -450,17 +545,17 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
 // then the group's code (inlined, or a call when the groups are compiled
 // separately)
 void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k1, int block, bool inl,
-                   const std::string& name) {
+                   const std::string& name, bool rec) {
     const smg::DevGrid& g = h->g;
     const int tpr = (g.B[0] + 1) / 2;
     const int nchunks = (tpr + block - 1) / block;
     const long long per = (long long)nchunks * g.B[1] * g.B[2];
     char b[1024];
     if (!inl)
-        for (int k = k0; k < k1; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + kGroupArgs + ";\n";
+        for (int k = k0; k < k1; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + group_args(rec) + ";\n";
     std::snprintf(b, sizeof b,
                   "extern \"C\" __global__ void __launch_bounds__(%d) %s(double* __restrict__ U, "
-                  "const DevField* __restrict__ F, double hdt, int kf, int mode) {\n"
+                  "const DevField* __restrict__ F, double hdt, int kf, int mode%s) {\n"
                   "    const int bid = blockIdx.x;\n"
                   "    const int grp = %d + bid / %lld;\n"
                   "    const int rest = bid %% %lld;\n"
@@ -469,10 +564,12 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
                   "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
                   "    if (x0 >= %d) return;\n"
                   "    switch (grp) {\n",
-                  block, name.c_str(), k0, per, per, nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
+                  block, name.c_str(), rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", k0, per, per,
+                  nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
     o += b;
     for (int k = k0; k < k1; ++k)
-        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z); break;\n";
+        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z" +
+             (rec ? ", WR, PR" : "") + "); break;\n";
     o += "    default: break;\n    }\n}\n";
 }
 
@@ -498,7 +595,8 @@ struct KernelSrc {
 //   inline (calls false): `per` groups per program (0: all of the phase),
 //          each program one kernel over its groups with their code inlined;
 //          the kernels of a phase run concurrently.
-std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int per, bool calls) {
+std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int per, bool calls, bool rec = false) {
+    const std::string sfx = rec ? "_r" : "";
     const smg::DevGrid& g = h->g;
     const int tpr = (g.B[0] + 1) / 2;
     const long long cta_per_group = (long long)((tpr + block - 1) / block) * g.B[1] * g.B[2];
@@ -512,10 +610,10 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
             const int ng = ((int)D.size() + group - 1) / group;
             for (int k = 0; k < ng; ++k) {
                 std::string s;
-                emit_group(s, h, phase, k, D, group, false);
+                emit_group(s, h, phase, k, D, group, false, rec);
                 fns.push_back(std::move(s));
             }
-            emit_dispatch(disp.src, h, phase, 0, ng, block, false, "smg_jit_p" + std::to_string(phase));
+            emit_dispatch(disp.src, h, phase, 0, ng, block, false, "smg_jit_p" + std::to_string(phase) + sfx, rec);
         }
         P.push_back(std::move(disp));
         const size_t step = per > 0 ? (size_t)per : fns.size();
@@ -533,10 +631,10 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         const int step = per > 0 ? per : ng;
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
+            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase,
                         (long long)(k1 - k0) * cta_per_group};
-            for (int j = k0; j < k1; ++j) emit_group(k.src, h, phase, j, D, group, true);
-            emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name);
+            for (int j = k0; j < k1; ++j) emit_group(k.src, h, phase, j, D, group, true, rec);
+            emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
             P.push_back(std::move(k));
         }
     }
@@ -572,6 +670,184 @@ int compile_one(const std::string& src, int regs, bool rdc, std::vector<char>& c
     a.GetCUBIN(prog, cubin.data());
     a.DestroyProgram(&prog);
     return SMG_OK;
+}
+
+// ---- adjoint kernels -------------------------------------------------------
+// One launch set per backward phase r over the sources i of the phase (the
+// destinations of the neighbouring phases), with the adjoint kept scaled as
+// Y_j = (dU'/dW)_j lambda'_j (see smg_adjoint.cu).  Per target i and point pair:
+//   pm:   lambda_i = rho Y_i and the gradient contributions of the pending
+//         phase r+1 (i is one of its destinations, slot pslot in the recording)
+//   coup: lambda_i -= sum_j M_d(j,i) D_d^T Y_j over phase r's destinations j
+//   nm:   Y_i = (dU'/dW)_{r-1,i} lambda_i for the phase before
+// The kinds of r+1 and r-1 arrive at run time as (number of substeps, filter
+// order swapped); everything else is a constant.
+
+// coefficient value of field f at the point pair (two names: .x/.y or scalar)
+std::string adj_coef(const smg_handle* h, int f, const char* n) {
+    char b[256];
+    if (is_array(h, f)) std::snprintf(b, sizeof b, "const double2 %s = L2(fp(F, %d) + pt); ", n, f);
+    else std::snprintf(b, sizeof b, "const double %s = fs(F, %d); ", n, f);
+    return b;
+}
+
+void emit_adj_target(std::string& o, const smg_handle* h, int l, int i) {
+    const smg::DevGrid& g = h->g;
+    const smg::DevComp& c = h->comps[i];
+    char b[4096];
+    // i as a destination of the other phase type: its slot and coefficients
+    const std::vector<int> Dother = phase_dests(h, 1 - l);
+    int pslot = -1;
+    for (size_t k = 0; k < Dother.size(); ++k)
+        if (Dother[k] == i) pslot = (int)k;
+    const Coefs f = coefs_of(h, 1 - l, i);
+    std::string cond;
+    const char* ax[3] = {"x0", "y", "z"};
+    for (int a = 0; a < 3; ++a)
+        if (c.ext[a] < g.B[a]) {
+            if (!cond.empty()) cond += " && ";
+            cond += std::string(ax[a]) + " < " + std::to_string(c.ext[a]);
+        }
+    o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
+    const bool v1_always = c.ext[0] % 2 == 0;
+    std::snprintf(b, sizeof b, "        double* Yi = Y + pt + %lld;\n        const bool v1 = %s;\n"
+                  "        const double2 yv = L2(Yi); double l0 = yv.x, l1 = yv.y;\n",
+                  (long long)i * g.cs, v1_always ? "true" : ("x1 < " + std::to_string(c.ext[0])).c_str());
+    o += b;
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    auto X = [&](int fi, const char* n) { return cx(h, fi, n); };
+    auto Yc = [&](int fi, const char* n) { return cy(h, fi, n); };
+    if (pslot >= 0) {
+        std::string dEdecl;
+        const bool sarr = is_array(h, f.s);
+        // d(decay)/d(sigma) of sigma field f.s: the table DE holds an array or a scalar
+        dEdecl = sarr ? "const double2 dE = L2(fp(DE, " + std::to_string(f.s) + ") + pt); "
+                      : "const double dE = fs(DE, " + std::to_string(f.s) + "); ";
+        std::snprintf(b, sizeof b,
+                      "        if (pm) {\n"
+                      "          %s%s%s%s\n          %s%s\n"
+                      "          double* gs = Gt[%d]; double* gq = %s;\n"
+                      "          const long long rp = %lld + pt;\n",
+                      adj_coef(h, f.s, "s").c_str(), adj_coef(h, f.E, "E").c_str(), adj_coef(h, f.q, "q").c_str(),
+                      dEdecl.c_str(), filt ? adj_coef(h, f.F1, "fk1").c_str() : "",
+                      filt ? adj_coef(h, f.F2, "fk2").c_str() : "", f.s,
+                      f.q == h->field_zero ? "nullptr" : ("Gt[" + std::to_string(f.q) + "]").c_str(),
+                      (long long)pslot * g.cs);
+        o += b;
+        const std::string F0 = filt ? "(pm_swap ? " + X(f.F2, "fk2") + " : " + X(f.F1, "fk1") + ")" : "1.0";
+        const std::string F1 = filt ? "(pm_swap ? " + Yc(f.F2, "fk2") + " : " + Yc(f.F1, "fk1") + ")" : "1.0";
+        const std::string dE0 = sarr ? "dE.x" : "dE", dE1 = sarr ? "dE.y" : "dE";
+        std::snprintf(b, sizeof b,
+                      "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs, gq, pt, hdt);\n"
+                      "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs, gq, pt + 1, hdt);\n"
+                      "        }\n",
+                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), X(f.q, "q").c_str(), F0.c_str(), dE0.c_str(),
+                      Yc(f.s, "s").c_str(), Yc(f.E, "E").c_str(), Yc(f.q, "q").c_str(), F1.c_str(), dE1.c_str());
+        o += b;
+    }
+    // transposed couplings from phase l's destinations, in the fold order
+    // of smg_adjoint.cu's tables (destination order, then sumcell order)
+    const std::vector<int> Dl = phase_dests(h, l);
+    std::string body;
+    for (int j : Dl)
+        for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
+            const smg::DevCoup& cp = h->coups[q];
+            if (cp.src != i) continue;
+            const int a = cp.code >> 1, g2 = cp.code & 1;
+            const std::string fw = lit(cp.w / g.h[a]);
+            if (a == 0) {
+                std::snprintf(b, sizeof b,
+                              "          { const double* v = Y + pt + %lld;\n"
+                              "            a0 += %s * dT(v, x0, %d, %d, %d, 1);\n"
+                              "            if (v1) a1 += %s * dT(v + 1, x1, %d, %d, %d, 1); }\n",
+                              (long long)j * g.cs, fw.c_str(), g.n[0], g.bc[0], g2, fw.c_str(), g.n[0], g.bc[0], g2);
+            } else {
+                const long long st = a == 1 ? g.s1 : g.s2;
+                std::snprintf(b, sizeof b,
+                              "          { const double2 d = dT_row(Y + pt + %lld, %s, %d, %d, %d, %lld);\n"
+                              "            a0 += %s * d.x; a1 += %s * d.y; }\n",
+                              (long long)j * g.cs, a == 1 ? "y" : "z", g.n[a], g.bc[a], g2, st, fw.c_str(), fw.c_str());
+            }
+            body += b;
+        }
+    if (!body.empty()) o += "        if (coup) {\n          double a0 = 0.0, a1 = 0.0;\n" + body +
+                            "          l0 -= a0; l1 -= a1;\n        }\n";
+    if (pslot >= 0) {
+        std::snprintf(b, sizeof b, "        if (nm) {\n          %s%s%s%s\n",
+                      adj_coef(h, f.s, "s").c_str(), adj_coef(h, f.E, "E").c_str(),
+                      filt ? adj_coef(h, f.F1, "fk1").c_str() : "", filt ? adj_coef(h, f.F2, "fk2").c_str() : "");
+        o += b;
+        // first / last substep filters of the phase before (swap: k=2 first)
+        const std::string a0 = filt ? "(nm_swap ? " + X(f.F2, "fk2") + " : " + X(f.F1, "fk1") + ")" : "1.0";
+        const std::string a1 = filt ? "(nm_swap ? " + Yc(f.F2, "fk2") + " : " + Yc(f.F1, "fk1") + ")" : "1.0";
+        const std::string z0 = filt ? "(nm_swap ? " + X(f.F1, "fk1") + " : " + X(f.F2, "fk2") + ")" : "1.0";
+        const std::string z1 = filt ? "(nm_swap ? " + Yc(f.F1, "fk1") + " : " + Yc(f.F2, "fk2") + ")" : "1.0";
+        std::snprintf(b, sizeof b,
+                      "          l0 *= dwdu(nm, %s, %s, %s, %s, hdt);\n"
+                      "          l1 *= dwdu(nm, %s, %s, %s, %s, hdt);\n        }\n",
+                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), a0.c_str(), z0.c_str(), Yc(f.s, "s").c_str(),
+                      Yc(f.E, "E").c_str(), a1.c_str(), z1.c_str());
+        o += b;
+    }
+    o += "        if (v1) *reinterpret_cast<double2*>(Yi) = make_double2(l0, l1); else Yi[0] = l0;\n    }\n";
+}
+
+const char* kAdjArgs =
+    "(double* __restrict__ Y, const DevField* __restrict__ F, const DevField* __restrict__ DE, "
+    "double* const* __restrict__ Gt, const double* __restrict__ PRE, const double* __restrict__ WR, int pm, "
+    "int pm_swap, int nm, int nm_swap, int coup, double hdt";
+
+// kernels over the targets of backward phases of type l (l = 0: A phases,
+// whose sources are the B destinations; l = 1: B phases)
+std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, int per) {
+    const smg::DevGrid& g = h->g;
+    const int tpr = (g.B[0] + 1) / 2;
+    const int nchunks = (tpr + block - 1) / block;
+    const long long cta_per_group = (long long)nchunks * g.B[1] * g.B[2];
+    std::vector<KernelSrc> P;
+    for (int l = 0; l < 2; ++l) {
+        const std::vector<int> T = l == 0 ? h->destB : h->destA;   // sources of the phase type
+        if (T.empty()) continue;
+        const int ng = ((int)T.size() + group - 1) / group;
+        const int step = per > 0 ? per : ng;
+        for (int k0 = 0; k0 < ng; k0 += step) {
+            const int k1 = std::min(ng, k0 + step);
+            KernelSrc K{std::string(kPrelude) + kAdjPrelude, "smg_adj_p" + std::to_string(l) + "_" + std::to_string(k0),
+                        l, (long long)(k1 - k0) * cta_per_group};
+            for (int k = k0; k < k1; ++k) {
+                K.src += "static __device__ __forceinline__ void smg_ag" + std::to_string(l) + "_" + std::to_string(k) +
+                         std::string(kAdjArgs) + ", int x0, int y, int z) {\n"
+                         "    const int x1 = x0 + 1; (void)x1;\n";
+                char b[256];
+                std::snprintf(b, sizeof b, "    const int pt = z * %lld + y * %lld + x0;\n", (long long)g.s2,
+                              (long long)g.s1);
+                K.src += b;
+                for (int t = k * group; t < std::min<int>((k + 1) * group, (int)T.size()); ++t)
+                    emit_adj_target(K.src, h, l, T[t]);
+                K.src += "}\n";
+            }
+            char b[1024];
+            std::snprintf(b, sizeof b,
+                          "extern \"C\" __global__ void __launch_bounds__(%d) %s%s) {\n"
+                          "    const int bid = blockIdx.x;\n"
+                          "    const int grp = %d + bid / %lld;\n"
+                          "    const int rest = bid %% %lld;\n"
+                          "    const int row = rest / %d, chunk = rest - row * %d;\n"
+                          "    const int y = row %% %d, z = row / %d;\n"
+                          "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
+                          "    if (x0 >= %d) return;\n"
+                          "    switch (grp) {\n",
+                          block, K.name.c_str(), kAdjArgs, k0, cta_per_group, cta_per_group, nchunks, nchunks, g.B[1],
+                          g.B[1], block, g.B[0]);
+            K.src += b;
+            for (int k = k0; k < k1; ++k)
+                K.src += "    case " + std::to_string(k) + ": smg_ag" + std::to_string(l) + "_" + std::to_string(k) +
+                         "(Y, F, DE, Gt, PRE, WR, pm, pm_swap, nm, nm_swap, coup, hdt, x0, y, z); break;\n";
+            K.src += "    default: break;\n    }\n}\n";
+            P.push_back(std::move(K));
+        }
+    }
+    return P;
 }
 
 std::map<std::string, std::vector<std::vector<char>>> g_cubins;   // sources -> cubins, process-wide
@@ -685,8 +961,7 @@ int jit_compile(const smg_handle* h, int block, int group, std::string& err) {
     return compile_programs(programs(h, block, group, h->jit_split, h->jit_calls), 64, h->jit_calls, cubins, err);
 }
 
-void jit_free(smg_handle* h) {
-    JitState* J = h->jit;
+void free_state(JitState*& J) {
     if (!J) return;
     for (cudaStream_t st : J->side) cudaStreamDestroy(st);
     if (J->fork) cudaEventDestroy(J->fork);
@@ -694,11 +969,19 @@ void jit_free(smg_handle* h) {
     if (api().cu_ok)
         for (CUmodule_t m : J->mods) api().ModuleUnload(m);
     delete J;
-    h->jit = nullptr;
+    J = nullptr;
 }
 
-int jit_build(smg_handle* h, std::string& err) {
-    if (h->jit) return SMG_OK;
+void jit_free(smg_handle* h) {
+    free_state(h->jit);
+    free_state(h->jit_rec);
+    free_state(h->jit_adj);
+}
+
+namespace {
+
+// Generate, compile and load one form of the kernels (plain or recording).
+int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
     if (!(h->pair[0].ok && h->pair[1].ok)) {
         err = "the problem exceeds 32-bit element offsets";
         return SMG_EINVAL;
@@ -710,16 +993,15 @@ int jit_build(smg_handle* h, std::string& err) {
     }
     const int block = h->jit_block, group = h->jit_group;
     const bool calls = h->jit_calls != 0;
-    const std::vector<KernelSrc> P = programs(h, block, group, h->jit_split, calls);
+    const std::vector<KernelSrc> P = programs(h, block, group, h->jit_split, calls, rec);
     std::vector<std::vector<char>> cubins;
     int rc = compile_programs(P, h->jit_regs, calls, cubins, err);
     if (rc != SMG_OK) return rc;
     JitState* J = new JitState();
-    h->jit = J;
     J->block = block;
     auto fail = [&](const std::string& m) {
         err = m;
-        jit_free(h);
+        free_state(J);
         return SMG_ECUDA;
     };
     for (const auto& c : cubins) {
@@ -735,7 +1017,7 @@ int jit_build(smg_handle* h, std::string& err) {
             if (D.empty()) continue;
             JitKernel k;
             k.grid = ((long long)D.size() + group - 1) / group * per;
-            const std::string name = "smg_jit_p" + std::to_string(phase);
+            const std::string name = "smg_jit_p" + std::to_string(phase) + (rec ? "_r" : "");
             if (a.ModuleGetFunction(&k.fn, J->mods[0], name.c_str()) != 0) return fail("cuModuleGetFunction " + name);
             J->k[phase].push_back(k);
         }
@@ -747,36 +1029,36 @@ int jit_build(smg_handle* h, std::string& err) {
                 return fail("cuModuleGetFunction " + P[i].name);
             J->k[P[i].phase].push_back(k);
         }
-        const size_t nk = std::max(J->k[0].size(), J->k[1].size());
-        if (nk > 1) {
-            if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
-            for (size_t i = 0; i < nk; ++i) {
-                cudaStream_t st = nullptr;
-                cudaEvent_t ev = nullptr;
-                if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail("cudaStreamCreate");
-                J->side.push_back(st);
-                if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
-                J->join.push_back(ev);
-            }
+    }
+    const size_t nk = std::max(J->k[0].size(), J->k[1].size());
+    if (nk > 1) {
+        if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+        for (size_t i = 0; i < nk; ++i) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail("cudaStreamCreate");
+            J->side.push_back(st);
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+            J->join.push_back(ev);
         }
     }
+    out = J;
     return SMG_OK;
 }
 
-// One phase: its kernel, or its kernels forked onto the side streams after
-// the work already queued on s and joined back into s (inside a stream
-// capture this becomes parallel branches of the graph).
-cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s) {
+// One phase of state J: its kernel, or its kernels forked onto the side
+// streams after the work already queued on s and joined back into s (inside
+// a stream capture this becomes parallel branches of the graph).
+cudaError_t launch_state(const smg_handle* h, JitState* J, double* U, int mode, int kfilter, double* wrec,
+                         double* prec, cudaStream_t s) {
     const int phase = mode == 1 ? 1 : 0;
-    JitState* J = h->jit;
     const std::vector<JitKernel>& K = J->k[phase];
     if (K.empty()) return cudaSuccess;
-    double* U = h->dU;
     const DevField* F = h->dFieldTab;
     double hdt = h->hdt;
     int kf = kfilter;
     int md = mode;
-    void* args[] = {&U, &F, &hdt, &kf, &md};
+    void* args[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec};
     auto go = [&](const JitKernel& k, cudaStream_t st) {
         return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, (unsigned)J->block, 1, 1, 0, st, args, nullptr) == 0
                    ? cudaSuccess
@@ -794,9 +1076,118 @@ cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t 
     return cudaSuccess;
 }
 
+}  // namespace
+
+int jit_build(smg_handle* h, std::string& err) {
+    if (h->jit) return SMG_OK;
+    return build_state(h, false, h->jit, err);
+}
+
+int jit_build_rec(smg_handle* h, std::string& err) {
+    if (h->jit_rec) return SMG_OK;
+    return build_state(h, true, h->jit_rec, err);
+}
+
+cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t s) {
+    return launch_state(h, h->jit, h->dU, mode, kfilter, nullptr, nullptr, s);
+}
+
+cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U, double* wrec, double* prec,
+                           cudaStream_t s) {
+    return launch_state(h, h->jit_rec, U, mode, kfilter, wrec, prec, s);
+}
+
 int jit_launches(const smg_handle* h, int phase) { return h->jit ? (int)h->jit->k[phase].size() : 0; }
 
+// Generated adjoint kernels (compiled like the forward ones, inline layout).
+int jit_build_adj(smg_handle* h, std::string& err) {
+    if (h->jit_adj) return SMG_OK;
+    Api& a = api();
+    if (!a.cu_ok) {
+        err = a.cu_why;
+        return SMG_EINVAL;
+    }
+    const int block = h->jit_block, group = h->jit_group;
+    const std::vector<KernelSrc> P = adj_programs(h, block, group, h->jit_split > 0 ? h->jit_split : 16);
+    std::vector<std::vector<char>> cubins;
+    int rc = compile_programs(P, h->jit_regs, false, cubins, err);
+    if (rc != SMG_OK) return rc;
+    JitState* J = new JitState();
+    J->block = block;
+    for (size_t i = 0; i < cubins.size(); ++i) {
+        CUmodule_t m = nullptr;
+        JitKernel k;
+        k.grid = P[i].grid;
+        if (a.ModuleLoadData(&m, cubins[i].data()) != 0 ||
+            (J->mods.push_back(m), a.ModuleGetFunction(&k.fn, m, P[i].name.c_str()) != 0)) {
+            err = "loading the generated adjoint kernels failed";
+            free_state(J);
+            return SMG_ECUDA;
+        }
+        J->k[P[i].phase].push_back(k);
+    }
+    const size_t nk = std::max(J->k[0].size(), J->k[1].size());
+    if (nk > 1) {
+        if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) {
+            free_state(J);
+            err = "cudaEventCreate";
+            return SMG_ECUDA;
+        }
+        for (size_t i = 0; i < nk; ++i) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+                if (st) cudaStreamDestroy(st);
+                free_state(J);
+                err = "cudaStreamCreate";
+                return SMG_ECUDA;
+            }
+            J->side.push_back(st);
+            J->join.push_back(ev);
+        }
+    }
+    h->jit_adj = J;
+    return SMG_OK;
+}
+
+// One backward phase over the sources of a phase of type l (see adj_programs).
+cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_swap, int nm, int nm_swap,
+                           double* Y, const DevField* DE, double* const* Gt, const double* pre, const double* W,
+                           cudaStream_t s) {
+    JitState* J = h->jit_adj;
+    const std::vector<JitKernel>& K = J->k[l];
+    if (K.empty()) return cudaSuccess;
+    const DevField* F = h->dFieldTab;
+    double hdt = h->hdt;
+    void* args[] = {&Y, &F, &DE, &Gt, &pre, &W, &pm, &pm_swap, &nm, &nm_swap, &coup, &hdt};
+    auto go = [&](const JitKernel& k, cudaStream_t st) {
+        return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, (unsigned)J->block, 1, 1, 0, st, args, nullptr) == 0
+                   ? cudaSuccess
+                   : cudaErrorLaunchFailure;
+    };
+    if (K.size() == 1) return go(K[0], s);
+    cudaError_t e = cudaEventRecord(J->fork, s);
+    if (e != cudaSuccess) return e;
+    for (size_t i = 0; i < K.size(); ++i) {
+        if ((e = cudaStreamWaitEvent(J->side[i], J->fork, 0)) != cudaSuccess) return e;
+        if ((e = go(K[i], J->side[i])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(J->join[i], J->side[i])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, J->join[i], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int jit_adj_launches(const smg_handle* h, int l) { return h->jit_adj ? (int)h->jit_adj->k[l].size() : 0; }
+
 }  // namespace smg
+
+static size_t adj_count(const std::vector<KernelSrc>& v) {
+    size_t n = 0;
+    for (const auto& k : v)
+        if (k.name.rfind("smg_adj_", 0) == 0) ++n;
+    return n;
+}
 
 extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune,
                               int32_t compile, char* buf, int64_t cap, int64_t* len) {
@@ -819,7 +1210,14 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
             return rc;
         }
     }
-    const std::string s = smg::jit_source(h, h->jit_block, h->jit_group);
+    std::string s = smg::jit_source(h, h->jit_block, h->jit_group);
+    std::vector<KernelSrc> extra;
+    if (compile == 2) {   // also the recording and the backward-phase kernels of the adjoint
+        extra = programs(h, h->jit_block, h->jit_group, h->jit_split, h->jit_calls, true);
+        const std::vector<KernelSrc> adj = adj_programs(h, h->jit_block, h->jit_group, h->jit_split > 0 ? h->jit_split : 16);
+        extra.insert(extra.end(), adj.begin(), adj.end());
+        for (const KernelSrc& k : extra) s += "// ---- program (" + k.name + ")\n" + k.src;
+    }
     if (len) *len = (int64_t)s.size();
     if (buf && cap > 0) {
         const size_t n = std::min<size_t>((size_t)cap - 1, s.size());
@@ -829,6 +1227,13 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
     if (compile) {
         std::string err;
         rc = smg::jit_compile(h, h->jit_block, h->jit_group, err);
+        if (rc == SMG_OK && !extra.empty()) {
+            std::vector<std::vector<char>> cubins;
+            std::vector<KernelSrc> rec(extra.begin(), extra.begin() + (extra.size() - adj_count(extra)));
+            std::vector<KernelSrc> adj(extra.end() - adj_count(extra), extra.end());
+            rc = compile_programs(rec, 64, h->jit_calls != 0, cubins, err);
+            if (rc == SMG_OK) rc = compile_programs(adj, 64, false, cubins, err);
+        }
         if (rc != SMG_OK) smg::set_global_error("smg_jit_source: " + err);
     }
     delete h;

@@ -77,6 +77,7 @@ class GpuSolver:
                  decay_t=None, decay_a=-1, filter_mode=FILTER_NONE, filter1=None, filter2=None):
         L = _lib.lib()
         self._L = L
+        self.field_scalar = [np.ndim(v) == 0 for v, _ in fields]
         p, keep, info = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
                                       decay_t, decay_a, filter_mode, filter1, filter2)
         self.n_sys, self.n, self.bc, self.gt, self.field_grids = info
@@ -210,12 +211,15 @@ class GpuSolver:
         nf = len(self.field_grids)
         pf = (_lib.C.POINTER(_lib.C.c_double) * max(nf, 1))()
         gf = {}
+        scalar = getattr(self, "field_scalar", [False] * nf)
         for k in fields:
-            gf[k] = np.empty(int(np.prod(self.grid_extents(self.field_grids[k]))))
+            # a scalar coefficient's derivative is one number (its sum over the points it acts on)
+            gf[k] = np.empty(1 if scalar[k] else int(np.prod(self.grid_extents(self.field_grids[k]))))
             pf[k] = dptr(gf[k])
         check(self._L.smg_backward(self.h, pu, pf), self.h)
         gradU = {j: b.reshape(e, order="F") for j, (b, e) in gu.items()}
-        gradF = {k: v.reshape(self.grid_extents(self.field_grids[k]), order="F") for k, v in gf.items()}
+        gradF = {k: (float(v[0]) if scalar[k] else v.reshape(self.grid_extents(self.field_grids[k]), order="F"))
+                 for k, v in gf.items()}
         return gradU, gradF
 
     def state_sumsq(self):
@@ -247,7 +251,8 @@ def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay
                filter_mode=FILTER_NONE, filter1=None, filter2=None, compile=False, tune=None):
     """CUDA C++ source of the problem's specialised kernels (SMG_VARIANT_JIT)
     for the SMG_TUNE_JIT_* settings in ``tune`` ({key: value}); with
-    compile=True also compiled by NVRTC for sm_100a (no GPU needed)."""
+    compile=True (1) also compiled by NVRTC for sm_100a (no GPU needed);
+    compile=2 adds the adjoint's recording and backward-phase kernels."""
     L = _lib.lib()
     p, keep, _ = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
                                decay_t, decay_a, filter_mode, filter1, filter2)
@@ -255,9 +260,10 @@ def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay
     keys = (_lib.C.c_int32 * max(len(tune), 1))(*[int(k) for k in tune])
     vals = (_lib.C.c_int32 * max(len(tune), 1))(*[int(v) for v in tune.values()])
     ln = _lib.C.c_int64()
-    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), 0, None, 0, _lib.C.byref(ln)))
+    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), 2 if compile == 2 else 0, None, 0,
+                           _lib.C.byref(ln)))
     buf = _lib.C.create_string_buffer(ln.value + 1)
-    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), int(bool(compile)), buf, ln.value + 1,
+    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), int(compile), buf, ln.value + 1,
                            _lib.C.byref(ln)))
     return buf.value.decode()
 

@@ -56,3 +56,11 @@ def test_generated_source_compiles(name, layout):
 def test_bad_tuning_rejected():
     with pytest.raises(_lib.SmgError):
         _source("one_d_p5", block=48)
+
+
+@pytest.mark.parametrize("name", ["odd_mixed_bc", "pt3d_p3", "lattice_p5_substep", "lattice_p6_nofilter"])
+def test_adjoint_kernels_compile(name):
+    if not _nvrtc_available():
+        pytest.skip("NVRTC library not present")
+    S, src = _source(name, compile=2, block=64, group=3)
+    assert "smg_adj_p0_0(" in src and "smg_adj_p1_0(" in src and "_r(" in src

@@ -12,27 +12,38 @@ from starmap_b200.solver import GpuSolver, expm1div, first_step, handle_tables, 
 pytestmark = pytest.mark.gpu
 
 
-def adjoint_problem(n=12, N=3, bc=1, with_source=True, substep=True):
-    def sig_a(x, y):
-        return 0.3 + 0.2 * np.sin(2 * x) * np.cos(y)
-
-    prob = dict(name="adj", closure="P", n_mom=N, ax=[-1.0, 1.0, -1.0, 1.0], n=[n, n + 2], bc=[bc, bc],
-                ic=lambda x, y: np.exp(-8 * (x ** 2 + (y - 0.1) ** 2)), sigma_a=sig_a,
-                sigma_s0=lambda x, y: 0.8 + 0.1 * x, tfinal=1e9, t_plot=[0, 1e9], quiet=True)
-    if with_source:
-        prob["source"] = lambda x, y: np.exp(-6 * ((x - 0.3) ** 2 + y ** 2))
-    if substep:
-        prob.update(filterfunction=configs.exp_filter(2, 3.0), f_position="substep")
-    par = starmap_init(prob)
+def adjoint_problem(n=12, N=3, bc=1, with_source=True, substep=True, scalar=False):
+    par = adjoint_par(n, N, bc, with_source, substep, scalar)
     S = prepare(par)
     fs = first_step(S)
     return S, fs
 
 
-def make_solver(S, fs, T=None, fused=1):
+def adjoint_par(n=12, N=3, bc=1, with_source=True, substep=True, scalar=False):
+    def sig_a(x, y):
+        return 0.4 if scalar else 0.3 + 0.2 * np.sin(2 * x) * np.cos(y)
+
+    def sig_s(x, y):
+        return 0.9 if scalar else 0.8 + 0.1 * x
+
+    prob = dict(name="adj", closure="P", n_mom=N, ax=[-1.0, 1.0, -1.0, 1.0], n=[n, n + 2], bc=[bc, bc],
+                ic=lambda x, y: np.exp(-8 * (x ** 2 + (y - 0.1) ** 2)), sigma_a=sig_a,
+                sigma_s0=sig_s, tfinal=1e9, t_plot=[0, 1e9], quiet=True)
+    if with_source:
+        prob["source"] = lambda x, y: np.exp(-6 * ((x - 0.3) ** 2 + y ** 2))
+    if substep:
+        prob.update(filterfunction=configs.exp_filter(2, 3.0), f_position="substep")
+    return starmap_init(prob)
+
+
+def make_solver(S, fs, T=None, fused=1, variant=0):
+    """variant 0 (AUTO): generated recording and backward kernels; 4: the
+    precompiled pair kernel and the precompiled backward kernels."""
     T = T or _tables(S, fs)
     solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
     solver.tune(_lib.SMG_TUNE_ADJ_FUSED, fused)
+    if variant:
+        solver.set_variant(variant)
     return solver, T
 
 
@@ -196,15 +207,17 @@ def test_backward_reports_device_time_and_repeats():
         np.testing.assert_array_equal(g1[j], g2[j])
 
 
-@pytest.mark.parametrize("bc,substep,fused,K", [(1, True, 1, 3), (0, False, 1, 0), (1, True, 0, 4)])
-def test_gradients_match_cpu_adjoint(bc, substep, fused, K):
+@pytest.mark.parametrize("bc,substep,fused,K,scalar,variant", [
+    (1, True, 1, 3, False, 0), (0, False, 1, 0, False, 0), (1, True, 0, 4, False, 0), (1, True, 1, 2, True, 0),
+    (1, True, 1, 3, False, 4), (0, True, 1, 7, True, 4)])
+def test_gradients_match_cpu_adjoint(bc, substep, fused, K, scalar, variant):
     """GPU dJ/dU(0), dJ/dsigma_t, dJ/dsigma_a and dJ/dq against the oracle's
     CPU adjoint of the same loop (oracle/adjoint_np.py), relative 1e-11 per
     output array."""
     from oracle import adjoint_np as A
-    S, fs = adjoint_problem(bc=bc, substep=substep)
+    S, fs = adjoint_problem(bc=bc, substep=substep, scalar=scalar)
     nsteps = 7
-    solver, T = make_solver(S, fs, fused=fused)
+    solver, T = make_solver(S, fs, fused=fused, variant=variant)
     try:
         solver.set_state(S.U0)
         solver.set_dt(fs["dt"])
@@ -216,7 +229,8 @@ def test_gradients_match_cpu_adjoint(bc, substep, fused, K):
         gU, gF = solver.backward(fields=[T.index[k] for k in keys])
     finally:
         solver.close()
-    ref = A.adjoint(S.par, nsteps, A.misfit_seed(obs))
+    # the oracle takes the reference's par (prepare() keeps its own adjusted copy)
+    ref = A.adjoint(adjoint_par(bc=bc, substep=substep, scalar=scalar), nsteps, A.misfit_seed(obs))
     assert np.isclose(J, ref["J"], rtol=1e-13)
 
     def close(got, want, what):
