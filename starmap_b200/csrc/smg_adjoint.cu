@@ -71,6 +71,15 @@ struct AdjData {
     double* V = nullptr;
     double* rec_state = nullptr;   // [2K+1][maxdest*cs]: destination values before each phase
     double* rec_w = nullptr;       // [2K+1][maxdest*cs]: destination coupling sums
+    // second recording (and work state) when there are several segments: the
+    // next segment is recomputed on rstream while the adjoint of the current
+    // one runs on the handle's stream
+    double* rec_state2 = nullptr;
+    double* rec_w2 = nullptr;
+    double* work2 = nullptr;
+    cudaStream_t rstream = nullptr;
+    cudaEvent_t ev_rec[2] = {nullptr, nullptr};    // recording into buffer b complete
+    cudaEvent_t ev_free[2] = {nullptr, nullptr};   // adjoint done reading buffer b
     int maxdest = 0;
     std::vector<double*> gfield;   // per user field: gradient slot (cs) or nullptr
     std::vector<double*> dEslot;   // per sigma field: d(decay)/d(sigma) slot (arrays)
@@ -457,17 +466,17 @@ smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec, 
     return a;
 }
 
-cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec) {
-    if (h->jit_rec) return smg::launch_jit_rec(h, mode, kf, U, wrec, prec, h->stream);
+cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec, cudaStream_t st) {
+    if (h->jit_rec) return smg::launch_jit_rec(h, mode, kf, U, wrec, prec, st);
     const int phase = mode == 1 ? 1 : 0;
     const smg::PairArgs a = rec_args(h, phase, U, wrec, prec);
     if (a.ndest == 0) return cudaSuccess;
     const unsigned nb = (unsigned)((long long)a.ngroups * a.nchunks * h->g.B[1] * h->g.B[2]);
     const int div = std::min(a.exact_recip[0], std::min(a.exact_recip[1], a.exact_recip[2]));
 #define SMG_REC(D)                                                                          \
-    if (mode == 1) smg::k_pair_rec<1, D><<<nb, 64, 0, h->stream>>>(a, kf);                 \
-    else if (mode == 2) smg::k_pair_rec<2, D><<<nb, 64, 0, h->stream>>>(a, kf);            \
-    else smg::k_pair_rec<0, D><<<nb, 64, 0, h->stream>>>(a, kf);
+    if (mode == 1) smg::k_pair_rec<1, D><<<nb, 64, 0, st>>>(a, kf);                        \
+    else if (mode == 2) smg::k_pair_rec<2, D><<<nb, 64, 0, st>>>(a, kf);                   \
+    else smg::k_pair_rec<0, D><<<nb, 64, 0, st>>>(a, kf);
     if (div == 2) { SMG_REC(2) }
     else if (div == 1) { SMG_REC(1) }
     else { SMG_REC(0) }
@@ -478,15 +487,15 @@ cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double*
 // One segment of ks steps from state U with recording, in smg_run's phase
 // order: A(k=1), then per step B and the fused A(k=2)A(k=1) -- A(k=2) alone
 // after the last step.  Phase r records into slot r (2ks+1 slots).
-cudaError_t record_segment(smg_handle* h, int64_t ks, double* U) {
+cudaError_t record_segment(smg_handle* h, int64_t ks, double* U, double* rec_w, double* rec_state, cudaStream_t st) {
     const AdjData* A = h->adj;
     const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
     for (int64_t r = 0; r <= 2 * ks; ++r) {
         const int kind = r == 0 ? 0 : (r & 1 ? 1 : (r < 2 * ks ? 2 : 3));
         const int mode = kind == 1 ? 1 : (kind == 2 ? 2 : 0);
         const int kf = kind == 3 ? 2 : 1;
-        const cudaError_t e = launch_rec(h, mode, kf, U, (double*)((char*)A->rec_w + vb * r),
-                                         (double*)((char*)A->rec_state + vb * r));
+        const cudaError_t e = launch_rec(h, mode, kf, U, (double*)((char*)rec_w + vb * r),
+                                         (double*)((char*)rec_state + vb * r), st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -501,6 +510,14 @@ void free_adj(smg_handle* h) {
     cudaFree(A->V);
     cudaFree(A->rec_state);
     cudaFree(A->rec_w);
+    cudaFree(A->rec_state2);
+    cudaFree(A->rec_w2);
+    cudaFree(A->work2);
+    if (A->rstream) cudaStreamDestroy(A->rstream);
+    for (int b = 0; b < 2; ++b) {
+        if (A->ev_rec[b]) cudaEventDestroy(A->ev_rec[b]);
+        if (A->ev_free[b]) cudaEventDestroy(A->ev_free[b]);
+    }
     for (double* p : A->gfield) cudaFree(p);
     for (double* p : A->dEslot) cudaFree(p);
     cudaFree(A->dDE);
@@ -640,7 +657,7 @@ cudaError_t backward_split(smg_handle* h, int64_t* launches) {
         if (!(s == A->nseg - 1 && A->tail_valid)) {
             cudaError_t e = cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream);
             if (e != cudaSuccess) return e;
-            e = record_segment(h, ks, A->work);
+            e = record_segment(h, ks, A->work, A->rec_w, A->rec_state, h->stream);
             if (e != cudaSuccess) return e;
             *launches += 2 * ks + 1;
         }
@@ -723,19 +740,42 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         return cudaGetLastError();
     };
     auto slot = [&](const double* base, int64_t r) { return (const double*)((const char*)base + vb * r); };
+    // recording buffer of segment s (the last segment uses the first, which
+    // smg_forward filled); with one buffer everything runs on the handle's stream
+    const bool dbl = A->rec_w2 != nullptr;
+    auto buf = [&](int64_t s) { return dbl ? (int)((A->nseg - 1 - s) & 1) : 0; };
+    double* RW[2] = {A->rec_w, A->rec_w2};
+    double* RS[2] = {A->rec_state, A->rec_state2};
+    double* WK[2] = {A->work, A->work2};
+    cudaError_t e;
+    auto recompute = [&](int64_t s) -> cudaError_t {
+        const int b = buf(s);
+        const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
+        cudaStream_t st = dbl ? A->rstream : h->stream;
+        cudaError_t r;
+        if (dbl && (r = cudaStreamWaitEvent(st, A->ev_free[b], 0)) != cudaSuccess) return r;
+        if ((r = cudaMemcpyAsync(WK[b], A->ckpt[s], sb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return r;
+        if ((r = record_segment(h, ks, WK[b], RW[b], RS[b], st)) != cudaSuccess) return r;
+        *launches += 2 * ks + 1;
+        if (dbl && (r = cudaEventRecord(A->ev_rec[b], st)) != cudaSuccess) return r;
+        return cudaSuccess;
+    };
+    if (dbl) {
+        // the recompute stream starts after the work already queued on the handle's stream
+        if ((e = cudaEventRecord(A->ev_free[1], h->stream)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(A->ev_free[0], h->stream)) != cudaSuccess) return e;
+    }
+    if (!A->tail_valid && (e = recompute(A->nseg - 1)) != cudaSuccess) return e;
     // the adjoint seed of the last phase's (A(k=2)) destinations, scaled
-    cudaError_t e = launch(1, 0, -1, nullptr, nullptr, 3);
+    e = launch(1, 0, -1, nullptr, nullptr, 3);
     if (e != cudaSuccess) return e;
     for (int64_t s = A->nseg - 1; s >= 0; --s) {
         const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
         const bool last = s == A->nseg - 1;
-        if (!(last && A->tail_valid)) {
-            e = cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream);
-            if (e != cudaSuccess) return e;
-            e = record_segment(h, ks, A->work);
-            if (e != cudaSuccess) return e;
-            *launches += 2 * ks + 1;
-        }
+        const int b = buf(s);
+        if (s >= 1 && (e = recompute(s - 1)) != cudaSuccess) return e;   // overlaps this segment's sweep
+        if (dbl && !(last && A->tail_valid) && (e = cudaStreamWaitEvent(h->stream, A->ev_rec[b], 0)) != cudaSuccess)
+            return e;
         for (int64_t l = last ? 2 * ks : 2 * ks - 1; l >= 0; --l) {
             const int64_t p = l + 1;   // the phase after l (its pointwise part is pending)
             int pkind = -1;
@@ -743,13 +783,14 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
             int nkind = -1;            // the phase before l (the targets' destination phase)
             if (l >= 1) nkind = ((l - 1) & 1) ? 1 : (l - 1 >= 2 ? 2 : (s == 0 ? 0 : 2));
             else if (s > 0) nkind = 1;
-            e = launch((l & 1) ? 1 : 0, 1, pkind, pkind < 0 ? nullptr : slot(A->rec_state, p),
-                       pkind < 0 ? nullptr : slot(A->rec_w, p), nkind);
+            e = launch((l & 1) ? 1 : 0, 1, pkind, pkind < 0 ? nullptr : slot(RS[b], p),
+                       pkind < 0 ? nullptr : slot(RW[b], p), nkind);
             if (e != cudaSuccess) return e;
         }
+        if (dbl && s >= 1 && (e = cudaEventRecord(A->ev_free[b], h->stream)) != cudaSuccess) return e;
     }
     // the first phase's (A(k=1)) pointwise part on its destinations
-    return launch(1, 0, 0, slot(A->rec_state, 0), slot(A->rec_w, 0), -1);
+    return launch(1, 0, 0, slot(RS[buf(0)], 0), slot(RW[buf(0)], 0), -1);
 }
 
 }  // namespace
@@ -781,7 +822,8 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
         K = 1;
         for (int64_t k = nsteps; k >= 1; --k) {
             const int64_t ns = (nsteps + k - 1) / k;
-            if ((double)sb * (ns + 2) + 2.0 * (double)vb * (2 * k + 1) <= budget) {
+            const double rec = 2.0 * (double)vb * (2 * k + 1) * (ns > 1 ? 2 : 1) + (ns > 1 ? (double)sb : 0.0);
+            if ((double)sb * (ns + 2) + rec <= budget) {
                 K = k;
                 break;
             }
@@ -809,10 +851,21 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
         A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * (2 * K + 1), h->stream));
         A_CUDA(h, cudaMemsetAsync(A->rec_state, 0, vb * (2 * K + 1), h->stream));
         A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
+        if (nseg > 1) {   // second recording: recompute overlapped with the sweep
+            A_CUDA(h, cudaMalloc(&A->rec_state2, vb * (2 * K + 1)));
+            A_CUDA(h, cudaMalloc(&A->rec_w2, vb * (2 * K + 1)));
+            A_CUDA(h, cudaMalloc(&A->work2, sb));
+            A_CUDA(h, cudaStreamCreateWithFlags(&A->rstream, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b) {
+                A_CUDA(h, cudaEventCreateWithFlags(&A->ev_rec[b], cudaEventDisableTiming));
+                A_CUDA(h, cudaEventCreateWithFlags(&A->ev_free[b], cudaEventDisableTiming));
+            }
+            A->bytes += sb + vb * (4 * K + 2);
+        }
     } else {
         for (double* p : A->gfield) cudaFree(p);
         for (double* p : A->dEslot) cudaFree(p);
-        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
+        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3) + (nseg > 1 ? sb + vb * (4 * K + 2) : 0);
     }
     A->nsteps = nsteps;
     A->ready = false;
@@ -886,7 +939,7 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
             rc = smg::run_steps(h, ks, false);
             if (rc != SMG_OK) return rc;
         } else {
-            A_CUDA(h, record_segment(h, ks, h->dU));
+            A_CUDA(h, record_segment(h, ks, h->dU, A->rec_w, A->rec_state, h->stream));
             h->last_launches += 2 * ks + 1;
         }
     }

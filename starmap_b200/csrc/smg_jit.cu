@@ -252,26 +252,25 @@ static __device__ __forceinline__ double2 dT_row(const double* v, int q, int n, 
     return S2(L2(v), L2(v + op));
 }
 // phase's pointwise adjoint from Y = (dU'/dW) lambda' (one substep: M = 1,
-// two: M = 2; F1 the first substep's filter), with its gradient
-// contributions; returns lambda = (dU'/dU) lambda'
+// two: M = 2; F1 the first substep's filter): returns lambda = (dU'/dU)
+// lambda', adds the sigma-gradient contribution to ds and the source
+// gradient to gq (dU'/dQ = dU'/dW)
 static __device__ __forceinline__ double pend(int M, double u, double w, double Y, double s, double E, double q,
-                                              double F1, double dE, double* gs, double* gq, int pt, double hdt) {
+                                              double F1, double dE, double& ds, double* gq, int pt, double hdt) {
     const double r = 1.0 - hdt * s * E;
-    double rho, dsdw = 0.0;
+    double rho, dsdw;
     if (M == 1) {
         rho = r / (hdt * E);
-        if (gs) dsdw = (-u * E + (w + q - s * u) * dE) / E;
+        dsdw = (-u * E + (w + q - s * u) * dE) / E;
     } else {
         const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
         rho = F1 * r * r * den;
-        if (gs) {
-            const double G0 = w + q - s * u;
-            const double V1 = F1 * (u + hdt * G0 * E);
-            const double G1 = w + q - s * V1;
-            dsdw = (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
-        }
+        const double G0 = w + q - s * u;
+        const double V1 = F1 * (u + hdt * G0 * E);
+        const double G1 = w + q - s * V1;
+        dsdw = (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
     }
-    if (gs) atomicAdd(gs + pt, dsdw * Y);
+    ds += dsdw * Y;
     if (gq) atomicAdd(gq + pt, Y);
     return rho * Y;
 }
@@ -726,11 +725,11 @@ void emit_adj_target(std::string& o, const smg_handle* h, int l, int i) {
         std::snprintf(b, sizeof b,
                       "        if (pm) {\n"
                       "          %s%s%s%s\n          %s%s\n"
-                      "          double* gs = Gt[%d]; double* gq = %s;\n"
+                      "          double* gq = %s;\n"
                       "          const long long rp = %lld + pt;\n",
                       adj_coef(h, f.s, "s").c_str(), adj_coef(h, f.E, "E").c_str(), adj_coef(h, f.q, "q").c_str(),
                       dEdecl.c_str(), filt ? adj_coef(h, f.F1, "fk1").c_str() : "",
-                      filt ? adj_coef(h, f.F2, "fk2").c_str() : "", f.s,
+                      filt ? adj_coef(h, f.F2, "fk2").c_str() : "",
                       f.q == h->field_zero ? "nullptr" : ("Gt[" + std::to_string(f.q) + "]").c_str(),
                       (long long)pslot * g.cs);
         o += b;
@@ -738,11 +737,11 @@ void emit_adj_target(std::string& o, const smg_handle* h, int l, int i) {
         const std::string F1 = filt ? "(pm_swap ? " + Yc(f.F2, "fk2") + " : " + Yc(f.F1, "fk1") + ")" : "1.0";
         const std::string dE0 = sarr ? "dE.x" : "dE", dE1 = sarr ? "dE.y" : "dE";
         std::snprintf(b, sizeof b,
-                      "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs, gq, pt, hdt);\n"
-                      "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs, gq, pt + 1, hdt);\n"
+                      "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs%d_0, gq, pt, hdt);\n"
+                      "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs%d_1, gq, pt + 1, hdt);\n"
                       "        }\n",
-                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), X(f.q, "q").c_str(), F0.c_str(), dE0.c_str(),
-                      Yc(f.s, "s").c_str(), Yc(f.E, "E").c_str(), Yc(f.q, "q").c_str(), F1.c_str(), dE1.c_str());
+                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), X(f.q, "q").c_str(), F0.c_str(), dE0.c_str(), f.s,
+                      Yc(f.s, "s").c_str(), Yc(f.E, "E").c_str(), Yc(f.q, "q").c_str(), F1.c_str(), dE1.c_str(), f.s);
         o += b;
     }
     // transposed couplings from phase l's destinations, in the fold order
@@ -794,8 +793,8 @@ void emit_adj_target(std::string& o, const smg_handle* h, int l, int i) {
 
 const char* kAdjArgs =
     "(double* __restrict__ Y, const DevField* __restrict__ F, const DevField* __restrict__ DE, "
-    "double* const* __restrict__ Gt, const double* __restrict__ PRE, const double* __restrict__ WR, int pm, "
-    "int pm_swap, int nm, int nm_swap, int coup, double hdt";
+    "double* const* __restrict__ Gt, const double* __restrict__ PRE, const double* __restrict__ WR, int pm_a, "
+    "int pm_swap_a, int nm_a, int nm_swap_a, int coup_a, double hdt";
 
 // kernels over the targets of backward phases of type l (l = 0: A phases,
 // whose sources are the B destinations; l = 1: B phases)
@@ -806,24 +805,60 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
     const long long cta_per_group = (long long)nchunks * g.B[1] * g.B[2];
     std::vector<KernelSrc> P;
     for (int l = 0; l < 2; ++l) {
-        const std::vector<int> T = l == 0 ? h->destB : h->destA;   // sources of the phase type
+        std::vector<int> T = l == 0 ? h->destB : h->destA;   // sources of the phase type
+        // targets sharing a sigma field side by side (fewer gradient atomics per group)
+        std::stable_sort(T.begin(), T.end(),
+                         [&](int a, int b) { return coefs_of(h, 1 - l, a).s < coefs_of(h, 1 - l, b).s; });
         if (T.empty()) continue;
         const int ng = ((int)T.size() + group - 1) / group;
         const int step = per > 0 ? per : ng;
+        // two forms of every kernel: the general one takes the kinds of the
+        // phases before and after at run time; the steady one has them fixed to
+        // the interior of a run (both neighbours two-substep phases: fused
+        // A-A around a B phase, B around an A phase), with far less code
+        for (int form = 0; form < 2; ++form)
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            KernelSrc K{std::string(kPrelude) + kAdjPrelude, "smg_adj_p" + std::to_string(l) + "_" + std::to_string(k0),
-                        l, (long long)(k1 - k0) * cta_per_group};
+            const std::string tag = form ? "s" : "p";
+            KernelSrc K{std::string(kPrelude) + kAdjPrelude,
+                        "smg_adj_" + tag + std::to_string(l) + "_" + std::to_string(k0), l + 2 * form,
+                        (long long)(k1 - k0) * cta_per_group};
             for (int k = k0; k < k1; ++k) {
                 K.src += "static __device__ __forceinline__ void smg_ag" + std::to_string(l) + "_" + std::to_string(k) +
                          std::string(kAdjArgs) + ", int x0, int y, int z) {\n"
                          "    const int x1 = x0 + 1; (void)x1;\n";
-                char b[256];
+                if (form)
+                    K.src += "    constexpr int pm = 2, nm = 2, coup = 1, pm_swap = " + std::to_string(l) +
+                             ", nm_swap = " + std::to_string(l) + ";\n";
+                else
+                    K.src += "    const int pm = pm_a, nm = nm_a, coup = coup_a, pm_swap = pm_swap_a, nm_swap = nm_swap_a;\n";
+                K.src += "    (void)pm; (void)nm; (void)coup; (void)pm_swap; (void)nm_swap;\n";
+                char b[512];
                 std::snprintf(b, sizeof b, "    const int pt = z * %lld + y * %lld + x0;\n", (long long)g.s2,
                               (long long)g.s1);
                 K.src += b;
-                for (int t = k * group; t < std::min<int>((k + 1) * group, (int)T.size()); ++t)
-                    emit_adj_target(K.src, h, l, T[t]);
+                // sigma-gradient contributions of the group, summed per field in
+                // registers and added to the field's gradient once per point
+                std::map<int, int> fields;   // sigma field -> a target on its grid
+                const int t0 = k * group, t1 = std::min<int>((k + 1) * group, (int)T.size());
+                for (int t = t0; t < t1; ++t) fields.emplace(coefs_of(h, 1 - l, T[t]).s, T[t]);
+                for (const auto& fe : fields) {
+                    std::snprintf(b, sizeof b, "    double gs%d_0 = 0.0, gs%d_1 = 0.0;\n", fe.first, fe.first);
+                    K.src += b;
+                }
+                for (int t = t0; t < t1; ++t) emit_adj_target(K.src, h, l, T[t]);
+                for (const auto& fe : fields) {
+                    const smg::DevComp& c = h->comps[fe.second];
+                    std::string cond = "pm";
+                    const char* ax[3] = {"x0", "y", "z"};
+                    for (int a = 0; a < 3; ++a)
+                        if (c.ext[a] < g.B[a]) cond += std::string(" && ") + ax[a] + " < " + std::to_string(c.ext[a]);
+                    std::snprintf(b, sizeof b,
+                                  "    if (%s) { double* gp = Gt[%d]; if (gp) { atomicAdd(gp + pt, gs%d_0); "
+                                  "if (x1 < %d) atomicAdd(gp + pt + 1, gs%d_1); } }\n",
+                                  cond.c_str(), fe.first, fe.first, c.ext[0], fe.first);
+                    K.src += b;
+                }
                 K.src += "}\n";
             }
             char b[1024];
@@ -842,7 +877,7 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
             K.src += b;
             for (int k = k0; k < k1; ++k)
                 K.src += "    case " + std::to_string(k) + ": smg_ag" + std::to_string(l) + "_" + std::to_string(k) +
-                         "(Y, F, DE, Gt, PRE, WR, pm, pm_swap, nm, nm_swap, coup, hdt, x0, y, z); break;\n";
+                         "(Y, F, DE, Gt, PRE, WR, pm_a, pm_swap_a, nm_a, nm_swap_a, coup_a, hdt, x0, y, z); break;\n";
             K.src += "    default: break;\n    }\n}\n";
             P.push_back(std::move(K));
         }
@@ -941,7 +976,7 @@ struct JitKernel {
 
 struct JitState {
     std::vector<CUmodule_t> mods;
-    std::vector<JitKernel> k[2];           // kernels of each phase type
+    std::vector<JitKernel> k[4];           // kernels of each phase type (adjoint: 2, 3 the steady forms)
     int block = 64;
     std::vector<cudaStream_t> side;        // concurrent kernels of a phase (inline layout)
     cudaEvent_t fork = nullptr;
@@ -1030,7 +1065,7 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
             J->k[P[i].phase].push_back(k);
         }
     }
-    const size_t nk = std::max(J->k[0].size(), J->k[1].size());
+    const size_t nk = std::max(std::max(J->k[0].size(), J->k[1].size()), std::max(J->k[2].size(), J->k[3].size()));
     if (nk > 1) {
         if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
         for (size_t i = 0; i < nk; ++i) {
@@ -1126,7 +1161,7 @@ int jit_build_adj(smg_handle* h, std::string& err) {
         }
         J->k[P[i].phase].push_back(k);
     }
-    const size_t nk = std::max(J->k[0].size(), J->k[1].size());
+    const size_t nk = std::max(std::max(J->k[0].size(), J->k[1].size()), std::max(J->k[2].size(), J->k[3].size()));
     if (nk > 1) {
         if (cudaEventCreateWithFlags(&J->fork, cudaEventDisableTiming) != cudaSuccess) {
             free_state(J);
@@ -1156,7 +1191,8 @@ cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_
                            double* Y, const DevField* DE, double* const* Gt, const double* pre, const double* W,
                            cudaStream_t s) {
     JitState* J = h->jit_adj;
-    const std::vector<JitKernel>& K = J->k[l];
+    const bool steady = coup == 1 && pm == 2 && nm == 2 && pm_swap == l && nm_swap == l;
+    const std::vector<JitKernel>& K = J->k[l + (steady ? 2 : 0)];
     if (K.empty()) return cudaSuccess;
     const DevField* F = h->dFieldTab;
     double hdt = h->hdt;
