@@ -264,6 +264,8 @@ typedef struct smg_batch smg_batch;
 #define SMG_BATCH_BARRIER_EXTRA    5  /* test hook: barrier expects one CTA more than launched (0/1) */
 #define SMG_BATCH_USE_GRAPH        6  /* 1: replay the launch sequence from a CUDA graph */
 #define SMG_BATCH_PERSISTENT       7  /* 1: one cooperative launch per block of steps; 0: one launch per phase */
+#define SMG_BATCH_JIT              8  /* 1: kernels generated per family of equal-structure instances (default;
+                                         built on the first run, NVRTC needed), 0: the precompiled kernels */
 
 int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch** out);
 void smg_batch_destroy(smg_batch* b);
@@ -279,6 +281,9 @@ int smg_batch_last_run_stats(smg_batch* b, double* ms, int64_t* launches);
 int smg_batch_tune(smg_batch* b, int32_t key, int64_t value);
 /* Current block, group, steps per launch and persistent grid size (0 when
  * the batch runs one launch per phase). */
+/* Whether the last runs used the generated family kernels, and how many
+ * families (sets of instances sharing kernels) the batch has. */
+int smg_batch_info(const smg_batch* b, int64_t* jit_active, int64_t* families);
 int smg_batch_config(const smg_batch* b, int64_t out[4]);
 /* Time probe_steps steps for each candidate configuration (block x group x
  * steps per launch), keep the fastest; every instance's state is restored. */

@@ -105,6 +105,7 @@ SIGNATURES = {
     "smg_jit_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32,
                                  C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),
+    "smg_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_batch_destroy": (None, [C.c_void_p]),
     "smg_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "smg_batch_instance": (C.c_void_p, [C.c_void_p, C.c_int32]),

@@ -14,7 +14,7 @@ from .solver import GpuSolver, build_problem, first_step, handle_tables, prepare
 
 __all__ = ["GpuBatch", "setup_batch"]
 
-BLOCK, GROUP, STEPS_PER_LAUNCH, SPIN_LIMIT, BARRIER_EXTRA, USE_GRAPH, PERSISTENT = 1, 2, 3, 4, 5, 6, 7
+BLOCK, GROUP, STEPS_PER_LAUNCH, SPIN_LIMIT, BARRIER_EXTRA, USE_GRAPH, PERSISTENT, JIT = 1, 2, 3, 4, 5, 6, 7, 8
 
 
 def _tables(S, fs):
@@ -67,6 +67,13 @@ class GpuBatch:
 
     def tune(self, key, value):
         check_batch(self._L.smg_batch_tune(self.b, int(key), int(value)), self.b)
+
+    def info(self):
+        """(generated family kernels used by the last runs, number of families)."""
+        j = _lib.C.c_int64()
+        f = _lib.C.c_int64()
+        check_batch(self._L.smg_batch_info(self.b, _lib.C.byref(j), _lib.C.byref(f)), self.b)
+        return bool(j.value), f.value
 
     def config(self):
         out = (_lib.C.c_int64 * 4)()

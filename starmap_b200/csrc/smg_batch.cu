@@ -160,6 +160,14 @@ struct smg_batch {
     double last_ms = 0;
     int64_t last_launches = 0;
     std::string err;
+    // generated family kernels (default): instances with the same structure
+    // share kernels, geometry from a per-instance table
+    int jit = 1;
+    smg::JitFamilySet* fam = nullptr;
+    bool fam_failed = false;
+    std::string fam_err;
+    bool graph_jit = false;
+    int64_t graph_launch_count = 0;
 };
 
 namespace {
@@ -289,8 +297,38 @@ cudaError_t launch_phase_batch(smg_batch* b, int mode, int kf) {
     return cudaGetLastError();
 }
 
+// the generated family kernels are built once (on the first run that wants
+// them); without NVRTC the batch keeps the precompiled kernels
+void ensure_fam(smg_batch* b) {
+    if (!b->jit || b->fam || b->fam_failed) return;
+    const smg_handle* h0 = b->inst[0];
+    std::string why;
+    if (smg::jit_family_build(b->inst, h0->jit_block, h0->jit_group, h0->jit_split > 0 ? h0->jit_split : 16,
+                              h0->jit_regs, b->fam, why) != SMG_OK) {
+        b->fam_failed = true;
+        b->fam_err = why;
+        b->fam = nullptr;
+    }
+}
+
+bool use_fam(const smg_batch* b) { return b->jit && b->fam; }
+
 cudaError_t enqueue_run(smg_batch* b, int64_t nsteps, int64_t* launches) {
     int64_t L = 0;
+    if (use_fam(b)) {
+        // A(k=1) [B AA]... B A(k=2), every phase one set of concurrent family kernels
+        if (nsteps > 0) {
+            cudaError_t e;
+            if ((e = smg::jit_family_phase(b->fam, 0, 1, b->stream, &L)) != cudaSuccess) return e;
+            for (int64_t k = 0; k < nsteps; ++k) {
+                if ((e = smg::jit_family_phase(b->fam, 1, 0, b->stream, &L)) != cudaSuccess) return e;
+                if ((e = smg::jit_family_phase(b->fam, k + 1 < nsteps ? 2 : 0, 2, b->stream, &L)) != cudaSuccess)
+                    return e;
+            }
+        }
+        if (launches) *launches = L;
+        return cudaSuccess;
+    }
     if (!b->persistent) {
         // A(k=1) [B AA]... B A(k=2): the fused sequence of the plain solver
         if (nsteps > 0) {
@@ -363,6 +401,7 @@ void smg_batch_destroy(smg_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
     free_items(b);
+    smg::jit_family_free(b->fam);
     cudaFree(b->d_bar);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -397,10 +436,12 @@ int smg_batch_run(smg_batch* b, int64_t nsteps) {
         B_CUDA(b, cudaStreamSynchronize(b->inst[i]->stream));
     }
     B_CUDA(b, cudaMemsetAsync(b->d_bar, 0, sizeof(BarrierState), b->stream));
+    ensure_fam(b);
+    if (use_fam(b)) B_CUDA(b, smg::jit_family_geometry(b->fam, b->inst, b->stream));
     int64_t launches = 0;
     bool graphed = false;
     if (b->use_graph && nsteps > 0) {
-        if (!b->graph || b->graph_steps != nsteps) {
+        if (!b->graph || b->graph_steps != nsteps || b->graph_jit != use_fam(b)) {
             if (b->graph) cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
             cudaGraph_t gr;
@@ -411,8 +452,13 @@ int smg_batch_run(smg_batch* b, int64_t nsteps) {
                 if (e1 == cudaSuccess && e2 == cudaSuccess) {
                     e = cudaGraphInstantiate(&b->graph, gr, 0);
                     cudaGraphDestroy(gr);
-                    if (e == cudaSuccess) b->graph_steps = nsteps;
-                    else b->graph = nullptr;
+                    if (e == cudaSuccess) {
+                        b->graph_steps = nsteps;
+                        b->graph_jit = use_fam(b);
+                        b->graph_launch_count = launches;
+                    } else {
+                        b->graph = nullptr;
+                    }
                 }
             }
             cudaGetLastError();   // a capture that is not supported falls back to direct launches
@@ -421,7 +467,7 @@ int smg_batch_run(smg_batch* b, int64_t nsteps) {
             B_CUDA(b, cudaEventRecord(b->ev0, b->stream));
             B_CUDA(b, cudaGraphLaunch(b->graph, b->stream));
             B_CUDA(b, cudaEventRecord(b->ev1, b->stream));
-            launches = b->persistent ? (nsteps + b->steps_per_launch - 1) / b->steps_per_launch : 2 * nsteps + 1;
+            launches = b->graph_launch_count;
             graphed = true;
         }
     }
@@ -477,10 +523,21 @@ int smg_batch_tune(smg_batch* b, int32_t key, int64_t value) {
         case SMG_BATCH_PERSISTENT:
             b->persistent = value != 0;
             break;
+        case SMG_BATCH_JIT:
+            if (value != 0 && value != 1) return bfail(b, SMG_EINVAL, "jit must be 0 or 1");
+            b->jit = (int)value;
+            break;
         default:
             return bfail(b, SMG_EINVAL, "smg_batch_tune: unknown key");
     }
     return build_items(b);
+}
+
+int smg_batch_info(const smg_batch* b, int64_t* jit_active, int64_t* families) {
+    if (!b) return bfail(nullptr, SMG_EINVAL, "smg_batch_info: NULL batch");
+    if (jit_active) *jit_active = use_fam(b) ? 1 : 0;
+    if (families) *families = smg::jit_family_count(b->fam);
+    return SMG_OK;
 }
 
 int smg_batch_config(const smg_batch* b, int64_t out[4]) {
@@ -507,7 +564,18 @@ int smg_batch_autotune(smg_batch* b, int64_t probe_steps, double* best_ms) {
     double best = 1e300;
     int bb = b->block, bg = b->group, bs = b->steps_per_launch;
     bool bp = b->persistent;
+    int bj = 0;
     int rc = SMG_OK;
+    // the generated family kernels first (when they can be built), then the
+    // precompiled configurations
+    b->jit = 1;
+    ensure_fam(b);
+    if (b->fam) {
+        if ((rc = smg_batch_run(b, probe_steps)) != SMG_OK) goto done;
+        best = b->last_ms;
+        bj = 1;
+    }
+    b->jit = 0;
     for (int blk : blocks)
         for (int grp : groups)
             for (int spl : spls) {
@@ -523,6 +591,7 @@ int smg_batch_autotune(smg_batch* b, int64_t probe_steps, double* best_ms) {
                     bg = grp;
                     bs = b->steps_per_launch;
                     bp = b->persistent;
+                    bj = 0;
                 }
             }
 done:
@@ -530,6 +599,7 @@ done:
     b->group = bg;
     b->steps_per_launch = bs;
     b->persistent = bp;
+    b->jit = bj;
     for (size_t i = 0; i < b->inst.size(); ++i) {
         const size_t bytes = (size_t)b->inst[i]->g.cs * b->inst[i]->n_sys * 8;
         cudaMemcpyAsync(b->inst[i]->dU, save[i], bytes, cudaMemcpyDeviceToDevice, b->stream);

@@ -14,6 +14,18 @@ struct smg_problem;
 namespace smg {
 struct AdjData;
 struct JitState;
+struct JitFamilySet;
+// per-instance geometry of the batched family kernels (layout shared with the
+// generated code)
+struct FamGeom {
+    double* U;
+    const DevField* F;
+    int n[4];
+    long long s1, s2, cs;
+    double h[3];
+    double rh[3];
+    double hdt;
+};
 }
 
 struct smg_handle {
@@ -123,6 +135,12 @@ int jit_build_adj(smg_handle* h, std::string& err);
 cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_swap, int nm, int nm_swap, double* Y,
                            const DevField* DE, double* const* Gt, const double* pre, const double* W, cudaStream_t s);
 int jit_adj_launches(const smg_handle* h, int l);
+int jit_family_build(const std::vector<smg_handle*>& inst, int block, int group, int split, int regs,
+                     JitFamilySet*& out, std::string& err);
+void jit_family_free(JitFamilySet*& S);
+cudaError_t jit_family_geometry(JitFamilySet* S, const std::vector<smg_handle*>& inst, cudaStream_t s);
+cudaError_t jit_family_phase(JitFamilySet* S, int mode, int kfilter, cudaStream_t s, int64_t* launches);
+int jit_family_count(const JitFamilySet* S);
 cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U, double* wrec, double* prec,
                            cudaStream_t s);
 std::string jit_source(const smg_handle* h, int block, int group);

@@ -162,6 +162,7 @@ Api& api() {
 // ---- source generation -------------------------------------------------------
 const char* kPrelude = R"(
 struct DevField { const double* p; double s; };
+struct FamGeom { double* U; const DevField* F; int n[4]; long long s1, s2, cs; double h[3]; double rh[3]; double hdt; };
 static __device__ __forceinline__ double ld1(const double* p) { return __ldg(p); }
 static __device__ __forceinline__ double2 ld2(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
 // correctly rounded d/h from y = RN(1/h): one or two Markstein correction
@@ -364,7 +365,10 @@ std::string xfast_cond(const smg_handle* h, int g2) {
 // the component's extent ends at x0 (that value is unused and not stored).
 // rec: also store the coupling sum W and the values before the update into
 // slot di of the recording buffers WR / PR (adjoint recording, smg_forward)
-void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bool rec) {
+// fam: the family form for the batched solver -- the grid sizes, strides,
+// spacing and decay step come from the instance's FamGeom at run time (names
+// N0..N2, S1, S2, CS, H0..H2, RH0..RH2), everything else stays a constant
+void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bool rec, bool fam = false) {
     const smg::DevComp& c = h->comps[j];
     const smg::DevGrid& g = h->g;
     char b[4096];
@@ -373,16 +377,24 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bo
     for (int a = 0; a < 3; ++a)
         if (c.ext[a] < g.B[a]) {
             if (!cond.empty()) cond += " && ";
-            cond += std::string(ax[a]) + " < " + std::to_string(c.ext[a]);
+            cond += std::string(ax[a]) + " < " +
+                    (fam ? "N" + std::to_string(a) + " + " + std::to_string(c.ext[a] - g.n[a]) : std::to_string(c.ext[a]));
         }
     o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
-    const bool v1_always = c.ext[0] % 2 == 0;
-    std::snprintf(b, sizeof b,
-                  "        double* Uj = U + pt + %lld;\n        const double2 u = *reinterpret_cast<const double2*>(Uj);\n",
-                  (long long)j * g.cs);
+    const bool v1_always = !fam && c.ext[0] % 2 == 0;
+    if (fam)
+        std::snprintf(b, sizeof b,
+                      "        double* Uj = U + pt + %dLL * CS;\n        const double2 u = *reinterpret_cast<const double2*>(Uj);\n",
+                      j);
+    else
+        std::snprintf(b, sizeof b,
+                      "        double* Uj = U + pt + %lld;\n        const double2 u = *reinterpret_cast<const double2*>(Uj);\n",
+                      (long long)j * g.cs);
     o += b;
     // the x stencil of the second point is evaluated only inside the extent
-    if (!v1_always) o += "        const bool v1 = x1 < " + std::to_string(c.ext[0]) + ";\n";
+    if (!v1_always)
+        o += "        const bool v1 = x1 < " +
+             (fam ? "N0 + " + std::to_string(c.ext[0] - g.n[0]) : std::to_string(c.ext[0])) + ";\n";
     const Coefs f = coefs_of(h, phase, j);
     const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
     o += "        " + coef_decl(h, f.q, "q") + coef_decl(h, f.s, "s") + coef_decl(h, f.E, "E") + "\n";
@@ -394,11 +406,37 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bo
         const int a = cp.code >> 1, g2 = cp.code & 1;
         const long long so = (long long)cp.src * g.cs;
         const int mode_div = h->exact_recip[a];
-        const std::string H = lit(g.h[a]), RH = lit(h->rh[a]), W = lit(cp.w);
-        const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
+        const std::string H = fam ? "H" + std::to_string(a) : lit(g.h[a]),
+                          RH = fam ? "RH" + std::to_string(a) : lit(h->rh[a]), W = lit(cp.w);
+        // the family form divides with two correction steps: exact for every
+        // normal spacing, so instances need not share one
+        const char* dv = fam ? "div1" : (mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0"));
         const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
         first = false;
-        if (a == 0 && !h->jit_xpair) {
+        if (fam) {
+            const std::string S = "Up + " + std::to_string(cp.src) + "LL * CS";
+            if (a == 0)
+                std::snprintf(b, sizeof b,
+                              "        { const double* S = %s;\n"
+                              "          const double a0 = ld1(S + hx0_%d), b0 = ld1(S + lx0_%d), a1 = ld1(S + (v1 ? hx1_%d : 0)), "
+                              "b1 = ld1(S + (v1 ? lx1_%d : 0));\n"
+                              "          const double tA = __dmul_rn(%s(__dsub_rn(a0, b0), %s, %s), %s);\n"
+                              "          const double tB = __dmul_rn(%s(__dsub_rn(a1, b1), %s, %s), %s);\n"
+                              "          %s }\n",
+                              S.c_str(), g2, g2, g2, g2, dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(),
+                              RH.c_str(), W.c_str(), fold);
+            else {
+                const char* n = a == 1 ? "y" : "z";
+                std::snprintf(b, sizeof b,
+                              "        { const double* S = %s;\n"
+                              "          const double2 hv = ld2(S + h%s_%d), lv = ld2(S + l%s_%d);\n"
+                              "          const double tA = __dmul_rn(%s(__dsub_rn(hv.x, lv.x), %s, %s), %s);\n"
+                              "          const double tB = __dmul_rn(%s(__dsub_rn(hv.y, lv.y), %s, %s), %s);\n"
+                              "          %s }\n",
+                              S.c_str(), n, g2, n, g2, dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(),
+                              RH.c_str(), W.c_str(), fold);
+            }
+        } else if (a == 0 && !h->jit_xpair) {
             // four 64-bit loads at the thread's stencil offsets
             std::snprintf(b, sizeof b,
                           "        { const double* S = Up + %lld;\n"
@@ -885,6 +923,93 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
     return P;
 }
 
+// ---- family kernels for the batched solver ---------------------------------
+// Instances whose generated code would be equal apart from the grid (same
+// closure and order, dimensions, boundary conditions, which coefficients are
+// arrays, filter mode) form a family and share kernels; the grid sizes,
+// strides, spacing and dt/2 of each instance come from a FamGeom table.  A
+// CTA takes one (instance, group, chunk, row) item from its kernel's list.
+void emit_fam_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group) {
+    const smg::DevGrid& g = h->g;
+    char b[1024];
+    const int d0 = k * group, d1 = std::min<int>((k + 1) * group, (int)D.size());
+    o += "static __device__ __forceinline__ void " + group_name(phase, k) +
+         "(const FamGeom& G, int kf, int mode, int x0, int y, int z) {\n"
+         "    double* U = G.U; const DevField* F = G.F; const double hdt = G.hdt;\n"
+         "    const int N0 = G.n[0], N1 = G.n[1], N2 = G.n[2];\n"
+         "    const long long S1 = G.s1, S2 = G.s2, CS = G.cs;\n"
+         "    const double H0 = G.h[0], H1 = G.h[1], H2 = G.h[2], RH0 = G.rh[0], RH1 = G.rh[1], RH2 = G.rh[2];\n"
+         "    (void)N0; (void)N1; (void)N2; (void)S2; (void)H0; (void)H1; (void)H2; (void)RH0; (void)RH1; (void)RH2;\n"
+         "    const int x1 = x0 + 1;\n"
+         "    const long long pt = z * S2 + y * S1 + x0;\n"
+         "    const double* Up = U + pt;\n"
+         "    (void)x1; (void)kf; (void)mode; (void)Up;\n";
+    bool used[3] = {false, false, false};
+    for (int i = d0; i < d1; ++i)
+        for (int q = h->comps[D[i]].cbeg; q < h->comps[D[i]].cend; ++q) used[h->coups[q].code >> 1] = true;
+    if (used[0])
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
+                          "    { int hi, lo; stencil(x0, N0, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
+                          "      stencil(x1, N0, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
+                          g2, g2, g2, g2, g.bc[0], g2, g2, g2, g.bc[0], g2, g2, g2);
+            o += b;
+        }
+    const char* an[3] = {"x", "y", "z"};
+    for (int a = 1; a < 3; ++a) {
+        if (!used[a]) continue;
+        const char* p = a == 1 ? "y" : "z";
+        const char* st = a == 1 ? "S1" : "S2";
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int h%s_%d, l%s_%d;\n"
+                          "    { int hi, lo; stencil(%s, N%d, %d, %d, hi, lo); h%s_%d = (int)((hi - %s) * %s); "
+                          "l%s_%d = (int)((lo - %s) * %s); }\n",
+                          an[a], g2, an[a], g2, p, a, g.bc[a], g2, an[a], g2, p, st, an[a], g2, p, st);
+            o += b;
+        }
+    }
+    for (int i = d0; i < d1; ++i) emit_dest(o, h, phase, D[i], i, false, true);
+    o += "}\n";
+}
+
+std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, int per) {
+    const smg::DevGrid& g = h->g;
+    std::vector<KernelSrc> P;
+    const int e0 = g.B[0] - g.n[0], e1 = g.B[1] - g.n[1];   // box extent beyond n (0 or 1)
+    for (int phase = 0; phase < 2; ++phase) {
+        const std::vector<int> D = phase_dests(h, phase);
+        if (D.empty()) continue;
+        const int ng = ((int)D.size() + group - 1) / group;
+        const int step = per > 0 ? per : ng;
+        for (int k0 = 0; k0 < ng; k0 += step) {
+            const int k1 = std::min(ng, k0 + step);
+            // grid: the item count, filled in per batch
+            KernelSrc K{kPrelude, "smg_fam_p" + std::to_string(phase) + "_" + std::to_string(k0), phase, k1 - k0};
+            for (int k = k0; k < k1; ++k) emit_fam_group(K.src, h, phase, k, D, group);
+            char b[1024];
+            std::snprintf(b, sizeof b,
+                          "extern \"C\" __global__ void __launch_bounds__(%d) %s(const FamGeom* __restrict__ geo, "
+                          "const int4* __restrict__ items, int kf, int mode) {\n"
+                          "    const int4 it = items[blockIdx.x];\n"
+                          "    const FamGeom& G = geo[it.x];\n"
+                          "    const int B1 = G.n[1] + %d;\n"
+                          "    const int y = it.w %% B1, z = it.w / B1;\n"
+                          "    const int x0 = 2 * (it.z * %d + (int)threadIdx.x);\n"
+                          "    if (x0 >= G.n[0] + %d) return;\n"
+                          "    switch (it.y) {\n",
+                          block, K.name.c_str(), e1, block, e0);
+            K.src += b;
+            for (int k = k0; k < k1; ++k)
+                K.src += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(G, kf, mode, x0, y, z); break;\n";
+            K.src += "    default: break;\n    }\n}\n";
+            P.push_back(std::move(K));
+        }
+    }
+    return P;
+}
+
 std::map<std::string, std::vector<std::vector<char>>> g_cubins;   // sources -> cubins, process-wide
 std::mutex g_cubin_mu;
 
@@ -1215,6 +1340,198 @@ cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_
 }
 
 int jit_adj_launches(const smg_handle* h, int l) { return h->jit_adj ? (int)h->jit_adj->k[l].size() : 0; }
+
+// ---- family kernels of a batch ---------------------------------------------
+struct FamKernel {
+    CUfunction_t fn = nullptr;
+    int phase = 0, fam = 0;
+    int4* d_items = nullptr;
+    long long nitems = 0;
+};
+
+struct JitFamilySet {
+    std::vector<CUmodule_t> mods;
+    std::vector<FamKernel> kernels;
+    std::vector<std::vector<int>> members;   // family -> batch instance indices
+    std::vector<FamGeom*> d_geo;             // family -> geometry table (one row per member)
+    int block = 64;
+    int nk[2] = {0, 0};
+    std::vector<cudaStream_t> side;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+};
+
+void jit_family_free(JitFamilySet*& S) {
+    if (!S) return;
+    for (auto& k : S->kernels) cudaFree(k.d_items);
+    for (FamGeom* g : S->d_geo) cudaFree(g);
+    for (cudaStream_t st : S->side) cudaStreamDestroy(st);
+    if (S->fork) cudaEventDestroy(S->fork);
+    for (cudaEvent_t e : S->join) cudaEventDestroy(e);
+    if (api().cu_ok)
+        for (CUmodule_t m : S->mods) api().ModuleUnload(m);
+    delete S;
+    S = nullptr;
+}
+
+int jit_family_build(const std::vector<smg_handle*>& inst, int block, int group, int split, int regs,
+                     JitFamilySet*& out, std::string& err) {
+    Api& a = api();
+    if (!a.cu_ok) {
+        err = a.cu_why;
+        return SMG_EINVAL;
+    }
+    for (const smg_handle* h : inst)
+        if (!(h->pair[0].ok && h->pair[1].ok) || std::min(h->exact_recip[0], std::min(h->exact_recip[1], h->exact_recip[2])) < 1) {
+            err = "an instance exceeds 32-bit offsets or has a subnormal grid spacing";
+            return SMG_EINVAL;
+        }
+    // families: instances whose generated code is the same text
+    std::map<std::string, int> fam_of;
+    std::vector<std::vector<KernelSrc>> fam_src;
+    JitFamilySet* S = new JitFamilySet();
+    S->block = block;
+    for (size_t i = 0; i < inst.size(); ++i) {
+        std::vector<KernelSrc> P = fam_programs(inst[i], block, group, split);
+        std::string key;
+        for (const auto& k : P) key += k.src;
+        auto it = fam_of.find(key);
+        if (it == fam_of.end()) {
+            it = fam_of.emplace(key, (int)fam_src.size()).first;
+            fam_src.push_back(std::move(P));
+            S->members.emplace_back();
+        }
+        S->members[it->second].push_back((int)i);
+    }
+    std::vector<KernelSrc> all;
+    std::vector<int> fam_idx;
+    for (size_t f = 0; f < fam_src.size(); ++f)
+        for (const auto& k : fam_src[f]) {
+            all.push_back(k);
+            fam_idx.push_back((int)f);
+        }
+    std::vector<std::vector<char>> cubins;
+    int rc = compile_programs(all, regs, false, cubins, err);
+    if (rc != SMG_OK) {
+        delete S;
+        return rc;
+    }
+    auto fail = [&](const std::string& m) {
+        err = m;
+        jit_family_free(S);
+        return SMG_ECUDA;
+    };
+    for (size_t i = 0; i < all.size(); ++i) {
+        CUmodule_t m = nullptr;
+        FamKernel K;
+        if (a.ModuleLoadData(&m, cubins[i].data()) != 0) return fail("cuModuleLoadData failed");
+        S->mods.push_back(m);
+        if (a.ModuleGetFunction(&K.fn, m, all[i].name.c_str()) != 0) return fail("cuModuleGetFunction " + all[i].name);
+        K.phase = all[i].phase;
+        K.fam = fam_idx[i];
+        // work items of the kernel's groups over the family's instances:
+        // (member, group, chunk, row), group-major so that CTAs running at
+        // the same time share code
+        const int k0 = std::stoi(all[i].name.substr(all[i].name.rfind('_') + 1));
+        const int k1 = k0 + (int)all[i].grid;
+        std::vector<int4> items;
+        const std::vector<int>& mem = S->members[K.fam];
+        for (int grp = k0; grp < k1; ++grp)
+            for (size_t li = 0; li < mem.size(); ++li) {
+                const smg_handle* h = inst[mem[li]];
+                const int tpr = (h->g.B[0] + 1) / 2;
+                const int nch = (tpr + block - 1) / block;
+                const int rows = h->g.B[1] * h->g.B[2];
+                for (int r = 0; r < rows; ++r)
+                    for (int c = 0; c < nch; ++c) items.push_back(make_int4((int)li, grp, c, r));
+            }
+        K.nitems = (long long)items.size();
+        if (cudaMalloc(&K.d_items, sizeof(int4) * std::max<size_t>(items.size(), 1)) != cudaSuccess)
+            return fail("cudaMalloc (batch items)");
+        if (!items.empty() &&
+            cudaMemcpy(K.d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail("cudaMemcpy (batch items)");
+        S->nk[K.phase]++;
+        S->kernels.push_back(K);
+    }
+    for (size_t f = 0; f < S->members.size(); ++f) {
+        FamGeom* g = nullptr;
+        if (cudaMalloc(&g, sizeof(FamGeom) * S->members[f].size()) != cudaSuccess) return fail("cudaMalloc (geometry)");
+        S->d_geo.push_back(g);
+    }
+    const int nk = std::max(S->nk[0], S->nk[1]);
+    if (nk > 1) {
+        if (cudaEventCreateWithFlags(&S->fork, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+        for (int i = 0; i < nk; ++i) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail("cudaStreamCreate");
+            S->side.push_back(st);
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail("cudaEventCreate");
+            S->join.push_back(ev);
+        }
+    }
+    out = S;
+    return SMG_OK;
+}
+
+// Geometry tables from the instances' current state (dt/2 follows smg_batch_set_dt).
+cudaError_t jit_family_geometry(JitFamilySet* S, const std::vector<smg_handle*>& inst, cudaStream_t s) {
+    for (size_t f = 0; f < S->members.size(); ++f) {
+        std::vector<FamGeom> G;
+        for (int i : S->members[f]) {
+            const smg_handle* h = inst[i];
+            FamGeom g{};
+            g.U = h->dU;
+            g.F = h->dFieldTab;
+            for (int a = 0; a < 3; ++a) {
+                g.n[a] = h->g.n[a];
+                g.h[a] = h->g.h[a];
+                g.rh[a] = h->rh[a];
+            }
+            g.s1 = h->g.s1;
+            g.s2 = h->g.s2;
+            g.cs = h->g.cs;
+            g.hdt = h->hdt;
+            G.push_back(g);
+        }
+        cudaError_t e = cudaMemcpyAsync(S->d_geo[f], G.data(), sizeof(FamGeom) * G.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;   // G is a host temporary
+    }
+    return cudaSuccess;
+}
+
+// One phase of every instance: the family kernels of the phase type, concurrent.
+cudaError_t jit_family_phase(JitFamilySet* S, int mode, int kfilter, cudaStream_t s, int64_t* launches) {
+    const int phase = mode == 1 ? 1 : 0;
+    int kf = kfilter, md = mode;
+    std::vector<const FamKernel*> K;
+    for (const auto& k : S->kernels)
+        if (k.phase == phase && k.nitems > 0) K.push_back(&k);
+    if (K.empty()) return cudaSuccess;
+    *launches += (int64_t)K.size();
+    auto go = [&](const FamKernel* k, cudaStream_t st) {
+        const FamGeom* geo = S->d_geo[k->fam];
+        const int4* items = k->d_items;
+        void* args[] = {&geo, &items, &kf, &md};
+        return api().LaunchKernel(k->fn, (unsigned)k->nitems, 1, 1, (unsigned)S->block, 1, 1, 0, st, args, nullptr) == 0
+                   ? cudaSuccess
+                   : cudaErrorLaunchFailure;
+    };
+    if (K.size() == 1) return go(K[0], s);
+    cudaError_t e = cudaEventRecord(S->fork, s);
+    if (e != cudaSuccess) return e;
+    for (size_t i = 0; i < K.size(); ++i) {
+        if ((e = cudaStreamWaitEvent(S->side[i], S->fork, 0)) != cudaSuccess) return e;
+        if ((e = go(K[i], S->side[i])) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(S->join[i], S->side[i])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, S->join[i], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int jit_family_count(const JitFamilySet* S) { return S ? (int)S->members.size() : 0; }
 
 }  // namespace smg
 

@@ -6,7 +6,7 @@ import pytest
 
 from starmap_b200 import configs, starmap_init
 from starmap_b200._lib import SmgError, SMG_ETIMEOUT
-from starmap_b200.batch import BARRIER_EXTRA, PERSISTENT, SPIN_LIMIT, STEPS_PER_LAUNCH, setup_batch
+from starmap_b200.batch import BARRIER_EXTRA, JIT, PERSISTENT, SPIN_LIMIT, STEPS_PER_LAUNCH, setup_batch
 from starmap_b200.solver import setup_gpu
 
 pytestmark = pytest.mark.gpu
@@ -35,6 +35,7 @@ def test_batch_matches_plain_runs(spl):
     nsteps = 13
     setups, batch = setup_batch(pars)
     try:
+        batch.tune(JIT, 0)   # the precompiled kernels
         if spl == 0:
             batch.tune(PERSISTENT, 0)
         else:
@@ -53,10 +54,42 @@ def test_batch_matches_plain_runs(spl):
         batch.close()
 
 
+def test_batch_family_kernels_match_plain_runs():
+    """Generated family kernels (the default): instances of equal structure and
+    different grids share kernels; every instance bit-identical to its plain run."""
+    probs = configs.batched_sweep(n_inst=10, seed=11, edges=(16, 24, 33, 40), orders=(1, 3, 5))
+    for p in probs[::2]:
+        p["bc"] = [1, 1]   # extrapolation boundaries: staggered extents differ from the cell counts
+    pars = [starmap_init(p) for p in probs]
+    nsteps = 9
+    setups, batch = setup_batch(pars)
+    try:
+        batch.set_states([S.U0 for S, _ in setups])
+        batch.set_dt([fs["dt"] for _, fs in setups])
+        batch.run(nsteps)
+        used, fams = batch.info()
+        assert used and 1 <= fams <= 6
+        for i, par in enumerate(pars):
+            ref = plain_reference(par, nsteps)
+            got = batch.get_state(i)
+            for j in ref:
+                np.testing.assert_array_equal(got[j], ref[j])
+        # a second run replays the captured graph with fresh geometry and state
+        batch.set_states([S.U0 for S, _ in setups])
+        batch.run(nsteps)
+        got = batch.get_state(3)
+        ref = plain_reference(pars[3], nsteps)
+        for j in ref:
+            np.testing.assert_array_equal(got[j], ref[j])
+    finally:
+        batch.close()
+
+
 def test_batch_barrier_timeout_is_reported_and_recoverable():
     pars = small_batch(n=3)
     setups, batch = setup_batch(pars)
     try:
+        batch.tune(JIT, 0)   # the persistent kernel's grid barrier
         batch.set_states([S.U0 for S, _ in setups])
         batch.set_dt([fs["dt"] for _, fs in setups])
         batch.tune(SPIN_LIMIT, 20000)
