@@ -104,7 +104,7 @@ struct smg_handle {
     smg::JitState* jit = nullptr;    // problem-specialised kernels (SMG_VARIANT_JIT)
     smg::JitState* jit_rec = nullptr;  // the same with adjoint recording (smg_forward / smg_backward)
     smg::JitState* jit_adj = nullptr;  // generated backward-phase kernels (smg_backward)
-    int jit_block = 64, jit_group = 4, jit_regs = 64;
+    int jit_block = 64, jit_group = 8, jit_regs = 80;
     int jit_split = 16;              // groups per NVRTC program (0: one program per phase)
     int jit_calls = 0;               // 1: one kernel per phase calling separately compiled groups
     int jit_xpair = 0;               // x differences from aligned 128-bit pairs (1) or 64-bit loads (0)

@@ -47,6 +47,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -522,6 +523,14 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bo
     o += "    }\n";
 }
 
+// __launch_bounds__ arguments: the CTA size and, with a register limit per
+// thread (regs > 0), the resident CTAs per SM that this limit allows (the
+// bound takes precedence over --maxrregcount for kernels)
+std::string bounds(int block, int regs) {
+    if (regs <= 0) return std::to_string(block);
+    return std::to_string(block) + ", " + std::to_string(std::max(1, 65536 / (block * regs)));
+}
+
 std::string group_name(int phase, int k) { return "smg_g" + std::to_string(phase) + "_" + std::to_string(k); }
 std::string group_args(bool rec) {
     return std::string("(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, "
@@ -591,7 +600,7 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
     if (!inl)
         for (int k = k0; k < k1; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + group_args(rec) + ";\n";
     std::snprintf(b, sizeof b,
-                  "extern \"C\" __global__ void __launch_bounds__(%d) %s(double* __restrict__ U, "
+                  "extern \"C\" __global__ void __launch_bounds__(%s) %s(double* __restrict__ U, "
                   "const DevField* __restrict__ F, double hdt, int kf, int mode%s) {\n"
                   "    const int bid = blockIdx.x;\n"
                   "    const int grp = %d + bid / %lld;\n"
@@ -601,7 +610,8 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
                   "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
                   "    if (x0 >= %d) return;\n"
                   "    switch (grp) {\n",
-                  block, name.c_str(), rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", k0, per, per,
+                  bounds(block, h->jit_regs).c_str(), name.c_str(),
+                  rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", k0, per, per,
                   nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
     o += b;
     for (int k = k0; k < k1; ++k)
@@ -616,6 +626,218 @@ std::vector<int> phase_dests(const smg_handle* h, int phase) {
     for (const auto& d : h->pair[phase].dests) D.push_back((int)((long long)d.off / h->g.cs));
     if (D.empty()) D = phase == 0 ? h->destA : h->destB;
     return D;
+}
+
+// ---- groups that share loads (the inline layout) ----------------------------
+// Destinations of one phase are grouped by grid type (one extent condition per
+// group) and, within a grid type, greedily by the (axis, source) pairs of
+// their couplings, so that the destinations of a group read many of the same
+// source rows.  The group's code loads every distinct source value and
+// coefficient once, at its first use, and later destinations reuse the
+// register: a phase never writes its sources, so a value loaded before an
+// earlier destination's store is still current.
+std::vector<std::vector<int>> shared_groups(const smg_handle* h, int phase, int group) {
+    const std::vector<int> D = phase_dests(h, phase);
+    std::vector<std::set<std::pair<int, int>>> K(D.size());
+    std::map<std::vector<int>, std::vector<int>> by_ext;   // extents -> positions in D
+    std::vector<std::vector<int>> order;
+    for (size_t p = 0; p < D.size(); ++p) {
+        const smg::DevComp& c = h->comps[D[p]];
+        for (int q = c.cbeg; q < c.cend; ++q) K[p].insert({h->coups[q].code >> 1, h->coups[q].src});
+        std::vector<int> e(c.ext, c.ext + 3);
+        if (!by_ext.count(e)) order.push_back(e);
+        by_ext[e].push_back((int)p);
+    }
+    std::vector<std::vector<int>> G;
+    for (const auto& e : order) {
+        std::vector<int> left = by_ext[e];
+        while (!left.empty()) {
+            std::vector<int> g{left.front()};
+            left.erase(left.begin());
+            std::set<std::pair<int, int>> ks = K[g[0]];
+            while ((int)g.size() < group && !left.empty()) {
+                size_t best = 0;
+                int bestn = -1;
+                for (size_t i = 0; i < left.size(); ++i) {
+                    int n = 0;
+                    for (const auto& k : K[left[i]]) n += (int)ks.count(k);
+                    if (n > bestn) {
+                        bestn = n;
+                        best = i;
+                    }
+                }
+                g.push_back(left[best]);
+                ks.insert(K[left[best]].begin(), K[left[best]].end());
+                left.erase(left.begin() + best);
+            }
+            G.push_back(std::move(g));
+        }
+    }
+    return G;
+}
+
+// one group's device function (inline layout): positions P into the phase's
+// destination list (the position is the destination's recording slot)
+void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, bool rec) {
+    const smg::DevGrid& g = h->g;
+    const std::vector<int> D = phase_dests(h, phase);
+    char b[4096];
+    o += "static __device__ __forceinline__ void " + group_name(phase, k) + group_args(rec) + " {\n";
+    std::snprintf(b, sizeof b,
+                  "    const int x1 = x0 + 1;\n"
+                  "    const int pt = z * %lld + y * %lld + x0;\n"
+                  "    const double* Up = U + pt;\n"
+                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up;\n",
+                  (long long)g.s2, (long long)g.s1);
+    o += b;
+    bool used[3] = {false, false, false};
+    for (int p : P)
+        for (int q = h->comps[D[p]].cbeg; q < h->comps[D[p]].cend; ++q) used[h->coups[q].code >> 1] = true;
+    if (used[0])
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
+                          "    { int hi, lo; stencil(x0, %d, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
+                          "      stencil(x1, %d, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
+                          g2, g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2);
+            o += b;
+        }
+    const char* an[3] = {"x", "y", "z"};
+    for (int a = 1; a < 3; ++a) {
+        if (!used[a]) continue;
+        const long long st = a == 1 ? g.s1 : g.s2;
+        const char* pp = a == 1 ? "y" : "z";
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int h%s_%d, l%s_%d;\n"
+                          "    { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); h%s_%d = (hi - %s) * %lld; "
+                          "l%s_%d = (lo - %s) * %lld; }\n",
+                          an[a], g2, an[a], g2, pp, g.n[a], g.bc[a], g2, an[a], g2, pp, st, an[a], g2, pp, st);
+            o += b;
+        }
+    }
+    // the group's extent condition (all its destinations share a grid)
+    const smg::DevComp& c0 = h->comps[D[P[0]]];
+    std::string cond;
+    const char* ax[3] = {"x0", "y", "z"};
+    for (int a = 0; a < 3; ++a)
+        if (c0.ext[a] < g.B[a]) {
+            if (!cond.empty()) cond += " && ";
+            cond += std::string(ax[a]) + " < " + std::to_string(c0.ext[a]);
+        }
+    o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
+    const bool v1_always = c0.ext[0] % 2 == 0;
+    const std::string v1 = v1_always ? "true" : "v1";
+    if (!v1_always) o += "    const bool v1 = x1 < " + std::to_string(c0.ext[0]) + ";\n";
+    const std::string sel1 = v1_always ? "" : "v1 ? ", sel2 = v1_always ? "" : " : 0";
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    std::set<int> coef_done;
+    std::set<std::pair<int, int>> val_done;
+    auto coef = [&](int f) {
+        const std::string n = "C" + std::to_string(f);
+        if (coef_done.insert(f).second) {
+            if (is_array(h, f)) std::snprintf(b, sizeof b, "    const double2 %s = ld2(fp(F, %d) + pt);\n", n.c_str(), f);
+            else std::snprintf(b, sizeof b, "    const double %s = fs(F, %d);\n", n.c_str(), f);
+            o += b;
+        }
+        return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
+    };
+    for (int p : P) {
+        const int j = D[p];
+        const smg::DevComp& c = h->comps[j];
+        const Coefs f = coefs_of(h, phase, j);
+        const auto q = coef(f.q), sv = coef(f.s), E = coef(f.E);
+        std::pair<std::string, std::string> k1{"1.0", "1.0"}, k2{"1.0", "1.0"};
+        if (filt) {
+            k1 = coef(f.F1);
+            k2 = coef(f.F2);
+        }
+        // source values of this destination's couplings not loaded yet
+        for (int qq = c.cbeg; qq < c.cend; ++qq) {
+            const smg::DevCoup& cp = h->coups[qq];
+            const int a = cp.code >> 1, g2 = cp.code & 1;
+            if (!val_done.insert({a, cp.src}).second) continue;
+            const long long so = (long long)cp.src * g.cs;
+            if (a == 0)
+                std::snprintf(b, sizeof b,
+                              "    const double X%d_a0 = ld1(Up + %lld + hx0_%d), X%d_b0 = ld1(Up + %lld + lx0_%d), "
+                              "X%d_a1 = ld1(Up + %lld + (%shx1_%d%s)), X%d_b1 = ld1(Up + %lld + (%slx1_%d%s));\n",
+                              cp.src, so, g2, cp.src, so, g2, cp.src, so, sel1.c_str(), g2, sel2.c_str(), cp.src, so,
+                              sel1.c_str(), g2, sel2.c_str());
+            else
+                std::snprintf(b, sizeof b,
+                              "    const double2 %c%d_h = ld2(Up + %lld + h%s_%d), %c%d_l = ld2(Up + %lld + l%s_%d);\n",
+                              a == 1 ? 'Y' : 'Z', cp.src, so, an[a], g2, a == 1 ? 'Y' : 'Z', cp.src, so, an[a], g2);
+            o += b;
+        }
+        std::snprintf(b, sizeof b,
+                      "    {\n        double* Uj = U + pt + %lld;\n"
+                      "        const double2 u = *reinterpret_cast<const double2*>(Uj);\n"
+                      "        double SA = 0.0, SB = 0.0;\n",
+                      (long long)j * g.cs);
+        o += b;
+        bool first = true;
+        for (int qq = c.cbeg; qq < c.cend; ++qq) {
+            const smg::DevCoup& cp = h->coups[qq];
+            const int a = cp.code >> 1;
+            const int mode_div = h->exact_recip[a];
+            const std::string H = lit(g.h[a]), RH = lit(h->rh[a]), W = lit(cp.w);
+            const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
+            const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
+            first = false;
+            std::string dA, dB;
+            if (a == 0) {
+                dA = "__dsub_rn(X" + std::to_string(cp.src) + "_a0, X" + std::to_string(cp.src) + "_b0)";
+                dB = "__dsub_rn(X" + std::to_string(cp.src) + "_a1, X" + std::to_string(cp.src) + "_b1)";
+            } else {
+                const std::string n = std::string(1, a == 1 ? 'Y' : 'Z') + std::to_string(cp.src);
+                dA = "__dsub_rn(" + n + "_h.x, " + n + "_l.x)";
+                dB = "__dsub_rn(" + n + "_h.y, " + n + "_l.y)";
+            }
+            std::snprintf(b, sizeof b,
+                          "        { const double tA = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                          "          const double tB = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                          "          %s }\n",
+                          dv, dA.c_str(), H.c_str(), RH.c_str(), W.c_str(), dv, dB.c_str(), H.c_str(), RH.c_str(),
+                          W.c_str(), fold);
+            o += b;
+        }
+        o += "        double u0 = u.x, u1 = u.y;\n";
+        if (rec) {
+            const long long so = (long long)p * g.cs;
+            std::snprintf(b, sizeof b,
+                          "        { double* wp = WR + pt + %lld; double* pp = PR + pt + %lld;\n"
+                          "          if (%s) { *reinterpret_cast<double2*>(wp) = make_double2(-SA, -SB); "
+                          "*reinterpret_cast<double2*>(pp) = u; } else { wp[0] = -SA; pp[0] = u.x; } }\n",
+                          so, so, v1.c_str());
+            o += b;
+        }
+        auto sub = [&]() {
+            std::snprintf(b, sizeof b, "u0 = upd(u0, -SA, %s, %s, %s, hdt); u1 = upd(u1, -SB, %s, %s, %s, hdt);",
+                          q.first.c_str(), sv.first.c_str(), E.first.c_str(), q.second.c_str(), sv.second.c_str(),
+                          E.second.c_str());
+            return std::string(b);
+        };
+        auto fl = [&](const std::pair<std::string, std::string>& F) {
+            return filt ? " u0 = __dmul_rn(u0, " + F.first + "); u1 = __dmul_rn(u1, " + F.second + ");" : std::string();
+        };
+        if (phase == 0) {
+            const std::string one =
+                "        " + sub() +
+                (filt ? " u0 = __dmul_rn(u0, kf == 1 ? " + k1.first + " : " + k2.first + "); u1 = __dmul_rn(u1, kf == 1 ? " +
+                            k1.second + " : " + k2.second + ");"
+                      : std::string()) +
+                "\n";
+            const std::string two = "        " + sub() + fl(k2) + "\n        " + sub() + fl(k1) + "\n";
+            if (h->filter_mode == SMG_FILTER_FULL) o += one;
+            else o += "        if (mode == 0) {\n" + one + "        } else {\n" + two + "        }\n";
+        } else {
+            o += "        " + sub() + fl(k1) + "\n        " + sub() + fl(k2) + "\n";
+        }
+        if (v1_always) o += "        *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1);\n    }\n";
+        else o += "        if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1); else *Uj = u0;\n    }\n";
+    }
+    o += "    }\n}\n";
 }
 
 // One generated kernel: its program, phase type, name and CTA count.
@@ -664,13 +886,14 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
         if (D.empty()) continue;
-        const int ng = ((int)D.size() + group - 1) / group;
+        const std::vector<std::vector<int>> G = shared_groups(h, phase, group);
+        const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
             KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase,
                         (long long)(k1 - k0) * cta_per_group};
-            for (int j = k0; j < k1; ++j) emit_group(k.src, h, phase, j, D, group, true, rec);
+            for (int j = k0; j < k1; ++j) emit_shared_group(k.src, h, phase, j, G[j], rec);
             emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
             P.push_back(std::move(k));
         }
@@ -901,7 +1124,7 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
             }
             char b[1024];
             std::snprintf(b, sizeof b,
-                          "extern \"C\" __global__ void __launch_bounds__(%d) %s%s) {\n"
+                          "extern \"C\" __global__ void __launch_bounds__(%s) %s%s) {\n"
                           "    const int bid = blockIdx.x;\n"
                           "    const int grp = %d + bid / %lld;\n"
                           "    const int rest = bid %% %lld;\n"
@@ -910,7 +1133,8 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
                           "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
                           "    if (x0 >= %d) return;\n"
                           "    switch (grp) {\n",
-                          block, K.name.c_str(), kAdjArgs, k0, cta_per_group, cta_per_group, nchunks, nchunks, g.B[1],
+                          bounds(block, h->jit_regs).c_str(), K.name.c_str(), kAdjArgs, k0, cta_per_group,
+                          cta_per_group, nchunks, nchunks, g.B[1],
                           g.B[1], block, g.B[0]);
             K.src += b;
             for (int k = k0; k < k1; ++k)
@@ -990,7 +1214,7 @@ std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, i
             for (int k = k0; k < k1; ++k) emit_fam_group(K.src, h, phase, k, D, group);
             char b[1024];
             std::snprintf(b, sizeof b,
-                          "extern \"C\" __global__ void __launch_bounds__(%d) %s(const FamGeom* __restrict__ geo, "
+                          "extern \"C\" __global__ void __launch_bounds__(%s) %s(const FamGeom* __restrict__ geo, "
                           "const int4* __restrict__ items, int kf, int mode) {\n"
                           "    const int4 it = items[blockIdx.x];\n"
                           "    const FamGeom& G = geo[it.x];\n"
@@ -999,7 +1223,7 @@ std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, i
                           "    const int x0 = 2 * (it.z * %d + (int)threadIdx.x);\n"
                           "    if (x0 >= G.n[0] + %d) return;\n"
                           "    switch (it.y) {\n",
-                          block, K.name.c_str(), e1, block, e0);
+                          bounds(block, h->jit_regs).c_str(), K.name.c_str(), e1, block, e0);
             K.src += b;
             for (int k = k0; k < k1; ++k)
                 K.src += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(G, kf, mode, x0, y, z); break;\n";
