@@ -111,17 +111,25 @@ class GpuSolver:
         ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)(*[dptr(a) for a in arrs])
         check(self._L.smg_set_state(self.h, ptrs), self.h)
 
-    def get_state(self, which=None):
+    def get_state(self, which=None, out=None):
+        """Components ``which`` (default all) as arrays of their extents.  With
+        ``out`` ({j: float64 buffer of the component's size}, e.g. in pinned
+        host memory) the values are written there."""
         which = range(self.n_sys) if which is None else which
-        out = {}
+        res = {}
         ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
         for j in which:
             e = self.extents(j)
-            buf = np.empty(int(np.prod(e)), dtype=np.float64)
-            out[j] = (buf, e)
+            if out is not None:
+                buf = out[j].reshape(-1, order="A")
+                if buf.dtype != np.float64 or buf.size != int(np.prod(e)) or not buf.flags.c_contiguous:
+                    raise ValueError(f"out[{j}] must be a contiguous float64 buffer of {int(np.prod(e))} values")
+            else:
+                buf = np.empty(int(np.prod(e)), dtype=np.float64)
+            res[j] = (buf, e)
             ptrs[j] = dptr(buf)
         check(self._L.smg_get_state(self.h, ptrs), self.h)
-        return {j: buf.reshape(e, order="F") for j, (buf, e) in out.items()}
+        return {j: buf.reshape(e, order="F") for j, (buf, e) in res.items()}
 
     def set_field(self, k, val):
         if np.ndim(val) == 0:
