@@ -50,6 +50,7 @@
 #include <set>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/starmap_gpu.h"
@@ -943,113 +944,206 @@ int compile_one(const std::string& src, int regs, bool rdc, std::vector<char>& c
 // The kinds of r+1 and r-1 arrive at run time as (number of substeps, filter
 // order swapped); everything else is a constant.
 
-// coefficient value of field f at the point pair (two names: .x/.y or scalar)
-std::string adj_coef(const smg_handle* h, int f, const char* n) {
-    char b[256];
-    if (is_array(h, f)) std::snprintf(b, sizeof b, "const double2 %s = L2(fp(F, %d) + pt); ", n, f);
-    else std::snprintf(b, sizeof b, "const double %s = fs(F, %d); ", n, f);
-    return b;
-}
 
-void emit_adj_target(std::string& o, const smg_handle* h, int l, int i) {
-    const smg::DevGrid& g = h->g;
-    const smg::DevComp& c = h->comps[i];
-    char b[4096];
-    // i as a destination of the other phase type: its slot and coefficients
-    const std::vector<int> Dother = phase_dests(h, 1 - l);
-    int pslot = -1;
-    for (size_t k = 0; k < Dother.size(); ++k)
-        if (Dother[k] == i) pslot = (int)k;
-    const Coefs f = coefs_of(h, 1 - l, i);
-    std::string cond;
-    const char* ax[3] = {"x0", "y", "z"};
-    for (int a = 0; a < 3; ++a)
-        if (c.ext[a] < g.B[a]) {
-            if (!cond.empty()) cond += " && ";
-            cond += std::string(ax[a]) + " < " + std::to_string(c.ext[a]);
-        }
-    o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
-    const bool v1_always = c.ext[0] % 2 == 0;
-    std::snprintf(b, sizeof b, "        double* Yi = Y + pt + %lld;\n        const bool v1 = %s;\n"
-                  "        const double2 yv = L2(Yi); double l0 = yv.x, l1 = yv.y;\n",
-                  (long long)i * g.cs, v1_always ? "true" : ("x1 < " + std::to_string(c.ext[0])).c_str());
-    o += b;
-    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
-    auto X = [&](int fi, const char* n) { return cx(h, fi, n); };
-    auto Yc = [&](int fi, const char* n) { return cy(h, fi, n); };
-    if (pslot >= 0) {
-        std::string dEdecl;
-        const bool sarr = is_array(h, f.s);
-        // d(decay)/d(sigma) of sigma field f.s: the table DE holds an array or a scalar
-        dEdecl = sarr ? "const double2 dE = L2(fp(DE, " + std::to_string(f.s) + ") + pt); "
-                      : "const double dE = fs(DE, " + std::to_string(f.s) + "); ";
-        std::snprintf(b, sizeof b,
-                      "        if (pm) {\n"
-                      "          %s%s%s%s\n          %s%s\n"
-                      "          double* gq = %s;\n"
-                      "          const long long rp = %lld + pt;\n",
-                      adj_coef(h, f.s, "s").c_str(), adj_coef(h, f.E, "E").c_str(), adj_coef(h, f.q, "q").c_str(),
-                      dEdecl.c_str(), filt ? adj_coef(h, f.F1, "fk1").c_str() : "",
-                      filt ? adj_coef(h, f.F2, "fk2").c_str() : "",
-                      f.q == h->field_zero ? "nullptr" : ("Gt[" + std::to_string(f.q) + "]").c_str(),
-                      (long long)pslot * g.cs);
-        o += b;
-        const std::string F0 = filt ? "(pm_swap ? " + X(f.F2, "fk2") + " : " + X(f.F1, "fk1") + ")" : "1.0";
-        const std::string F1 = filt ? "(pm_swap ? " + Yc(f.F2, "fk2") + " : " + Yc(f.F1, "fk1") + ")" : "1.0";
-        const std::string dE0 = sarr ? "dE.x" : "dE", dE1 = sarr ? "dE.y" : "dE";
-        std::snprintf(b, sizeof b,
-                      "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs%d_0, gq, pt, hdt);\n"
-                      "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs%d_1, gq, pt + 1, hdt);\n"
-                      "        }\n",
-                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), X(f.q, "q").c_str(), F0.c_str(), dE0.c_str(), f.s,
-                      Yc(f.s, "s").c_str(), Yc(f.E, "E").c_str(), Yc(f.q, "q").c_str(), F1.c_str(), dE1.c_str(), f.s);
-        o += b;
-    }
-    // transposed couplings from phase l's destinations, in the fold order
-    // of smg_adjoint.cu's tables (destination order, then sumcell order)
-    const std::vector<int> Dl = phase_dests(h, l);
-    std::string body;
-    for (int j : Dl)
+// transposed-coupling terms of target i in phase type l: (destination j,
+// axis, grid flag of i along the axis, M_d(j,i)/h), in the fold order of
+// smg_adjoint.cu's tables (destination order, then sumcell order)
+std::vector<std::tuple<int, int, int, double>> adj_terms(const smg_handle* h, int l, int i) {
+    std::vector<std::tuple<int, int, int, double>> T;
+    for (int j : phase_dests(h, l))
         for (int q = h->comps[j].cbeg; q < h->comps[j].cend; ++q) {
             const smg::DevCoup& cp = h->coups[q];
             if (cp.src != i) continue;
-            const int a = cp.code >> 1, g2 = cp.code & 1;
-            const std::string fw = lit(cp.w / g.h[a]);
-            if (a == 0) {
-                std::snprintf(b, sizeof b,
-                              "          { const double* v = Y + pt + %lld;\n"
-                              "            a0 += %s * dT(v, x0, %d, %d, %d, 1);\n"
-                              "            if (v1) a1 += %s * dT(v + 1, x1, %d, %d, %d, 1); }\n",
-                              (long long)j * g.cs, fw.c_str(), g.n[0], g.bc[0], g2, fw.c_str(), g.n[0], g.bc[0], g2);
-            } else {
-                const long long st = a == 1 ? g.s1 : g.s2;
-                std::snprintf(b, sizeof b,
-                              "          { const double2 d = dT_row(Y + pt + %lld, %s, %d, %d, %d, %lld);\n"
-                              "            a0 += %s * d.x; a1 += %s * d.y; }\n",
-                              (long long)j * g.cs, a == 1 ? "y" : "z", g.n[a], g.bc[a], g2, st, fw.c_str(), fw.c_str());
-            }
-            body += b;
+            const int a = cp.code >> 1;
+            T.emplace_back(j, a, cp.code & 1, cp.w / h->g.h[a]);
         }
-    if (!body.empty()) o += "        if (coup) {\n          double a0 = 0.0, a1 = 0.0;\n" + body +
-                            "          l0 -= a0; l1 -= a1;\n        }\n";
-    if (pslot >= 0) {
-        std::snprintf(b, sizeof b, "        if (nm) {\n          %s%s%s%s\n",
-                      adj_coef(h, f.s, "s").c_str(), adj_coef(h, f.E, "E").c_str(),
-                      filt ? adj_coef(h, f.F1, "fk1").c_str() : "", filt ? adj_coef(h, f.F2, "fk2").c_str() : "");
-        o += b;
-        // first / last substep filters of the phase before (swap: k=2 first)
-        const std::string a0 = filt ? "(nm_swap ? " + X(f.F2, "fk2") + " : " + X(f.F1, "fk1") + ")" : "1.0";
-        const std::string a1 = filt ? "(nm_swap ? " + Yc(f.F2, "fk2") + " : " + Yc(f.F1, "fk1") + ")" : "1.0";
-        const std::string z0 = filt ? "(nm_swap ? " + X(f.F1, "fk1") + " : " + X(f.F2, "fk2") + ")" : "1.0";
-        const std::string z1 = filt ? "(nm_swap ? " + Yc(f.F1, "fk1") + " : " + Yc(f.F2, "fk2") + ")" : "1.0";
-        std::snprintf(b, sizeof b,
-                      "          l0 *= dwdu(nm, %s, %s, %s, %s, hdt);\n"
-                      "          l1 *= dwdu(nm, %s, %s, %s, %s, hdt);\n        }\n",
-                      X(f.s, "s").c_str(), X(f.E, "E").c_str(), a0.c_str(), z0.c_str(), Yc(f.s, "s").c_str(),
-                      Yc(f.E, "E").c_str(), a1.c_str(), z1.c_str());
+    return T;
+}
+
+// Targets of the backward phases of type l grouped by grid type (one extent
+// condition per group), then greedily by the (axis, destination) pairs whose
+// transposed differences they read.
+std::vector<std::vector<int>> adj_groups(const smg_handle* h, int l, int group) {
+    const std::vector<int> T = l == 0 ? h->destB : h->destA;
+    std::map<std::vector<int>, std::vector<int>> by_ext;
+    std::vector<std::vector<int>> order;
+    std::map<int, std::set<std::pair<int, int>>> K;
+    for (int i : T) {
+        for (const auto& t : adj_terms(h, l, i)) K[i].insert({std::get<1>(t), std::get<0>(t)});
+        std::vector<int> e(h->comps[i].ext, h->comps[i].ext + 3);
+        if (!by_ext.count(e)) order.push_back(e);
+        by_ext[e].push_back(i);
+    }
+    std::vector<std::vector<int>> G;
+    for (const auto& e : order) {
+        std::vector<int> left = by_ext[e];
+        while (!left.empty()) {
+            std::vector<int> g{left.front()};
+            left.erase(left.begin());
+            std::set<std::pair<int, int>> ks = K[g[0]];
+            while ((int)g.size() < group && !left.empty()) {
+                size_t best = 0;
+                int bestn = -1;
+                for (size_t x = 0; x < left.size(); ++x) {
+                    int n = 0;
+                    for (const auto& k : K[left[x]]) n += (int)ks.count(k);
+                    if (n > bestn) {
+                        bestn = n;
+                        best = x;
+                    }
+                }
+                g.push_back(left[best]);
+                ks.insert(K[left[best]].begin(), K[left[best]].end());
+                left.erase(left.begin() + best);
+            }
+            G.push_back(std::move(g));
+        }
+    }
+    return G;
+}
+
+// One group of targets (all on one grid).  Shared at group level: every
+// coefficient value and every transposed difference D^T Y_j (per destination
+// and axis; it does not depend on the target); per target: Y_i, the pending
+// pointwise part (pm), the fold of its terms (coup), the rescaling (nm), the
+// store.  Sigma-gradient contributions are summed per field and added once.
+void emit_adj_group(std::string& o, const smg_handle* h, int l, const std::vector<int>& tg) {
+    const smg::DevGrid& g = h->g;
+    char b[4096];
+    const std::vector<int> Dother = phase_dests(h, 1 - l);
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    const smg::DevComp& c0 = h->comps[tg[0]];
+    std::string cond;
+    const char* ax[3] = {"x0", "y", "z"};
+    for (int a = 0; a < 3; ++a)
+        if (c0.ext[a] < g.B[a]) {
+            if (!cond.empty()) cond += " && ";
+            cond += std::string(ax[a]) + " < " + std::to_string(c0.ext[a]);
+        }
+    // gradient accumulators per sigma field of the group
+    std::map<int, int> fields;
+    for (int i : tg) fields.emplace(coefs_of(h, 1 - l, i).s, i);
+    for (const auto& fe : fields) {
+        std::snprintf(b, sizeof b, "    double gs%d_0 = 0.0, gs%d_1 = 0.0;\n", fe.first, fe.first);
         o += b;
     }
-    o += "        if (v1) *reinterpret_cast<double2*>(Yi) = make_double2(l0, l1); else Yi[0] = l0;\n    }\n";
+    o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
+    const bool v1_always = c0.ext[0] % 2 == 0;
+    o += std::string("    const bool v1 = ") + (v1_always ? "true" : ("x1 < " + std::to_string(c0.ext[0])).c_str()) +
+         ";\n";
+    std::set<int> cdone;
+    auto coef = [&](int f) {
+        const std::string n = "C" + std::to_string(f);
+        if (cdone.insert(f).second) {
+            if (is_array(h, f)) std::snprintf(b, sizeof b, "    const double2 %s = L2(fp(F, %d) + pt);\n", n.c_str(), f);
+            else std::snprintf(b, sizeof b, "    const double %s = fs(F, %d);\n", n.c_str(), f);
+            o += b;
+        }
+        return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
+    };
+    std::set<int> ddone;
+    auto dEc = [&](int f) {   // d(decay)/d(sigma) of sigma field f
+        const std::string n = "DE" + std::to_string(f);
+        if (ddone.insert(f).second) {
+            if (is_array(h, f)) std::snprintf(b, sizeof b, "    const double2 %s = L2(fp(DE, %d) + pt);\n", n.c_str(), f);
+            else std::snprintf(b, sizeof b, "    const double %s = fs(DE, %d);\n", n.c_str(), f);
+            o += b;
+        }
+        return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
+    };
+    std::set<std::pair<int, int>> tdone;
+    auto tval = [&](int j, int a, int g2) {   // D^T Y_j along axis a at the point pair
+        const std::string n = "T" + std::to_string(a) + "_" + std::to_string(j);
+        if (tdone.insert({a, j}).second) {
+            if (a == 0)
+                std::snprintf(b, sizeof b,
+                              "    const double %s_0 = dT(Y + pt + %lld, x0, %d, %d, %d, 1), "
+                              "%s_1 = v1 ? dT(Y + pt + %lld + 1, x1, %d, %d, %d, 1) : 0.0;\n",
+                              n.c_str(), (long long)j * g.cs, g.n[0], g.bc[0], g2, n.c_str(), (long long)j * g.cs,
+                              g.n[0], g.bc[0], g2);
+            else
+                std::snprintf(b, sizeof b, "    const double2 %s = dT_row(Y + pt + %lld, %s, %d, %d, %d, %lld);\n",
+                              n.c_str(), (long long)j * g.cs, a == 1 ? "y" : "z", g.n[a], g.bc[a], g2,
+                              a == 1 ? (long long)g.s1 : (long long)g.s2);
+            o += b;
+        }
+        return a == 0 ? std::make_pair(n + "_0", n + "_1") : std::make_pair(n + ".x", n + ".y");
+    };
+    for (int i : tg) {
+        int pslot = -1;
+        for (size_t k = 0; k < Dother.size(); ++k)
+            if (Dother[k] == i) pslot = (int)k;
+        const Coefs f = coefs_of(h, 1 - l, i);
+        const auto sv = coef(f.s), E = coef(f.E), q = coef(f.q);
+        std::pair<std::string, std::string> k1{"1.0", "1.0"}, k2{"1.0", "1.0"};
+        if (filt) {
+            k1 = coef(f.F1);
+            k2 = coef(f.F2);
+        }
+        const auto dE = dEc(f.s);
+        const auto terms = adj_terms(h, l, i);
+        std::vector<std::pair<double, std::pair<std::string, std::string>>> tv;
+        if (!terms.empty()) {
+            // the transposed differences at group scope (shared with later targets)
+            for (const auto& t : terms) tv.push_back({std::get<3>(t), tval(std::get<0>(t), std::get<1>(t), std::get<2>(t))});
+            o += "    double ta0_" + std::to_string(i) + " = 0.0, ta1_" + std::to_string(i) + " = 0.0;\n";
+            o += "    if (coup) {\n";
+            for (const auto& t : tv) {
+                std::snprintf(b, sizeof b, "      ta0_%d += %s * %s; ta1_%d += %s * %s;\n", i, lit(t.first).c_str(),
+                              t.second.first.c_str(), i, lit(t.first).c_str(), t.second.second.c_str());
+                o += b;
+            }
+            o += "    }\n";
+        }
+        std::snprintf(b, sizeof b, "    {\n        double* Yi = Y + pt + %lld;\n"
+                                   "        const double2 yv = L2(Yi); double l0 = yv.x, l1 = yv.y;\n",
+                      (long long)i * g.cs);
+        o += b;
+        if (pslot >= 0) {
+            const std::string F0 = filt ? "(pm_swap ? " + k2.first + " : " + k1.first + ")" : "1.0";
+            const std::string F1 = filt ? "(pm_swap ? " + k2.second + " : " + k1.second + ")" : "1.0";
+            std::snprintf(b, sizeof b,
+                          "        if (pm) {\n"
+                          "          double* gq = %s;\n"
+                          "          const long long rp = %lld + pt;\n"
+                          "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs%d_0, gq, pt, hdt);\n"
+                          "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs%d_1, gq, "
+                          "pt + 1, hdt);\n"
+                          "        }\n",
+                          f.q == h->field_zero ? "nullptr" : ("Gt[" + std::to_string(f.q) + "]").c_str(),
+                          (long long)pslot * g.cs, sv.first.c_str(), E.first.c_str(), q.first.c_str(), F0.c_str(),
+                          dE.first.c_str(), f.s, sv.second.c_str(), E.second.c_str(), q.second.c_str(), F1.c_str(),
+                          dE.second.c_str(), f.s);
+            o += b;
+        }
+        if (!terms.empty()) {
+            std::snprintf(b, sizeof b, "        l0 -= ta0_%d; l1 -= ta1_%d;\n", i, i);
+            o += b;
+        }
+        if (pslot >= 0) {
+            const std::string a0 = filt ? "(nm_swap ? " + k2.first + " : " + k1.first + ")" : "1.0";
+            const std::string a1 = filt ? "(nm_swap ? " + k2.second + " : " + k1.second + ")" : "1.0";
+            const std::string z0 = filt ? "(nm_swap ? " + k1.first + " : " + k2.first + ")" : "1.0";
+            const std::string z1 = filt ? "(nm_swap ? " + k1.second + " : " + k2.second + ")" : "1.0";
+            std::snprintf(b, sizeof b,
+                          "        if (nm) { l0 *= dwdu(nm, %s, %s, %s, %s, hdt); l1 *= dwdu(nm, %s, %s, %s, %s, hdt); }\n",
+                          sv.first.c_str(), E.first.c_str(), a0.c_str(), z0.c_str(), sv.second.c_str(),
+                          E.second.c_str(), a1.c_str(), z1.c_str());
+            o += b;
+        }
+        o += "        if (v1) *reinterpret_cast<double2*>(Yi) = make_double2(l0, l1); else Yi[0] = l0;\n    }\n";
+    }
+    o += "    }\n";
+    for (const auto& fe : fields) {
+        std::string c2 = "pm";
+        for (int a = 0; a < 3; ++a)
+            if (c0.ext[a] < g.B[a]) c2 += std::string(" && ") + ax[a] + " < " + std::to_string(c0.ext[a]);
+        std::snprintf(b, sizeof b,
+                      "    if (%s) { double* gp = Gt[%d]; if (gp) { atomicAdd(gp + pt, gs%d_0); "
+                      "if (x1 < %d) atomicAdd(gp + pt + 1, gs%d_1); } }\n",
+                      c2.c_str(), fe.first, fe.first, c0.ext[0], fe.first);
+        o += b;
+    }
 }
 
 const char* kAdjArgs =
@@ -1066,12 +1160,9 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
     const long long cta_per_group = (long long)nchunks * g.B[1] * g.B[2];
     std::vector<KernelSrc> P;
     for (int l = 0; l < 2; ++l) {
-        std::vector<int> T = l == 0 ? h->destB : h->destA;   // sources of the phase type
-        // targets sharing a sigma field side by side (fewer gradient atomics per group)
-        std::stable_sort(T.begin(), T.end(),
-                         [&](int a, int b) { return coefs_of(h, 1 - l, a).s < coefs_of(h, 1 - l, b).s; });
-        if (T.empty()) continue;
-        const int ng = ((int)T.size() + group - 1) / group;
+        const std::vector<std::vector<int>> G = adj_groups(h, l, group);
+        if (G.empty()) continue;
+        const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
         // two forms of every kernel: the general one takes the kinds of the
         // phases before and after at run time; the steady one has them fixed to
@@ -1098,28 +1189,7 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
                 std::snprintf(b, sizeof b, "    const int pt = z * %lld + y * %lld + x0;\n", (long long)g.s2,
                               (long long)g.s1);
                 K.src += b;
-                // sigma-gradient contributions of the group, summed per field in
-                // registers and added to the field's gradient once per point
-                std::map<int, int> fields;   // sigma field -> a target on its grid
-                const int t0 = k * group, t1 = std::min<int>((k + 1) * group, (int)T.size());
-                for (int t = t0; t < t1; ++t) fields.emplace(coefs_of(h, 1 - l, T[t]).s, T[t]);
-                for (const auto& fe : fields) {
-                    std::snprintf(b, sizeof b, "    double gs%d_0 = 0.0, gs%d_1 = 0.0;\n", fe.first, fe.first);
-                    K.src += b;
-                }
-                for (int t = t0; t < t1; ++t) emit_adj_target(K.src, h, l, T[t]);
-                for (const auto& fe : fields) {
-                    const smg::DevComp& c = h->comps[fe.second];
-                    std::string cond = "pm";
-                    const char* ax[3] = {"x0", "y", "z"};
-                    for (int a = 0; a < 3; ++a)
-                        if (c.ext[a] < g.B[a]) cond += std::string(" && ") + ax[a] + " < " + std::to_string(c.ext[a]);
-                    std::snprintf(b, sizeof b,
-                                  "    if (%s) { double* gp = Gt[%d]; if (gp) { atomicAdd(gp + pt, gs%d_0); "
-                                  "if (x1 < %d) atomicAdd(gp + pt + 1, gs%d_1); } }\n",
-                                  cond.c_str(), fe.first, fe.first, c.ext[0], fe.first);
-                    K.src += b;
-                }
+                emit_adj_group(K.src, h, l, G[k]);
                 K.src += "}\n";
             }
             char b[1024];
@@ -1134,8 +1204,7 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
                           "    if (x0 >= %d) return;\n"
                           "    switch (grp) {\n",
                           bounds(block, h->jit_regs).c_str(), K.name.c_str(), kAdjArgs, k0, cta_per_group,
-                          cta_per_group, nchunks, nchunks, g.B[1],
-                          g.B[1], block, g.B[0]);
+                          cta_per_group, nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
             K.src += b;
             for (int k = k0; k < k1; ++k)
                 K.src += "    case " + std::to_string(k) + ": smg_ag" + std::to_string(l) + "_" + std::to_string(k) +
