@@ -108,6 +108,7 @@ struct smg_handle {
     int jit_split = 16;              // groups per NVRTC program (0: one program per phase)
     int jit_calls = 0;               // 1: one kernel per phase calling separately compiled groups
     int jit_xpair = 0;               // x differences from aligned 128-bit pairs (1) or 64-bit loads (0)
+    int jit_prefetch = 0;            // L2 prefetch of a group's rows before its loads
     bool jit_failed = false;         // AUTO tried the JIT and it was unavailable
     std::string jit_err;
 };

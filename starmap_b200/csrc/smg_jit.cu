@@ -204,6 +204,8 @@ static __device__ __forceinline__ const double* fp(const DevField* F, int i) {
     return reinterpret_cast<const double*>(__ldg(reinterpret_cast<const unsigned long long*>(&F[i].p)));
 }
 static __device__ __forceinline__ double fs(const DevField* F, int i) { return __ldg(&F[i].s); }
+// request a line into L2 ahead of its load (no register, no wait)
+static __device__ __forceinline__ void pf(const void* p) { asm volatile("prefetch.global.L2 [%0];" :: "l"(p)); }
 )";
 
 // Helpers of the generated adjoint kernels: D^T of a staggered difference
@@ -535,7 +537,7 @@ std::string bounds(int block, int regs) {
 std::string group_name(int phase, int k) { return "smg_g" + std::to_string(phase) + "_" + std::to_string(k); }
 std::string group_args(bool rec) {
     return std::string("(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, "
-                       "int y, int z") +
+                       "int y, int z, bool act") +
            (rec ? ", double* __restrict__ WR, double* __restrict__ PR)" : ")");
 }
 
@@ -553,7 +555,7 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
                   "    const double* Up = U + pt;\n"
-                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up;\n",
+                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
                   (long long)g.s2, (long long)g.s1);
     o += b;
     bool used[3] = {false, false, false};
@@ -608,15 +610,20 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
                   "    const int rest = bid %% %lld;\n"
                   "    const int row = rest / %d, chunk = rest - row * %d;\n"
                   "    const int y = row %% %d, z = row / %d;\n"
-                  "    const int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
-                  "    if (x0 >= %d) return;\n"
+                  "    int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
+                  "    const bool act = x0 < %d;\n"
+                  "    %s\n"
                   "    switch (grp) {\n",
                   bounds(block, h->jit_regs).c_str(), name.c_str(),
                   rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", k0, per, per,
-                  nchunks, nchunks, g.B[1], g.B[1], block, g.B[0]);
+                  nchunks, nchunks, g.B[1], g.B[1], block, g.B[0],
+                  // with x differences from lane shuffles every lane of a warp takes part:
+                  // lanes past the row compute on the last pair and store nothing
+                  (h->jit_xpair == 2 && inl) ? ("if (!act) x0 = " + std::to_string((g.B[0] - 1) & ~1) + ";").c_str()
+                                             : "if (!act) return;");
     o += b;
     for (int k = k0; k < k1; ++k)
-        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z" +
+        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z, act" +
              (rec ? ", WR, PR" : "") + "); break;\n";
     o += "    default: break;\n    }\n}\n";
 }
@@ -688,7 +695,7 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
                   "    const double* Up = U + pt;\n"
-                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up;\n",
+                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
                   (long long)g.s2, (long long)g.s1);
     o += b;
     bool used[3] = {false, false, false};
@@ -717,11 +724,14 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
             o += b;
         }
     }
-    // the group's extent condition (all its destinations share a grid)
+    // the group's extent condition (all its destinations share a grid); with
+    // x differences from lane shuffles the x part only guards the stores, so
+    // that every lane of a warp runs the shuffles
+    const bool shfl = h->jit_xpair == 2;
     const smg::DevComp& c0 = h->comps[D[P[0]]];
     std::string cond;
     const char* ax[3] = {"x0", "y", "z"};
-    for (int a = 0; a < 3; ++a)
+    for (int a = shfl ? 1 : 0; a < 3; ++a)
         if (c0.ext[a] < g.B[a]) {
             if (!cond.empty()) cond += " && ";
             cond += std::string(ax[a]) + " < " + std::to_string(c0.ext[a]);
@@ -730,6 +740,14 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
     const bool v1_always = c0.ext[0] % 2 == 0;
     const std::string v1 = v1_always ? "true" : "v1";
     if (!v1_always) o += "    const bool v1 = x1 < " + std::to_string(c0.ext[0]) + ";\n";
+    const std::string stx = !shfl ? "true"
+                                  : (c0.ext[0] < g.B[0] ? "(act && x0 < " + std::to_string(c0.ext[0]) + ")" : "act");
+    if (shfl && used[0])
+        std::snprintf(b, sizeof b,
+                      "    const int lane = (int)(threadIdx.x & 31);\n"
+                      "    const bool xedge = x0 == 0 || x1 + 2 >= %d;\n", g.B[0]);
+    else b[0] = 0;
+    o += b;
     const std::string sel1 = v1_always ? "" : "v1 ? ", sel2 = v1_always ? "" : " : 0";
     const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
     std::set<int> coef_done;
@@ -743,6 +761,27 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         }
         return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
     };
+    if (h->jit_prefetch) {
+        // every row the group reads, requested into L2 up front: the loads
+        // below then wait for L2 rather than DRAM
+        std::set<std::pair<int, int>> seen;
+        for (int p : P) {
+            const int j = D[p];
+            const smg::DevComp& c = h->comps[j];
+            std::snprintf(b, sizeof b, "    pf(U + pt + %lld);\n", (long long)j * g.cs);
+            o += b;
+            for (int qq = c.cbeg; qq < c.cend; ++qq) {
+                const smg::DevCoup& cp = h->coups[qq];
+                const int a = cp.code >> 1, g2 = cp.code & 1;
+                if (!seen.insert({a, cp.src}).second) continue;
+                const long long so = (long long)cp.src * g.cs;
+                if (a == 0) std::snprintf(b, sizeof b, "    pf(Up + %lld);\n", so);
+                else std::snprintf(b, sizeof b, "    pf(Up + %lld + h%s_%d); pf(Up + %lld + l%s_%d);\n", so, an[a], g2, so,
+                                   an[a], g2);
+                o += b;
+            }
+        }
+    }
     for (int p : P) {
         const int j = D[p];
         const smg::DevComp& c = h->comps[j];
@@ -759,7 +798,32 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
             const int a = cp.code >> 1, g2 = cp.code & 1;
             if (!val_done.insert({a, cp.src}).second) continue;
             const long long so = (long long)cp.src * g.cs;
-            if (a == 0)
+            if (a == 0 && shfl) {
+                // one 128-bit load of the pair; the third value from the
+                // neighbouring lane (lane 0 / 31 load it); pairs at the row
+                // edges (xedge) use the stencil offsets
+                const int n = cp.src;
+                if (xpattern_a(g2, g.bc[0]))
+                    std::snprintf(b, sizeof b,
+                                  "    const double2 P%d = ld2(Up + %lld);\n"
+                                  "    double X%d_b0 = __shfl_up_sync(0xffffffffu, P%d.y, 1);\n"
+                                  "    if (lane == 0) X%d_b0 = ld1(Up + %lld + (x0 > 0 ? -1 : 0));\n"
+                                  "    double X%d_a0 = P%d.x, X%d_a1 = P%d.y, X%d_b1 = P%d.x;\n",
+                                  n, so, n, n, n, so, n, n, n, n, n, n);
+                else
+                    std::snprintf(b, sizeof b,
+                                  "    const double2 P%d = ld2(Up + %lld);\n"
+                                  "    double X%d_a1 = __shfl_down_sync(0xffffffffu, P%d.x, 1);\n"
+                                  "    if (lane == 31) X%d_a1 = ld1(Up + %lld + (x1 + 1 < %d ? 2 : 0));\n"
+                                  "    double X%d_a0 = P%d.y, X%d_b0 = P%d.x, X%d_b1 = P%d.y;\n",
+                                  n, so, n, n, n, so, g.B[0], n, n, n, n, n, n);
+                o += b;
+                std::snprintf(b, sizeof b,
+                              "    if (xedge) { X%d_a0 = ld1(Up + %lld + hx0_%d); X%d_b0 = ld1(Up + %lld + lx0_%d); "
+                              "X%d_a1 = ld1(Up + %lld + (%shx1_%d%s)); X%d_b1 = ld1(Up + %lld + (%slx1_%d%s)); }\n",
+                              n, so, g2, n, so, g2, n, so, sel1.c_str(), g2, sel2.c_str(), n, so, sel1.c_str(), g2,
+                              sel2.c_str());
+            } else if (a == 0)
                 std::snprintf(b, sizeof b,
                               "    const double X%d_a0 = ld1(Up + %lld + hx0_%d), X%d_b0 = ld1(Up + %lld + lx0_%d), "
                               "X%d_a1 = ld1(Up + %lld + (%shx1_%d%s)), X%d_b1 = ld1(Up + %lld + (%slx1_%d%s));\n",
@@ -807,10 +871,10 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         if (rec) {
             const long long so = (long long)p * g.cs;
             std::snprintf(b, sizeof b,
-                          "        { double* wp = WR + pt + %lld; double* pp = PR + pt + %lld;\n"
+                          "        if (%s) { double* wp = WR + pt + %lld; double* pp = PR + pt + %lld;\n"
                           "          if (%s) { *reinterpret_cast<double2*>(wp) = make_double2(-SA, -SB); "
                           "*reinterpret_cast<double2*>(pp) = u; } else { wp[0] = -SA; pp[0] = u.x; } }\n",
-                          so, so, v1.c_str());
+                          stx.c_str(), so, so, v1.c_str());
             o += b;
         }
         auto sub = [&]() {
@@ -835,8 +899,10 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         } else {
             o += "        " + sub() + fl(k1) + "\n        " + sub() + fl(k2) + "\n";
         }
-        if (v1_always) o += "        *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1);\n    }\n";
-        else o += "        if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1); else *Uj = u0;\n    }\n";
+        const std::string guard = stx == "true" ? "" : "if (" + stx + ") ";
+        if (v1_always) o += "        " + guard + "*reinterpret_cast<double2*>(Uj) = make_double2(u0, u1);\n    }\n";
+        else
+            o += "        " + guard + "{ if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1); else *Uj = u0; }\n    }\n";
     }
     o += "    }\n}\n";
 }
