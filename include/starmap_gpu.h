@@ -178,6 +178,7 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
 #define SMG_TUNE_JIT_XPAIR  11   /* x differences: 0 = four 64-bit loads per point pair, 1 = two aligned 128-bit loads,
                                     2 = one 128-bit load and the neighbouring lane's value (warp shuffle) */
 #define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them */
+#define SMG_TUNE_JIT_BAND   13   /* CTA order of the generated kernels: 0 group-major, R > 0 bands of R rows */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the

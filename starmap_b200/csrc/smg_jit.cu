@@ -602,21 +602,42 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
     char b[1024];
     if (!inl)
         for (int k = k0; k < k1; ++k) o += "extern \"C\" __device__ void " + group_name(phase, k) + group_args(rec) + ";\n";
+    // CTA order: group-major (every row of a group, then the next group), or,
+    // with bands of R rows, band-major (every group of the kernel on R rows,
+    // then the next band), so that the source rows a band needs stay in L2
+    // while all groups use them
+    const int R = inl ? h->jit_band : 0;
+    const long long rows = (long long)g.B[1] * g.B[2];
+    std::string map;
+    if (R > 0) {
+        const long long per_band = (long long)(k1 - k0) * R * nchunks;
+        std::snprintf(b, sizeof b,
+                      "    const int band = bid / %lld, r0 = bid - band * %lld;\n"
+                      "    const int grp = %d + r0 / %d, r1 = r0 %% %d;\n"
+                      "    const int row = band * %d + r1 / %d, chunk = r1 %% %d;\n"
+                      "    if (row >= %lld) return;\n",
+                      per_band, per_band, k0, R * nchunks, R * nchunks, R, nchunks, nchunks, rows);
+    } else {
+        std::snprintf(b, sizeof b,
+                      "    const int grp = %d + bid / %lld;\n"
+                      "    const int rest = bid %% %lld;\n"
+                      "    const int row = rest / %d, chunk = rest - row * %d;\n",
+                      k0, per, per, nchunks, nchunks);
+    }
+    map = b;
     std::snprintf(b, sizeof b,
                   "extern \"C\" __global__ void __launch_bounds__(%s) %s(double* __restrict__ U, "
                   "const DevField* __restrict__ F, double hdt, int kf, int mode%s) {\n"
                   "    const int bid = blockIdx.x;\n"
-                  "    const int grp = %d + bid / %lld;\n"
-                  "    const int rest = bid %% %lld;\n"
-                  "    const int row = rest / %d, chunk = rest - row * %d;\n"
+                  "%s"
                   "    const int y = row %% %d, z = row / %d;\n"
                   "    int x0 = 2 * (chunk * %d + (int)threadIdx.x);\n"
                   "    const bool act = x0 < %d;\n"
                   "    %s\n"
                   "    switch (grp) {\n",
                   bounds(block, h->jit_regs).c_str(), name.c_str(),
-                  rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", k0, per, per,
-                  nchunks, nchunks, g.B[1], g.B[1], block, g.B[0],
+                  rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", map.c_str(), g.B[1], g.B[1],
+                  block, g.B[0],
                   // with x differences from lane shuffles every lane of a warp takes part:
                   // lanes past the row compute on the last pair and store nothing
                   (h->jit_xpair == 2 && inl) ? ("if (!act) x0 = " + std::to_string((g.B[0] - 1) & ~1) + ";").c_str()
@@ -958,8 +979,11 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         const int step = per > 0 ? per : ng;
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase,
-                        (long long)(k1 - k0) * cta_per_group};
+            const int R = h->jit_band;
+            const long long rows = (long long)g.B[1] * g.B[2];
+            const long long ctas = R > 0 ? (long long)(k1 - k0) * ((rows + R - 1) / R) * R * (cta_per_group / rows)
+                                         : (long long)(k1 - k0) * cta_per_group;
+            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase, ctas};
             for (int j = k0; j < k1; ++j) emit_shared_group(k.src, h, phase, j, G[j], rec);
             emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
             P.push_back(std::move(k));

@@ -49,7 +49,7 @@ def test_generated_source_structure(name):
 @pytest.mark.parametrize("name", ["lin_p7_periodic", "odd_mixed_bc", "pt3d_p3", "lattice_p4_full", "spn_3d"])
 @pytest.mark.parametrize("layout", [dict(calls=0, split=4, xpair=0), dict(calls=1, split=2, xpair=1),
                                     dict(calls=0, split=0, xpair=1), dict(calls=0, split=16, prefetch=1),
-                                    dict(calls=0, split=16, xpair=2)])
+                                    dict(calls=0, split=16, xpair=2), dict(calls=0, split=16, band=5)])
 def test_generated_source_compiles(name, layout):
     if not _nvrtc_available():
         pytest.skip("NVRTC library not present")

@@ -162,7 +162,8 @@ def test_auto_runs_the_specialised_kernels():
 @pytest.mark.parametrize("block,group,split,calls,xpair,prefetch", [
     (32, 1, 4, 0, 0, 0), (128, 3, 1, 1, 0, 0), (256, 64, 4, 0, 1, 0), (64, 4, 0, 0, 1, 0), (64, 2, 3, 1, 1, 0),
     (64, 8, 16, 0, 0, 1), (64, 8, 16, 0, 2, 0), (32, 3, 16, 0, 2, 0)])
-def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch):
+@pytest.mark.parametrize("band", [0, 3])
+def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, band):
     from starmap_b200 import _lib
     from starmap_b200.solver import setup_gpu
     par = starmap_init(cases.odd_mixed_bc())
@@ -177,6 +178,7 @@ def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch):
                 solver.tune(_lib.SMG_TUNE_JIT_CALLS, calls)
                 solver.tune(_lib.SMG_TUNE_JIT_XPAIR, xpair)
                 solver.tune(_lib.SMG_TUNE_JIT_PREFETCH, prefetch)
+                solver.tune(_lib.SMG_TUNE_JIT_BAND, band)
                 solver.set_variant(5)
             else:
                 solver.set_variant(4)
