@@ -365,7 +365,7 @@ def host_threads():
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU path (oracle C port; GNU Octave is not on the box)."""
+    """--impl reference: the reference's CPU path (oracle C port; GNU Octave is not installed)."""
     if rank != 0:
         return 0
     par = workload()

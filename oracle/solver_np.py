@@ -12,8 +12,8 @@ quirk of the loop (constant dt with overshoot for autonomous problems, the
 filter substep index reused between phases, absorption-only zeroth moment).
 Each block cites the reference lines it follows.
 
-Parity status: the reference is MATLAB/GNU Octave only and no Octave or MATLAB
-exists on any machine available to this build, and the reference ships no
+Parity status: the reference is MATLAB/GNU Octave only, no Octave or MATLAB
+is installed where this code is developed and tested, and the reference ships no
 stored outputs or golden vectors.  The restatement is therefore *parity
 unpinned* with respect to Octave itself; it is pinned instead by the
 reference's own known-answer properties (P_N == SP_N for isotropic data,
