@@ -702,6 +702,16 @@ std::vector<std::vector<int>> shared_groups(const smg_handle* h, int phase, int 
             G.push_back(std::move(g));
         }
     }
+    // groups in the order of their destinations' coupling-graph levels (the
+    // destination list is level-sorted), so that groups running at the same
+    // time, in one kernel or in the concurrent kernels of the phase, read
+    // overlapping sources while these are in L2
+    std::stable_sort(G.begin(), G.end(), [](const std::vector<int>& a, const std::vector<int>& b) {
+        long long sa = 0, sb = 0;
+        for (int p : a) sa += p;
+        for (int p : b) sb += p;
+        return sa * (long long)b.size() < sb * (long long)a.size();
+    });
     return G;
 }
 
@@ -1089,6 +1099,18 @@ std::vector<std::vector<int>> adj_groups(const smg_handle* h, int l, int group) 
             G.push_back(std::move(g));
         }
     }
+    // groups in the coupling-graph level order of their targets (their slots in
+    // the other phase's level-sorted destination list): concurrent groups
+    // share the rows they read while these are in L2
+    std::map<int, int> lvl;
+    const std::vector<int> Dother = phase_dests(h, 1 - l);
+    for (size_t k = 0; k < Dother.size(); ++k) lvl[Dother[k]] = (int)k;
+    std::stable_sort(G.begin(), G.end(), [&](const std::vector<int>& x, const std::vector<int>& y) {
+        long long sx = 0, sy = 0;
+        for (int i : x) sx += lvl[i];
+        for (int i : y) sy += lvl[i];
+        return sx * (long long)y.size() < sy * (long long)x.size();
+    });
     return G;
 }
 
