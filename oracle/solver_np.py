@@ -21,7 +21,7 @@ starmap_2d_ex_boxes.m:7-16), by an independent discrete-symbol (von Neumann)
 check of the staggered update, and by agreement with the independent C
 restatement in ``oracle/loop_ref.c``.
 
-Scope: ``par.timestep == 0`` (hyperbolic dt); autonomous and time-dependent
+Scope: hyperbolic and parabolic dt (``par.timestep`` 0, 1, 2); autonomous and time-dependent
 material hooks; filters ``''``, ``'substep'`` and ``'full'``; 1D/2D/3D; both
 boundary conditions.  Plot callbacks are replaced by optional snapshot capture.
 """
@@ -106,6 +106,59 @@ class OracleResult:
     dt: float
     snapshots: list = field(default_factory=list)
     setup: dict = field(default_factory=dict)
+    dts: list = field(default_factory=list)       # dt of every step
+
+
+def _mat_min(A):
+    """MATLAB ``min(A)``: along the first non-singleton dimension."""
+    A = np.asarray(A, dtype=np.float64)
+    for d, n in enumerate(A.shape):
+        if n != 1:
+            return np.min(A, axis=d, keepdims=True)
+    return A
+
+
+def _min2(A):
+    """``min(min(A))`` as the decay vector needs it (starmap_solver.m:175-179):
+    a scalar for 2D arrays; a 3D array with several planes leaves a vector,
+    which the reference cannot store into ``decay(j)``."""
+    v = _mat_min(_mat_min(A))
+    if v.size != 1:
+        raise ValueError("min(min(.)) of a 3D coefficient field is not a scalar (the reference fails here too)")
+    return float(v.reshape(()))
+
+
+def _decay(sA, sT, n_sys, gtx, gty, gtz, mom_order):
+    """Smallest absorption and total cross-sections per component
+    (starmap_solver.m:175-179 and 255-259)."""
+    decay = np.ones(n_sys) * _min2(sA)
+    for j in range(1, n_sys):
+        decay[j] = _min2(sT[int(gtx[j]), int(gty[j]), int(gtz[j]), int(mom_order[j])])
+    return decay
+
+
+def _growth_factor(Msym, c, decay, dt, timestep):
+    """Largest eigenvalue modulus of the von Neumann growth matrix of one full
+    step (starmap_solver.m:506-514): G = diag(dt*phi(-decay*dt/2))*(M -
+    diag(decay/2)); the even update leaves the odd rows at the identity and
+    vice versa; one step is G_o*G_e*G_e*G_o; timestep 2 scales by
+    exp(decay(1)*dt)."""
+    decay = np.asarray(decay, dtype=np.float64)
+    G = np.diag(dt * expm1div(-decay * dt / 2)) @ (Msym + np.diag(-decay / 2))
+    I = np.eye(len(decay))
+    even = c["111"] + c["221"] + c["212"] + c["122"]
+    odd = c["211"] + c["121"] + c["112"] + c["222"]
+    Ge = G.copy()
+    Ge[odd, :] = 0
+    Ge = Ge + I
+    Go = G.copy()
+    Go[even, :] = 0
+    Go = Go + I
+    G = Go @ Ge @ Ge @ Go
+    la = float(np.max(np.abs(np.linalg.eigvals(G))))
+    if timestep == 2:
+        la = la * np.exp(decay[0] * dt)
+    return la
 
 
 def _classify(Mx, My, Mz):
@@ -193,8 +246,9 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
         dt_hyp = dt_hyp / 3
     elif n[1] != 1:
         dt_hyp = dt_hyp / 2
-    if par.get("timestep", 0) != 0:
-        raise NotImplementedError("parabolic time step selection (timestep>0) is not restated")
+    timestep = int(par.get("timestep", 0))
+    # von Neumann symbol at the largest wave numbers (starmap_solver.m:108)
+    Msym = -1j * (Mx / h[0] + My / h[1] + Mz / h[2])
     time_dependent = np.array([nargin(par["sigma_a"]) > 3, nargin(par["sigma_s0"]) > 3,
                                nargin(par["sigma_sm"]) > 4])
 
@@ -242,6 +296,7 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
     t = 0.0
     dt = 0.0
     step_count = 0
+    dts = []
     sA = sS = sT = sA0 = sT0 = sA1 = sT1 = None
     sS = {}
     sT = {}
@@ -259,7 +314,34 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
         for k in range(int(t > 0), 2):
             if (not time_dependent.any()) and t > 0:
                 break
-            dt_bracket = dt_hyp
+            flag_check_stab = k > 0 and timestep > 0
+            if flag_check_stab:
+                # parabolic step: bracket and bisect the largest stable dt
+                # (starmap_solver.m:173-203)
+                dt = max(dt, dt_hyp)
+                decay = _decay(sA[1, 1, 1], sT, n_sys, gtx, gty, gtz, mom_order)
+                gf = lambda d: _growth_factor(Msym, c, decay, d, timestep)
+                la = gf(dt)
+                dt_br = [dt, dt]
+                la_br = [la, la]
+                la0 = 1 + 1e-8
+                while ((la_br[0] < la0) == (la_br[1] < la0)) and (dt_br[0] <= tleft or la_br[0] > la0):
+                    ind = int(la_br[0] < la0) + 1
+                    base = dt_br[ind - 1]
+                    dt_br = [base * 1 * 2.0 ** (ind - 2), base * 2 * 2.0 ** (ind - 2)]
+                    la_br = [la_br[1], la_br[0]]
+                    la_br[ind - 1] = gf(dt_br[ind - 1])
+                    if min(la_br) < 1:
+                        la0 = 1
+                while dt_br[0] / dt_br[1] < 0.98 and dt_br[0] <= tleft:
+                    dt_mid = np.sqrt(dt_br[0] * dt_br[1])
+                    la_mid = gf(dt_mid)
+                    ind = 1 + int(la_mid >= la0)
+                    dt_br[ind - 1] = dt_mid
+                    la_br[ind - 1] = la_mid
+                dt_bracket = dt_br[0]
+            else:
+                dt_bracket = dt_hyp
             if k > 0:
                 dt = min(dt_bracket, tleft) * cn
                 sA0 = sA
@@ -286,12 +368,20 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
             if k > 0:
                 sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
                 sT1 = {key: (sT0[key] + sT[key]) / 2 for key in sg_rows}
+            if flag_check_stab:
+                # averaged materials unstable with dt: fall back to those at t
+                # (starmap_solver.m:253-265)
+                decay = _decay(sA1, sT1, n_sys, gtx, gty, gtz, mom_order)
+                if not _growth_factor(Msym, c, decay, dt, timestep) < la0:
+                    sA1 = sA0[1, 1, 1]
+                    sT1 = sT0
         # decay terms (starmap_solver.m:267-274)
         if t == 0 or time_dependent.any():
             EA = expm1div(-sA1 * dt / 2)
             for key in sg_rows:
                 ET[key] = expm1div(-sT1[key] * dt / 2)
         t = t + dt
+        dts.append(dt)
         step_count += 1
         for j1 in source_ind:
             j = j1 - 1
@@ -328,7 +418,7 @@ def starmap_solver(par: dict, *, capture_snapshots: bool = False, max_steps: int
             out.append({"x": xs[gtx[j] - 1], "y": ys[gty[j] - 1], "z": zs[gtz[j] - 1], "U": U[j]})
     setup = dict(c=c, gtx=gtx, gty=gty, gtz=gtz, h=h, dt_hyp=dt_hyp, EA=EA, ET=ET, sA1=sA1, sT1=sT1,
                  filterTerm=filterTerm, Q=Q, mom_order=mom_order)
-    return OracleResult(out, U, step_count, t, dt, snapshots, setup)
+    return OracleResult(out, U, step_count, t, dt, snapshots, setup, dts)
 
 
 def _advance(U, Q, Ix, Iy, Iz, c, extend, h, Mx, My, Mz, dt, gtx, gty, gtz, mom_order, f_mom_order, f_position,

@@ -26,6 +26,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import FILTER_FULL, FILTER_NONE, FILTER_SUBSTEP, SmgError, check, dptr, iptr
+from . import timestep
 from .init import _noop_output, capargs, nargin, zero
 
 __all__ = ["starmap_solver", "GpuSolver", "prepare", "expm1div", "colon", "step_times"]
@@ -371,8 +372,9 @@ def prepare(par: dict) -> _Setup:
         dt_hyp = dt_hyp / 3
     elif n[1] != 1:
         dt_hyp = dt_hyp / 2
-    if par.get("timestep", 0) != 0:
-        raise NotImplementedError("timestep > 0 (parabolic step search) is handled by the reference's host code only")
+    S.timestep = int(par.get("timestep", 0))
+    if S.timestep not in (0, 1, 2):
+        raise ValueError("timestep must be 0 (hyperbolic), 1 or 2 (parabolic)")
     S.time_dependent = np.array([nargin(par["sigma_a"]) > 3, nargin(par["sigma_s0"]) > 3,
                                  nargin(par["sigma_sm"]) > 4])
     xs = [colon(ax[0] + h[0] / 2, h[0], ax[1] - h[0] / 2), colon(ax[0] + h[0] * (1 - bc[0]), h[0], ax[1])]
@@ -402,6 +404,11 @@ def prepare(par: dict) -> _Setup:
         val = capargs(ic, X, Y, Z, j + 1)
         U.append(X * 0 + np.asarray(val, dtype=np.float64) * float(nargin(ic) > 3 or j == 0))
     S.U0 = U
+    if S.timestep > 0:
+        S.M_sym = timestep.symbol(Mx, My, Mz, h)
+        n2 = np.sum(gt == 2, axis=1)
+        S.even = [j for j in range(n_sys) if n2[j] % 2 == 0]     # c111, c221, c212, c122
+        S.odd = [j for j in range(n_sys) if n2[j] % 2 == 1]      # c211, c121, c112, c222
     S.source_ind = [int(v) for v in np.atleast_1d(np.asarray(par.get("source_ind", [])))]
     S.src_td = nargin(par["source"]) >= 4 and len(S.source_ind) > 0
     S.filter_td = flag_filter and nargin(par["filterfunction"]) > 6
@@ -523,20 +530,41 @@ def _output_struct(S, U):
     return out
 
 
+def step_materials(S, t, dt_prev, sA, sT):
+    """dt and the materials of the step from time t (starmap_solver.m:168-265):
+    the hyperbolic step, or with ``timestep > 0`` the parabolic search from
+    the materials at t; for time-dependent materials those at t + dt,
+    averaged with the ones at t (with the parabolic step, falling back to the
+    ones at t when the average is unstable).  Returns
+    ``(dt, sA, sT, sA1, sT1)`` with sA, sT the materials to carry to the next step."""
+    tfinal = float(S.par["tfinal"])
+    cn = float(S.par["cn"])
+    tleft = (tfinal - t) / cn
+    la0 = None
+    if S.timestep > 0:
+        decay = timestep.decay_vector(S.n_sys, S.gt, S.mom_order, sA[1, 1, 1], sT)
+        dt_b, la0 = timestep.search(S.M_sym, S.even, S.odd, decay, dt_prev, S.dt_hyp, tleft, S.timestep)
+    else:
+        dt_b = S.dt_hyp
+    dt = min(dt_b, tleft) * cn
+    if not S.time_dependent.any():
+        return dt, sA, sT, sA[1, 1, 1], sT
+    sA0, sT0 = sA, sT
+    sA, sT = _materials(S, t + dt)
+    sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
+    sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
+    if S.timestep > 0:
+        decay = timestep.decay_vector(S.n_sys, S.gt, S.mom_order, sA1, sT1)
+        if not timestep.stable(S.M_sym, S.even, S.odd, decay, dt, la0, S.timestep):
+            sA1, sT1 = sA0[1, 1, 1], sT0
+    return dt, sA, sT, sA1, sT1
+
+
 def first_step(S):
     """Materials, dt, decay factors, source and filter tables as the reference
     evaluates them for the first step (starmap_solver.m:165-305)."""
-    tfinal = float(S.par["tfinal"])
-    cn = float(S.par["cn"])
     sA, sT = _materials(S, 0.0)
-    dt = min(S.dt_hyp, (tfinal - 0.0) / cn) * cn
-    if S.time_dependent.any():
-        sA0, sT0 = sA, sT
-        sA, sT = _materials(S, dt)
-        sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
-        sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
-    else:
-        sA1, sT1 = sA[1, 1, 1], sT
+    dt, sA, sT, sA1, sT1 = step_materials(S, 0.0, 0.0, sA, sT)
     EA = expm1div(-sA1 * dt / 2)
     ET = {k: expm1div(-sT1[k] * dt / 2) for k in S.sg}
     Q = _sources(S, dt, dt)
@@ -585,13 +613,8 @@ def starmap_solver(par: dict):
         while t_cur < tfinal:
             if per_step and step_count > 0:
                 # time-dependent data re-evaluated where the reference does
-                tleft = (tfinal - t_cur) / cn
                 if td_any:
-                    dt_new = min(S.dt_hyp, tleft) * cn
-                    sA0, sT0 = sA, sT
-                    sA, sT = _materials(S, t_cur + dt_new)
-                    sA1 = (sA0[1, 1, 1] + sA[1, 1, 1]) / 2
-                    sT1 = {k: (sT0[k] + sT[k]) / 2 for k in S.sg}
+                    dt_new, sA, sT, sA1, sT1 = step_materials(S, t_cur, dt, sA, sT)
                     if dt_new != dt:
                         dt = dt_new
                         solver.set_dt(dt)

@@ -99,6 +99,24 @@ def td_sigma():
                 tfinal=1.5, t_plot=[0, 1.5], quiet=True)
 
 
+def parabolic_homog():
+    """Parabolic time step (timestep 1) with homogeneous scalar materials, as
+    starmap_2d_ex_homogeneous.m runs it (smaller grid and end time)."""
+    return dict(name="parab", closure="P", n_mom=3, timestep=1, ax=[-1, 1, -1, 1], n=[14, 12], bc=[1, 1],
+                ic=lambda x, y, k: np.exp(-((x ** 2 + y ** 2) / .25 ** 2) ** 2) * (k == 1),
+                sigma_a=lambda x, y: 6.0, sigma_s0=lambda x, y: 6.0, tfinal=0.7, t_plot=[0, 0.7], quiet=True)
+
+
+def parabolic_td():
+    """Relative-stability parabolic step (timestep 2) with time-dependent
+    absorption and a spatially varying scattering field: dt is searched every
+    step."""
+    return dict(name="parab_td", closure="P", n_mom=2, timestep=2, ax=[0, 1, 0, 1], n=[9, 11], bc=[0, 1],
+                ic=lambda x, y: np.exp(-15 * ((x - .5) ** 2 + (y - .4) ** 2)),
+                sigma_a=lambda x, y, t: 2.0 + np.sin(6 * t) + 0 * x, sigma_s0=lambda x, y: 4.0 + x * y,
+                tfinal=0.35, t_plot=[0, 0.35], quiet=True)
+
+
 ALL = {
     "lin_p7_periodic": lin_p7_periodic,
     "lattice_p5_substep": lattice_p5_substep,
@@ -113,4 +131,6 @@ ALL = {
     "one_d_p5": one_d_p5,
     "boxes_td_source": boxes_td_source,
     "td_sigma": td_sigma,
+    "parabolic_homog": parabolic_homog,
+    "parabolic_td": parabolic_td,
 }
