@@ -158,7 +158,8 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
  * them; defaults otherwise); *len receives its length, buf (cap bytes) a
  * NUL-terminated copy.  compile = 1 also compiles it with NVRTC for sm_100a
  * (no GPU needed); compile = 2 adds (to the source and the compilation) the
- * adjoint's recording and backward-phase kernels.  No reference counterpart. */
+ * adjoint's recording and backward-phase kernels, compile = 3 the batched
+ * solver's family kernels.  No reference counterpart. */
 int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune, int32_t compile,
                    char* buf, int64_t cap, int64_t* len);
 
@@ -179,6 +180,7 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
                                     2 = one 128-bit load and the neighbouring lane's value (warp shuffle) */
 #define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them */
 #define SMG_TUNE_JIT_BAND   13   /* CTA order of the generated kernels: 0 group-major, R > 0 bands of R rows */
+#define SMG_TUNE_JIT_CONST  14   /* 1 (default): coupling weights and grid constants read from a __constant__ table; 0: immediates */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the

@@ -1011,6 +1011,12 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             smg::jit_free(h);
             h->jit_failed = false;
             break;
+        case SMG_TUNE_JIT_CONST:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: jit const must be 0 or 1");
+            h->jit_const = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
         case SMG_TUNE_JIT_BAND:
             if (value < 0 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: jit band must be 0..4096");
             h->jit_band = value;

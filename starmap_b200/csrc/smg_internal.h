@@ -109,6 +109,7 @@ struct smg_handle {
     int jit_calls = 0;               // 1: one kernel per phase calling separately compiled groups
     int jit_xpair = 0;               // x differences from aligned 128-bit pairs (1) or 64-bit loads (0)
     int jit_prefetch = 0;            // L2 prefetch of a group's rows before its loads
+    int jit_const = 1;               // coupling weights and grid constants from a __constant__ table
     int jit_band = 0;                // rows per band of the CTA order (0: group-major)
     bool jit_failed = false;         // AUTO tried the JIT and it was unavailable
     std::string jit_err;

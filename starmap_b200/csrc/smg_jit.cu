@@ -295,6 +295,38 @@ std::string lit(double v) {
     return buf;
 }
 
+// Constant table of the program being emitted (null: literals in the code).
+// With a table, coupling weights and grid constants are read from
+// __constant__ memory, which the FP64 instructions take as an operand,
+// instead of being built in registers from immediates.
+struct ConstTable {
+    std::vector<double> v;
+    std::map<unsigned long long, int> at;
+};
+thread_local ConstTable* g_ctab = nullptr;
+
+std::string clit(double v) {
+    if (!g_ctab) return lit(v);
+    unsigned long long bits;
+    std::memcpy(&bits, &v, sizeof bits);
+    auto it = g_ctab->at.find(bits);
+    int i;
+    if (it != g_ctab->at.end()) i = it->second;
+    else {
+        i = (int)g_ctab->v.size();
+        g_ctab->v.push_back(v);
+        g_ctab->at[bits] = i;
+    }
+    return "kC[" + std::to_string(i) + "]";
+}
+
+std::string ctab_decl(const ConstTable& t) {
+    if (t.v.empty()) return "";
+    std::string o = "__constant__ double kC[" + std::to_string(t.v.size()) + "] = {";
+    for (size_t i = 0; i < t.v.size(); ++i) o += (i ? ", " : "") + lit(t.v[i]);
+    return o + "};\n";
+}
+
 struct Coefs {
     int q, s, E, F1, F2;
 };
@@ -369,10 +401,7 @@ std::string xfast_cond(const smg_handle* h, int g2) {
 // the component's extent ends at x0 (that value is unused and not stored).
 // rec: also store the coupling sum W and the values before the update into
 // slot di of the recording buffers WR / PR (adjoint recording, smg_forward)
-// fam: the family form for the batched solver -- the grid sizes, strides,
-// spacing and decay step come from the instance's FamGeom at run time (names
-// N0..N2, S1, S2, CS, H0..H2, RH0..RH2), everything else stays a constant
-void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bool rec, bool fam = false) {
+void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bool rec) {
     const smg::DevComp& c = h->comps[j];
     const smg::DevGrid& g = h->g;
     char b[4096];
@@ -381,24 +410,17 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bo
     for (int a = 0; a < 3; ++a)
         if (c.ext[a] < g.B[a]) {
             if (!cond.empty()) cond += " && ";
-            cond += std::string(ax[a]) + " < " +
-                    (fam ? "N" + std::to_string(a) + " + " + std::to_string(c.ext[a] - g.n[a]) : std::to_string(c.ext[a]));
+            cond += std::string(ax[a]) + " < " + std::to_string(c.ext[a]);
         }
     o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
-    const bool v1_always = !fam && c.ext[0] % 2 == 0;
-    if (fam)
-        std::snprintf(b, sizeof b,
-                      "        double* Uj = U + pt + %dLL * CS;\n        const double2 u = *reinterpret_cast<const double2*>(Uj);\n",
-                      j);
-    else
-        std::snprintf(b, sizeof b,
+    const bool v1_always = c.ext[0] % 2 == 0;
+    std::snprintf(b, sizeof b,
                       "        double* Uj = U + pt + %lld;\n        const double2 u = *reinterpret_cast<const double2*>(Uj);\n",
                       (long long)j * g.cs);
     o += b;
     // the x stencil of the second point is evaluated only inside the extent
     if (!v1_always)
-        o += "        const bool v1 = x1 < " +
-             (fam ? "N0 + " + std::to_string(c.ext[0] - g.n[0]) : std::to_string(c.ext[0])) + ";\n";
+        o += "        const bool v1 = x1 < " + std::to_string(c.ext[0]) + ";\n";
     const Coefs f = coefs_of(h, phase, j);
     const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
     o += "        " + coef_decl(h, f.q, "q") + coef_decl(h, f.s, "s") + coef_decl(h, f.E, "E") + "\n";
@@ -410,37 +432,11 @@ void emit_dest(std::string& o, const smg_handle* h, int phase, int j, int di, bo
         const int a = cp.code >> 1, g2 = cp.code & 1;
         const long long so = (long long)cp.src * g.cs;
         const int mode_div = h->exact_recip[a];
-        const std::string H = fam ? "H" + std::to_string(a) : lit(g.h[a]),
-                          RH = fam ? "RH" + std::to_string(a) : lit(h->rh[a]), W = lit(cp.w);
-        // the family form divides with two correction steps: exact for every
-        // normal spacing, so instances need not share one
-        const char* dv = fam ? "div1" : (mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0"));
+        const std::string H = lit(g.h[a]), RH = lit(h->rh[a]), W = lit(cp.w);
+        const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
         const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
         first = false;
-        if (fam) {
-            const std::string S = "Up + " + std::to_string(cp.src) + "LL * CS";
-            if (a == 0)
-                std::snprintf(b, sizeof b,
-                              "        { const double* S = %s;\n"
-                              "          const double a0 = ld1(S + hx0_%d), b0 = ld1(S + lx0_%d), a1 = ld1(S + (v1 ? hx1_%d : 0)), "
-                              "b1 = ld1(S + (v1 ? lx1_%d : 0));\n"
-                              "          const double tA = __dmul_rn(%s(__dsub_rn(a0, b0), %s, %s), %s);\n"
-                              "          const double tB = __dmul_rn(%s(__dsub_rn(a1, b1), %s, %s), %s);\n"
-                              "          %s }\n",
-                              S.c_str(), g2, g2, g2, g2, dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(),
-                              RH.c_str(), W.c_str(), fold);
-            else {
-                const char* n = a == 1 ? "y" : "z";
-                std::snprintf(b, sizeof b,
-                              "        { const double* S = %s;\n"
-                              "          const double2 hv = ld2(S + h%s_%d), lv = ld2(S + l%s_%d);\n"
-                              "          const double tA = __dmul_rn(%s(__dsub_rn(hv.x, lv.x), %s, %s), %s);\n"
-                              "          const double tB = __dmul_rn(%s(__dsub_rn(hv.y, lv.y), %s, %s), %s);\n"
-                              "          %s }\n",
-                              S.c_str(), n, g2, n, g2, dv, H.c_str(), RH.c_str(), W.c_str(), dv, H.c_str(),
-                              RH.c_str(), W.c_str(), fold);
-            }
-        } else if (a == 0 && !h->jit_xpair) {
+        if (a == 0 && !h->jit_xpair) {
             // four 64-bit loads at the thread's stencil offsets
             std::snprintf(b, sizeof b,
                           "        { const double* S = Up + %lld;\n"
@@ -717,18 +713,43 @@ std::vector<std::vector<int>> shared_groups(const smg_handle* h, int phase, int 
 
 // one group's device function (inline layout): positions P into the phase's
 // destination list (the position is the destination's recording slot)
-void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, bool rec) {
+void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, bool rec,
+                       bool fam = false) {
     const smg::DevGrid& g = h->g;
     const std::vector<int> D = phase_dests(h, phase);
     char b[4096];
-    o += "static __device__ __forceinline__ void " + group_name(phase, k) + group_args(rec) + " {\n";
-    std::snprintf(b, sizeof b,
-                  "    const int x1 = x0 + 1;\n"
-                  "    const int pt = z * %lld + y * %lld + x0;\n"
-                  "    const double* Up = U + pt;\n"
-                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
-                  (long long)g.s2, (long long)g.s1);
-    o += b;
+    if (fam) {
+        // family form: the geometry (extents, pitches, spacings, component
+        // stride, coefficient table) comes from the instance's FamGeom
+        rec = false;
+        o += "static __device__ __forceinline__ void " + group_name(phase, k) +
+             "(const FamGeom& G, int kf, int mode, int x0, int y, int z) {\n"
+             "    double* U = G.U; const DevField* F = G.F; const double hdt = G.hdt;\n"
+             "    const int N0 = G.n[0], N1 = G.n[1], N2 = G.n[2];\n"
+             "    const long long S1 = G.s1, S2 = G.s2, CS = G.cs;\n"
+             "    const double H0 = G.h[0], H1 = G.h[1], H2 = G.h[2], RH0 = G.rh[0], RH1 = G.rh[1], RH2 = G.rh[2];\n"
+             "    (void)N0; (void)N1; (void)N2; (void)S1; (void)S2; (void)H0; (void)H1; (void)H2; (void)RH0; (void)RH1; "
+             "(void)RH2;\n"
+             "    const int x1 = x0 + 1;\n"
+             "    const long long pt = z * S2 + y * S1 + x0;\n"
+             "    const double* Up = U + pt;\n"
+             "    (void)x1; (void)kf; (void)mode; (void)Up;\n";
+    } else {
+        o += "static __device__ __forceinline__ void " + group_name(phase, k) + group_args(rec) + " {\n";
+        std::snprintf(b, sizeof b,
+                      "    const int x1 = x0 + 1;\n"
+                      "    const int pt = z * %lld + y * %lld + x0;\n"
+                      "    const double* Up = U + pt;\n"
+                      "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
+                      (long long)g.s2, (long long)g.s1);
+        o += b;
+    }
+    // extents, pitches and component offsets: literals, or the family's
+    // run-time values
+    auto N = [&](int a) { return fam ? "N" + std::to_string(a) : std::to_string(g.n[a]); };
+    auto off = [&](int comp) {
+        return fam ? "(long long)" + std::to_string(comp) + " * CS" : std::to_string((long long)comp * g.cs);
+    };
     bool used[3] = {false, false, false};
     for (int p : P)
         for (int q = h->comps[D[p]].cbeg; q < h->comps[D[p]].cend; ++q) used[h->coups[q].code >> 1] = true;
@@ -736,41 +757,45 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         for (int g2 = 0; g2 < 2; ++g2) {
             std::snprintf(b, sizeof b,
                           "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
-                          "    { int hi, lo; stencil(x0, %d, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
-                          "      stencil(x1, %d, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
-                          g2, g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2);
+                          "    { int hi, lo; stencil(x0, %s, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
+                          "      stencil(x1, %s, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
+                          g2, g2, g2, g2, N(0).c_str(), g.bc[0], g2, g2, g2, N(0).c_str(), g.bc[0], g2, g2, g2);
             o += b;
         }
     const char* an[3] = {"x", "y", "z"};
     for (int a = 1; a < 3; ++a) {
         if (!used[a]) continue;
-        const long long st = a == 1 ? g.s1 : g.s2;
+        const std::string st = fam ? (a == 1 ? "S1" : "S2") : std::to_string(a == 1 ? g.s1 : g.s2);
         const char* pp = a == 1 ? "y" : "z";
         for (int g2 = 0; g2 < 2; ++g2) {
             std::snprintf(b, sizeof b,
                           "    int h%s_%d, l%s_%d;\n"
-                          "    { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); h%s_%d = (hi - %s) * %lld; "
-                          "l%s_%d = (lo - %s) * %lld; }\n",
-                          an[a], g2, an[a], g2, pp, g.n[a], g.bc[a], g2, an[a], g2, pp, st, an[a], g2, pp, st);
+                          "    { int hi, lo; stencil(%s, %s, %d, %d, hi, lo); h%s_%d = (int)((hi - %s) * %s); "
+                          "l%s_%d = (int)((lo - %s) * %s); }\n",
+                          an[a], g2, an[a], g2, pp, N(a).c_str(), g.bc[a], g2, an[a], g2, pp, st.c_str(), an[a], g2,
+                          pp, st.c_str());
             o += b;
         }
     }
     // the group's extent condition (all its destinations share a grid); with
     // x differences from lane shuffles the x part only guards the stores, so
     // that every lane of a warp runs the shuffles
-    const bool shfl = h->jit_xpair == 2;
+    const bool shfl = !fam && h->jit_xpair == 2;
     const smg::DevComp& c0 = h->comps[D[P[0]]];
     std::string cond;
     const char* ax[3] = {"x0", "y", "z"};
     for (int a = shfl ? 1 : 0; a < 3; ++a)
         if (c0.ext[a] < g.B[a]) {
             if (!cond.empty()) cond += " && ";
-            cond += std::string(ax[a]) + " < " + std::to_string(c0.ext[a]);
+            cond += std::string(ax[a]) + " < " +
+                    (fam ? N(a) + " + " + std::to_string(c0.ext[a] - g.n[a]) : std::to_string(c0.ext[a]));
         }
     o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
-    const bool v1_always = c0.ext[0] % 2 == 0;
+    const bool v1_always = !fam && c0.ext[0] % 2 == 0;
     const std::string v1 = v1_always ? "true" : "v1";
-    if (!v1_always) o += "    const bool v1 = x1 < " + std::to_string(c0.ext[0]) + ";\n";
+    if (!v1_always)
+        o += "    const bool v1 = x1 < " +
+             (fam ? "N0 + " + std::to_string(c0.ext[0] - g.n[0]) : std::to_string(c0.ext[0])) + ";\n";
     const std::string stx = !shfl ? "true"
                                   : (c0.ext[0] < g.B[0] ? "(act && x0 < " + std::to_string(c0.ext[0]) + ")" : "act");
     if (shfl && used[0])
@@ -792,7 +817,7 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         }
         return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
     };
-    if (h->jit_prefetch) {
+    if (h->jit_prefetch && !fam) {
         // every row the group reads, requested into L2 up front: the loads
         // below then wait for L2 rather than DRAM
         std::set<std::pair<int, int>> seen;
@@ -829,6 +854,7 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
             const int a = cp.code >> 1, g2 = cp.code & 1;
             if (!val_done.insert({a, cp.src}).second) continue;
             const long long so = (long long)cp.src * g.cs;
+            const std::string sos = off(cp.src);
             if (a == 0 && shfl) {
                 // one 128-bit load of the pair; the third value from the
                 // neighbouring lane (lane 0 / 31 load it); pairs at the row
@@ -856,29 +882,33 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
                               sel2.c_str());
             } else if (a == 0)
                 std::snprintf(b, sizeof b,
-                              "    const double X%d_a0 = ld1(Up + %lld + hx0_%d), X%d_b0 = ld1(Up + %lld + lx0_%d), "
-                              "X%d_a1 = ld1(Up + %lld + (%shx1_%d%s)), X%d_b1 = ld1(Up + %lld + (%slx1_%d%s));\n",
-                              cp.src, so, g2, cp.src, so, g2, cp.src, so, sel1.c_str(), g2, sel2.c_str(), cp.src, so,
-                              sel1.c_str(), g2, sel2.c_str());
+                              "    const double X%d_a0 = ld1(Up + %s + hx0_%d), X%d_b0 = ld1(Up + %s + lx0_%d), "
+                              "X%d_a1 = ld1(Up + %s + (%shx1_%d%s)), X%d_b1 = ld1(Up + %s + (%slx1_%d%s));\n",
+                              cp.src, sos.c_str(), g2, cp.src, sos.c_str(), g2, cp.src, sos.c_str(), sel1.c_str(), g2,
+                              sel2.c_str(), cp.src, sos.c_str(), sel1.c_str(), g2, sel2.c_str());
             else
                 std::snprintf(b, sizeof b,
-                              "    const double2 %c%d_h = ld2(Up + %lld + h%s_%d), %c%d_l = ld2(Up + %lld + l%s_%d);\n",
-                              a == 1 ? 'Y' : 'Z', cp.src, so, an[a], g2, a == 1 ? 'Y' : 'Z', cp.src, so, an[a], g2);
+                              "    const double2 %c%d_h = ld2(Up + %s + h%s_%d), %c%d_l = ld2(Up + %s + l%s_%d);\n",
+                              a == 1 ? 'Y' : 'Z', cp.src, sos.c_str(), an[a], g2, a == 1 ? 'Y' : 'Z', cp.src, sos.c_str(),
+                              an[a], g2);
             o += b;
         }
         std::snprintf(b, sizeof b,
-                      "    {\n        double* Uj = U + pt + %lld;\n"
+                      "    {\n        double* Uj = U + pt + %s;\n"
                       "        const double2 u = *reinterpret_cast<const double2*>(Uj);\n"
                       "        double SA = 0.0, SB = 0.0;\n",
-                      (long long)j * g.cs);
+                      off(j).c_str());
         o += b;
         bool first = true;
         for (int qq = c.cbeg; qq < c.cend; ++qq) {
             const smg::DevCoup& cp = h->coups[qq];
             const int a = cp.code >> 1;
             const int mode_div = h->exact_recip[a];
-            const std::string H = lit(g.h[a]), RH = lit(h->rh[a]), W = lit(cp.w);
-            const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
+            // the family form divides with two correction steps: exact for
+            // every normal spacing, so its instances need not share one
+            const std::string H = fam ? "H" + std::to_string(a) : clit(g.h[a]),
+                              RH = fam ? "RH" + std::to_string(a) : clit(h->rh[a]), W = clit(cp.w);
+            const char* dv = fam ? "div1" : (mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0"));
             const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
             first = false;
             std::string dA, dB;
@@ -994,7 +1024,12 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
             const long long ctas = R > 0 ? (long long)(k1 - k0) * ((rows + R - 1) / R) * R * (cta_per_group / rows)
                                          : (long long)(k1 - k0) * cta_per_group;
             KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase, ctas};
-            for (int j = k0; j < k1; ++j) emit_shared_group(k.src, h, phase, j, G[j], rec);
+            ConstTable tab;
+            std::string body;
+            g_ctab = h->jit_const ? &tab : nullptr;
+            for (int j = k0; j < k1; ++j) emit_shared_group(body, h, phase, j, G[j], rec);
+            g_ctab = nullptr;
+            k.src += ctab_decl(tab) + body;
             emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
             P.push_back(std::move(k));
         }
@@ -1332,53 +1367,10 @@ std::vector<KernelSrc> adj_programs(const smg_handle* h, int block, int group, i
 // Instances whose generated code would be equal apart from the grid (same
 // closure and order, dimensions, boundary conditions, which coefficients are
 // arrays, filter mode) form a family and share kernels; the grid sizes,
-// strides, spacing and dt/2 of each instance come from a FamGeom table.  A
-// CTA takes one (instance, group, chunk, row) item from its kernel's list.
-void emit_fam_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& D, int group) {
-    const smg::DevGrid& g = h->g;
-    char b[1024];
-    const int d0 = k * group, d1 = std::min<int>((k + 1) * group, (int)D.size());
-    o += "static __device__ __forceinline__ void " + group_name(phase, k) +
-         "(const FamGeom& G, int kf, int mode, int x0, int y, int z) {\n"
-         "    double* U = G.U; const DevField* F = G.F; const double hdt = G.hdt;\n"
-         "    const int N0 = G.n[0], N1 = G.n[1], N2 = G.n[2];\n"
-         "    const long long S1 = G.s1, S2 = G.s2, CS = G.cs;\n"
-         "    const double H0 = G.h[0], H1 = G.h[1], H2 = G.h[2], RH0 = G.rh[0], RH1 = G.rh[1], RH2 = G.rh[2];\n"
-         "    (void)N0; (void)N1; (void)N2; (void)S2; (void)H0; (void)H1; (void)H2; (void)RH0; (void)RH1; (void)RH2;\n"
-         "    const int x1 = x0 + 1;\n"
-         "    const long long pt = z * S2 + y * S1 + x0;\n"
-         "    const double* Up = U + pt;\n"
-         "    (void)x1; (void)kf; (void)mode; (void)Up;\n";
-    bool used[3] = {false, false, false};
-    for (int i = d0; i < d1; ++i)
-        for (int q = h->comps[D[i]].cbeg; q < h->comps[D[i]].cend; ++q) used[h->coups[q].code >> 1] = true;
-    if (used[0])
-        for (int g2 = 0; g2 < 2; ++g2) {
-            std::snprintf(b, sizeof b,
-                          "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
-                          "    { int hi, lo; stencil(x0, N0, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
-                          "      stencil(x1, N0, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
-                          g2, g2, g2, g2, g.bc[0], g2, g2, g2, g.bc[0], g2, g2, g2);
-            o += b;
-        }
-    const char* an[3] = {"x", "y", "z"};
-    for (int a = 1; a < 3; ++a) {
-        if (!used[a]) continue;
-        const char* p = a == 1 ? "y" : "z";
-        const char* st = a == 1 ? "S1" : "S2";
-        for (int g2 = 0; g2 < 2; ++g2) {
-            std::snprintf(b, sizeof b,
-                          "    int h%s_%d, l%s_%d;\n"
-                          "    { int hi, lo; stencil(%s, N%d, %d, %d, hi, lo); h%s_%d = (int)((hi - %s) * %s); "
-                          "l%s_%d = (int)((lo - %s) * %s); }\n",
-                          an[a], g2, an[a], g2, p, a, g.bc[a], g2, an[a], g2, p, st, an[a], g2, p, st);
-            o += b;
-        }
-    }
-    for (int i = d0; i < d1; ++i) emit_dest(o, h, phase, D[i], i, false, true);
-    o += "}\n";
-}
-
+// strides, spacing and dt/2 of each instance come from a FamGeom table.  The
+// groups are the plain kernels' shared-load groups in level order, emitted
+// in the family form of emit_shared_group.  A CTA takes one (instance,
+// group, chunk, row) item from its kernel's list.
 std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, int per) {
     const smg::DevGrid& g = h->g;
     std::vector<KernelSrc> P;
@@ -1386,13 +1378,20 @@ std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, i
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
         if (D.empty()) continue;
-        const int ng = ((int)D.size() + group - 1) / group;
+        // the plain kernels' shared-load groups, in coupling-level order
+        const std::vector<std::vector<int>> G = shared_groups(h, phase, group);
+        const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            // grid: the item count, filled in per batch
+            // grid: the group count (the work items are built per batch)
             KernelSrc K{kPrelude, "smg_fam_p" + std::to_string(phase) + "_" + std::to_string(k0), phase, k1 - k0};
-            for (int k = k0; k < k1; ++k) emit_fam_group(K.src, h, phase, k, D, group);
+            ConstTable tab;
+            std::string body;
+            g_ctab = h->jit_const ? &tab : nullptr;
+            for (int k = k0; k < k1; ++k) emit_shared_group(body, h, phase, k, G[k], false, true);
+            g_ctab = nullptr;
+            K.src += ctab_decl(tab) + body;
             char b[1024];
             std::snprintf(b, sizeof b,
                           "extern \"C\" __global__ void __launch_bounds__(%s) %s(const FamGeom* __restrict__ geo, "
@@ -1976,6 +1975,11 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
         extra.insert(extra.end(), adj.begin(), adj.end());
         for (const KernelSrc& k : extra) s += "// ---- program (" + k.name + ")\n" + k.src;
     }
+    std::vector<KernelSrc> fam;
+    if (compile == 3) {   // also the batched solver's family kernels
+        fam = fam_programs(h, h->jit_block, h->jit_group, h->jit_split > 0 ? h->jit_split : 16);
+        for (const KernelSrc& k : fam) s += "// ---- program (" + k.name + ")\n" + k.src;
+    }
     if (len) *len = (int64_t)s.size();
     if (buf && cap > 0) {
         const size_t n = std::min<size_t>((size_t)cap - 1, s.size());
@@ -1991,6 +1995,10 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
             std::vector<KernelSrc> adj(extra.end() - adj_count(extra), extra.end());
             rc = compile_programs(rec, 64, h->jit_calls != 0, cubins, err);
             if (rc == SMG_OK) rc = compile_programs(adj, 64, false, cubins, err);
+        }
+        if (rc == SMG_OK && !fam.empty()) {
+            std::vector<std::vector<char>> cubins;
+            rc = compile_programs(fam, h->jit_regs, false, cubins, err);
         }
         if (rc != SMG_OK) smg::set_global_error("smg_jit_source: " + err);
     }

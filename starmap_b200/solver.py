@@ -261,7 +261,8 @@ def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay
     """CUDA C++ source of the problem's specialised kernels (SMG_VARIANT_JIT)
     for the SMG_TUNE_JIT_* settings in ``tune`` ({key: value}); with
     compile=True (1) also compiled by NVRTC for sm_100a (no GPU needed);
-    compile=2 adds the adjoint's recording and backward-phase kernels."""
+    compile=2 adds the adjoint's recording and backward-phase kernels,
+    compile=3 the batched solver's family kernels."""
     L = _lib.lib()
     p, keep, _ = build_problem(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source,
                                decay_t, decay_a, filter_mode, filter1, filter2)
@@ -269,7 +270,7 @@ def jit_source(n, bc, h, gt, Mx, My, Mz, fields, sigma_t, sigma_a, source, decay
     keys = (_lib.C.c_int32 * max(len(tune), 1))(*[int(k) for k in tune])
     vals = (_lib.C.c_int32 * max(len(tune), 1))(*[int(v) for v in tune.values()])
     ln = _lib.C.c_int64()
-    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), 2 if compile == 2 else 0, None, 0,
+    check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), int(compile) if int(compile) >= 2 else 0, None, 0,
                            _lib.C.byref(ln)))
     buf = _lib.C.create_string_buffer(ln.value + 1)
     check(L.smg_jit_source(_lib.C.byref(p), keys, vals, len(tune), int(compile), buf, ln.value + 1,

@@ -49,7 +49,8 @@ def test_generated_source_structure(name):
 @pytest.mark.parametrize("name", ["lin_p7_periodic", "odd_mixed_bc", "pt3d_p3", "lattice_p4_full", "spn_3d"])
 @pytest.mark.parametrize("layout", [dict(calls=0, split=4, xpair=0), dict(calls=1, split=2, xpair=1),
                                     dict(calls=0, split=0, xpair=1), dict(calls=0, split=16, prefetch=1),
-                                    dict(calls=0, split=16, xpair=2), dict(calls=0, split=16, band=5)])
+                                    dict(calls=0, split=16, xpair=2), dict(calls=0, split=16, band=5),
+                                    dict(calls=0, split=16, const=1)])
 def test_generated_source_compiles(name, layout):
     if not _nvrtc_available():
         pytest.skip("NVRTC library not present")
@@ -67,3 +68,16 @@ def test_adjoint_kernels_compile(name):
         pytest.skip("NVRTC library not present")
     S, src = _source(name, compile=2, block=64, group=3)
     assert "smg_adj_p0_0(" in src and "smg_adj_p1_0(" in src and "_r(" in src
+
+
+@pytest.mark.parametrize("name", ["odd_mixed_bc", "pt3d_p3", "lattice_p5_substep", "spn_3d", "aniso_2d"])
+def test_family_kernels_compile(name):
+    """The batched solver's family kernels (shared-load groups with the grid
+    taken from the instance's geometry at run time) compile for sm_100a."""
+    if not _nvrtc_available():
+        pytest.skip("NVRTC library not present")
+    S, src = _source(name, compile=3, block=64, group=4)
+    assert "smg_fam_p1_0(" in src and "const FamGeom& G" in src
+    # one block per destination in the family kernels too
+    fam = src[src.index("// ---- program (smg_fam_"):]
+    assert fam.count("double* Uj = U + pt + ") == S.n_sys

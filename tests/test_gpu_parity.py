@@ -162,8 +162,8 @@ def test_auto_runs_the_specialised_kernels():
 @pytest.mark.parametrize("block,group,split,calls,xpair,prefetch", [
     (32, 1, 4, 0, 0, 0), (128, 3, 1, 1, 0, 0), (256, 64, 4, 0, 1, 0), (64, 4, 0, 0, 1, 0), (64, 2, 3, 1, 1, 0),
     (64, 8, 16, 0, 0, 1), (64, 8, 16, 0, 2, 0), (32, 3, 16, 0, 2, 0)])
-@pytest.mark.parametrize("band", [0, 3])
-def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, band):
+@pytest.mark.parametrize("band,const", [(0, 0), (3, 0), (0, 1)])
+def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, band, const):
     from starmap_b200 import _lib
     from starmap_b200.solver import setup_gpu
     par = starmap_init(cases.odd_mixed_bc())
@@ -179,6 +179,7 @@ def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, b
                 solver.tune(_lib.SMG_TUNE_JIT_XPAIR, xpair)
                 solver.tune(_lib.SMG_TUNE_JIT_PREFETCH, prefetch)
                 solver.tune(_lib.SMG_TUNE_JIT_BAND, band)
+                solver.tune(_lib.SMG_TUNE_JIT_CONST, const)
                 solver.set_variant(5)
             else:
                 solver.set_variant(4)
