@@ -137,7 +137,8 @@ int smg_set_dt(smg_handle* h, double dt);
 
 /* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
  * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
- * handle's stream; the step loop is replayed from a captured CUDA graph. */
+ * handle's stream; steps that move under 1 GB are replayed from captured
+ * 64-step CUDA graphs, heavier ones are launched directly (SMG_TUNE_GRAPH_STEPS). */
 int smg_run(smg_handle* h, int64_t nsteps);
 
 /* Wait for all work of `h`. */
@@ -181,6 +182,8 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
 #define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them */
 #define SMG_TUNE_JIT_BAND   13   /* CTA order of the generated kernels: 0 group-major, R > 0 bands of R rows */
 #define SMG_TUNE_JIT_CONST  14   /* 1 (default): coupling weights and grid constants read from a __constant__ table; 0: immediates */
+#define SMG_TUNE_GRAPH_STEPS 15  /* steps per captured CUDA graph of smg_run: 0 direct launches, no graph; -1 (default)
+                                    direct launches when a step moves 1 GB or more, else 64 */
 int smg_tune(smg_handle* h, int32_t key, int32_t value);
 
 /* Kernel-only timing of the last smg_run (milliseconds, CUDA events on the

@@ -36,6 +36,7 @@ SMG_TUNE_JIT_XPAIR = 11
 SMG_TUNE_JIT_PREFETCH = 12
 SMG_TUNE_JIT_BAND = 13
 SMG_TUNE_JIT_CONST = 14
+SMG_TUNE_GRAPH_STEPS = 15
 
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1

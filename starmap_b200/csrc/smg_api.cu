@@ -69,6 +69,9 @@ void free_device(smg_handle* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
     cudaFree(h->dU);
+    cudaFree(h->dStage);
+    h->dStage = nullptr;
+    h->stage_bytes = 0;
     cudaFree(h->dFields);
     cudaFree(h->dComps);
     cudaFree(h->dCoups);
@@ -99,6 +102,50 @@ void free_device(smg_handle* h) {
     if (h->stream) cudaStreamDestroy(h->stream);
     h->ev0 = h->ev1 = nullptr;
     h->stream = nullptr;
+}
+
+// State transfers go through a staging buffer: each component of a chunk is
+// one linear copy (the copy engines move padded rows of a few KB several
+// times slower than contiguous data), and one kernel scatters the chunk into
+// (or gathers it from) the padded slots.  A component larger than the
+// staging buffer takes the pitched copy below.
+constexpr size_t kStageBytes = 64u << 20;
+constexpr int kXferMax = 64;   // components per chunk (kernel parameter space)
+
+struct XferChunk {
+    int n;
+    int e0[kXferMax], rows[kXferMax], e1[kXferMax];
+    long long stage_off[kXferMax], slot_off[kXferMax];
+};
+
+// to_slots: stage -> padded slots, else slots -> stage.  blockIdx.z is the
+// component of the chunk, x runs along rows, blockIdx.y strides over rows.
+__global__ void k_xfer(XferChunk c, double* __restrict__ stage, double* __restrict__ U, long long s1, long long s2,
+                       int to_slots) {
+    const int k = blockIdx.z;
+    if (k >= c.n) return;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e0 = c.e0[k], e1 = c.e1[k];
+    if (x >= e0) return;
+    double* st = stage + c.stage_off[k];
+    double* sl = U + c.slot_off[k];
+    for (int r = blockIdx.y; r < c.rows[k]; r += gridDim.y) {
+        const long long d = (long long)(r / e1) * s2 + (long long)(r % e1) * s1 + x;
+        const long long q = (long long)r * e0 + x;
+        if (to_slots) sl[d] = st[q];
+        else st[q] = sl[d];
+    }
+}
+
+cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, bool to_slots) {
+    int e0max = 1, rows_max = 1;
+    for (int k = 0; k < c.n; ++k) {
+        e0max = std::max(e0max, c.e0[k]);
+        rows_max = std::max(rows_max, c.rows[k]);
+    }
+    dim3 grid((unsigned)((e0max + 127) / 128), (unsigned)std::min(rows_max, 4096), (unsigned)c.n);
+    k_xfer<<<grid, 128, 0, h->stream>>>(c, h->dStage, h->dU, h->g.s1, h->g.s2, to_slots ? 1 : 0);
+    return cudaGetLastError();
 }
 
 // Copy a column-major host array with extents e[] (kernel axes) into a
@@ -680,7 +727,9 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device) {
         return r;
     };
     const size_t slot_bytes = (size_t)h->g.cs * 8;
+    h->stage_bytes = std::min<size_t>(kStageBytes, slot_bytes * ns);
     if ((e = alloc((void**)&h->dU, slot_bytes * ns)) != cudaSuccess ||
+        (e = alloc((void**)&h->dStage, h->stage_bytes)) != cudaSuccess ||
         (e = alloc((void**)&h->dFields, slot_bytes * (size_t)std::max(nslots, 1))) != cudaSuccess ||
         (e = alloc((void**)&h->dComps, sizeof(DevComp) * ns)) != cudaSuccess ||
         (e = alloc((void**)&h->dCoups, sizeof(DevCoup) * std::max<size_t>(h->coups.size(), 1))) != cudaSuccess ||
@@ -765,8 +814,34 @@ int smg_set_state(smg_handle* h, const double* const* U) {
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_set_state: NULL argument");
     for (int j = 0; j < h->n_sys; ++j)
         if (!U[j]) return fail(h, SMG_EINVAL, "smg_set_state: NULL component pointer");
-    for (int j = 0; j < h->n_sys; ++j)
-        SMG_CUDA(h, put_slot(h, h->dU + (size_t)j * h->g.cs, U[j], h->comps[j].ext));
+    XferChunk c;
+    c.n = 0;
+    size_t used = 0;
+    auto flush = [&]() -> cudaError_t {
+        cudaError_t e = c.n ? xfer_launch(h, c, true) : cudaSuccess;
+        c.n = 0;
+        used = 0;
+        return e;
+    };
+    for (int j = 0; j < h->n_sys; ++j) {
+        const int* e = h->comps[j].ext;
+        const size_t bytes = (size_t)e[0] * e[1] * e[2] * 8;
+        if (bytes > h->stage_bytes) {
+            SMG_CUDA(h, put_slot(h, h->dU + (size_t)j * h->g.cs, U[j], e));
+            continue;
+        }
+        if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
+        SMG_CUDA(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->dStage) + used, U[j], bytes, cudaMemcpyHostToDevice,
+                                    h->stream));
+        c.e0[c.n] = e[0];
+        c.e1[c.n] = e[1];
+        c.rows[c.n] = e[1] * e[2];
+        c.stage_off[c.n] = (long long)(used / 8);
+        c.slot_off[c.n] = (long long)j * h->g.cs;
+        ++c.n;
+        used += (bytes + 255) / 256 * 256;
+    }
+    SMG_CUDA(h, flush());
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     h->state_set = true;
     return SMG_OK;
@@ -774,8 +849,44 @@ int smg_set_state(smg_handle* h, const double* const* U) {
 
 int smg_get_state(smg_handle* h, double* const* U) {
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_state: NULL argument");
-    for (int j = 0; j < h->n_sys; ++j)
-        if (U[j]) SMG_CUDA(h, get_slot(h, U[j], h->dU + (size_t)j * h->g.cs, h->comps[j].ext));
+    // per chunk: gather into the staging buffer, then one linear copy per
+    // component (the next chunk's gather waits for these on the stream)
+    XferChunk c;
+    c.n = 0;
+    size_t used = 0;
+    std::vector<std::pair<int, size_t>> pend;   // (component, staging byte offset)
+    auto flush = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        if (c.n) e = xfer_launch(h, c, false);
+        for (size_t i = 0; i < pend.size() && e == cudaSuccess; ++i) {
+            const int* x = h->comps[pend[i].first].ext;
+            e = cudaMemcpyAsync(U[pend[i].first], reinterpret_cast<const char*>(h->dStage) + pend[i].second,
+                                (size_t)x[0] * x[1] * x[2] * 8, cudaMemcpyDeviceToHost, h->stream);
+        }
+        c.n = 0;
+        used = 0;
+        pend.clear();
+        return e;
+    };
+    for (int j = 0; j < h->n_sys; ++j) {
+        if (!U[j]) continue;
+        const int* e = h->comps[j].ext;
+        const size_t bytes = (size_t)e[0] * e[1] * e[2] * 8;
+        if (bytes > h->stage_bytes) {
+            SMG_CUDA(h, get_slot(h, U[j], h->dU + (size_t)j * h->g.cs, e));
+            continue;
+        }
+        if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
+        c.e0[c.n] = e[0];
+        c.e1[c.n] = e[1];
+        c.rows[c.n] = e[1] * e[2];
+        c.stage_off[c.n] = (long long)(used / 8);
+        c.slot_off[c.n] = (long long)j * h->g.cs;
+        ++c.n;
+        pend.push_back({j, used});
+        used += (bytes + 255) / 256 * 256;
+    }
+    SMG_CUDA(h, flush());
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     return SMG_OK;
 }
@@ -905,7 +1016,16 @@ int smg_run(smg_handle* h, int64_t nsteps) {
 // nsteps steps on the handle's stream; with `events`, bracketed by the
 // handle's timing events (smg_last_run_stats)
 int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
-    const int64_t kBlock = 64;   // steps per captured graph
+    // steps per captured graph (0: none).  By default a step that moves a
+    // gigabyte or more (about 24 bytes per moment-cell update) runs as
+    // direct launches: the host enqueues a step far faster than the GPU runs
+    // it, and a fresh handle then pays no graph capture; lighter steps are
+    // replayed from 64-step graphs
+    int64_t kBlock = h->graph_block;
+    if (kBlock < 0) {
+        const double step_bytes = 24.0 * (double)h->g.B[0] * h->g.B[1] * h->g.B[2] * h->n_sys;
+        kBlock = step_bytes >= 1e9 ? 0 : 64;
+    }
     if (h->variant == SMG_VARIANT_AUTO && !h->jit && !h->jit_failed && nsteps > 0) {
         // first run: generate and compile the specialised kernels; without
         // NVRTC (or for tables beyond 32-bit offsets) AUTO keeps the pair kernel
@@ -920,7 +1040,16 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
         }
     }
     int64_t left = nsteps;
-    if (left >= kBlock) {
+    int64_t launches = 0, rem = 0;
+    if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    if (kBlock > 0 && left >= kBlock && (!h->graph || h->graph_steps != kBlock)) {
+        // the first block goes to the stream as direct launches, so that the
+        // GPU runs it while the graph for the following blocks is captured
+        SMG_CUDA(h, enqueue_steps(h, kBlock, h->stream, &rem));
+        launches += rem;
+        left -= kBlock;
+    }
+    if (kBlock > 0 && left >= kBlock) {
         if (!h->graph || h->graph_steps != kBlock) {
             if (h->graph) cudaGraphExecDestroy(h->graph);
             h->graph = nullptr;
@@ -936,9 +1065,7 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
             h->graph_steps = kBlock;
         }
     }
-    int64_t launches = 0, rem = 0;
-    if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
-    for (; left >= kBlock; left -= kBlock) {
+    for (; kBlock > 0 && left >= kBlock; left -= kBlock) {
         SMG_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
         launches += h->graph_launches;
     }
@@ -1022,6 +1149,10 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->jit_band = value;
             smg::jit_free(h);
             h->jit_failed = false;
+            break;
+        case SMG_TUNE_GRAPH_STEPS:
+            if (value < -1 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: graph steps must be -1..4096");
+            h->graph_block = value;
             break;
         case SMG_TUNE_ADJ_FUSED:
             if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj_fused must be 0 or 1");

@@ -46,6 +46,8 @@ struct smg_handle {
     int field_one = -1, field_zero = -1;
     // device memory
     double* dU = nullptr;
+    double* dStage = nullptr;        // staging for state transfers (linear copies, then a scatter kernel)
+    size_t stage_bytes = 0;
     double* dFields = nullptr;       // slots for array fields
     smg::DevComp* dComps = nullptr;
     smg::DevCoup* dCoups = nullptr;
@@ -66,6 +68,7 @@ struct smg_handle {
     cudaGraphExec_t graph = nullptr;
     int64_t graph_steps = 0;
     int64_t graph_launches = 0;
+    int graph_block = -1;            // steps per captured graph (0: direct launches; -1: by step size)
     std::string err;
     // strip-kernel schedules (phase 0 = A, 1 = B); empty if not usable
     struct HostSched {

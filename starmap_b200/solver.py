@@ -10,8 +10,8 @@ loop itself (:307-421) runs in ``libstarmap_gpu.so`` through the C ABI of
 ``include/starmap_gpu.h``; the final components come back in the reference's
 ``output`` layout (:484-500) and the reference's summary is printed (:477-482).
 
-Autonomous problems run the whole loop in one library call (a replayed CUDA
-graph).  Time-dependent materials, sources or filters are re-evaluated on the
+Autonomous problems run the whole loop in one library call (replayed CUDA
+graphs for light steps, direct launches for heavy ones).  Time-dependent materials, sources or filters are re-evaluated on the
 host every step exactly where the reference does, uploaded with
 ``smg_set_field`` and advanced one step at a time.  Output times ``t_plot``
 with a user ``output`` hook are served by running the loop in segments and

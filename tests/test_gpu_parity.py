@@ -193,6 +193,31 @@ def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, b
         np.testing.assert_array_equal(outs[0][j], outs[1][j])
 
 
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "pt3d_p3", "box3d_bc1_p2_full"])
+def test_graph_steps_keep_results(name):
+    """Direct launches, graphs of 1, 5 and 64 steps and the default policy
+    give bit-identical states (the block boundaries split the fused A-A
+    phases, which must not change a value)."""
+    from starmap_b200 import _lib
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(cases.ALL[name]())
+    outs = []
+    for gb in (-1, 0, 1, 5, 64):
+        S, fs, solver, T = setup_gpu(par)
+        try:
+            solver.tune(_lib.SMG_TUNE_GRAPH_STEPS, gb)
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.run(70)
+            solver.run(11)
+            outs.append(solver.get_state())
+        finally:
+            solver.close()
+    for o in outs[1:]:
+        for j in outs[0]:
+            np.testing.assert_array_equal(outs[0][j], o[j])
+
+
 def test_gpu_pn_equals_spn_boxes():
     from test_cpu_oracle_properties import boxes_prob
     outP = starmap_solver(starmap_init(boxes_prob("P", 9)))
