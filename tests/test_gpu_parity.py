@@ -91,6 +91,41 @@ def test_state_roundtrip_and_layout():
         solver.close()
 
 
+@pytest.mark.parametrize("which", ["many_components", "large_components"])
+def test_state_transfer_paths(which):
+    """The staged transfers: 820 components of 80 KB (chunks bounded by the
+    64-component kernel limit and by the staging size), and 3D components of
+    150 MB, larger than the staging buffer, which take the pitched copy.
+    Upload then download is the identity, and a partial download returns
+    only the components asked for."""
+    from starmap_b200 import configs
+    from starmap_b200.solver import GpuSolver, prepare
+    if which == "many_components":
+        par = starmap_init(configs.lattice(n=100, n_mom=39))
+    else:
+        par = starmap_init(dict(closure="P", n_mom=1, ax=[-1, 1, -1, 1, -1, 1], n=[265, 264, 263], bc=[1, 0, 1],
+                                ic=lambda x, y, z: 0 * x, sigma_a=lambda x, y, z: 0.0,
+                                sigma_s0=lambda x, y, z: 1.0, tfinal=1.0, quiet=True))
+    S = prepare(par)
+    rng = np.random.default_rng(11)
+    fields = [(0.3, (1, 1, 1)), (1.0, (1, 1, 1))]
+    solver = GpuSolver(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, fields, [0] * S.n_sys, 0, [-1] * S.n_sys,
+                       decay_t=[1] * S.n_sys, decay_a=1)
+    try:
+        U = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
+        if which == "large_components":
+            assert U[0].nbytes > 64 << 20
+        solver.set_state(U)
+        back = solver.get_state()
+        for j in range(S.n_sys):
+            np.testing.assert_array_equal(back[j], U[j])
+        some = solver.get_state(which=[0, S.n_sys - 1])
+        assert sorted(some) == [0, S.n_sys - 1]
+        np.testing.assert_array_equal(some[S.n_sys - 1], U[S.n_sys - 1])
+    finally:
+        solver.close()
+
+
 def test_full_size_lattice_prefix_vs_c_oracle():
     """The benchmark workload at full size (820 moments, 350x350) for a prefix
     of 4 steps, GPU (default fused strip kernels) vs the oracle's C restatement."""
