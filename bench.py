@@ -482,7 +482,9 @@ def main():
                    "updates_per_step": upd_step, "state_gb": alg["state_bytes"] / 1e9,
                    "l2": "inputs larger than L2 (state %.2f GB > 126 MB), no flush" % (alg["state_bytes"] / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU", "variant": args.variant,
-                   "kernel_family": family},
+                   "kernel_family": family,
+                   "launch": "direct launches (a step moves >= 1 GB)" if 24.0 * cells * n_sys >= 1e9
+                   else "replayed 64-step CUDA graphs"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_step": alg["step"],
