@@ -663,36 +663,41 @@ std::vector<int> phase_dests(const smg_handle* h, int phase) {
 // earlier destination's store is still current.
 std::vector<std::vector<int>> shared_groups(const smg_handle* h, int phase, int group) {
     const std::vector<int> D = phase_dests(h, phase);
-    std::vector<std::set<std::pair<int, int>>> K(D.size());
+    // the distinct (axis, source) keys of each destination, as ids axis*n_sys+src
+    std::vector<std::vector<int>> K(D.size());
     std::map<std::vector<int>, std::vector<int>> by_ext;   // extents -> positions in D
     std::vector<std::vector<int>> order;
     for (size_t p = 0; p < D.size(); ++p) {
         const smg::DevComp& c = h->comps[D[p]];
-        for (int q = c.cbeg; q < c.cend; ++q) K[p].insert({h->coups[q].code >> 1, h->coups[q].src});
+        for (int q = c.cbeg; q < c.cend; ++q) K[p].push_back((h->coups[q].code >> 1) * h->n_sys + h->coups[q].src);
+        std::sort(K[p].begin(), K[p].end());
+        K[p].erase(std::unique(K[p].begin(), K[p].end()), K[p].end());
         std::vector<int> e(c.ext, c.ext + 3);
         if (!by_ext.count(e)) order.push_back(e);
         by_ext[e].push_back((int)p);
     }
     std::vector<std::vector<int>> G;
+    std::vector<char> in(3 * (size_t)h->n_sys, 0);   // keys of the group being built
     for (const auto& e : order) {
         std::vector<int> left = by_ext[e];
         while (!left.empty()) {
             std::vector<int> g{left.front()};
             left.erase(left.begin());
-            std::set<std::pair<int, int>> ks = K[g[0]];
+            std::fill(in.begin(), in.end(), 0);
+            for (int k : K[g[0]]) in[k] = 1;
             while ((int)g.size() < group && !left.empty()) {
                 size_t best = 0;
                 int bestn = -1;
                 for (size_t i = 0; i < left.size(); ++i) {
                     int n = 0;
-                    for (const auto& k : K[left[i]]) n += (int)ks.count(k);
+                    for (int k : K[left[i]]) n += in[k];
                     if (n > bestn) {
                         bestn = n;
                         best = i;
                     }
                 }
                 g.push_back(left[best]);
-                ks.insert(K[left[best]].begin(), K[left[best]].end());
+                for (int k : K[left[best]]) in[k] = 1;
                 left.erase(left.begin() + best);
             }
             G.push_back(std::move(g));
