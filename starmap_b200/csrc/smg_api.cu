@@ -1145,7 +1145,7 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->jit_failed = false;
             break;
         case SMG_TUNE_JIT_BAND:
-            if (value < 0 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: jit band must be 0..4096");
+            if (value < -1 || value > (1 << 20)) return fail(h, SMG_EINVAL, "smg_tune: jit band must be -1..2^20");
             h->jit_band = value;
             smg::jit_free(h);
             h->jit_failed = false;

@@ -113,7 +113,7 @@ struct smg_handle {
     int jit_xpair = 0;               // x differences from aligned 128-bit pairs (1) or 64-bit loads (0)
     int jit_prefetch = 0;            // L2 prefetch of a group's rows before its loads
     int jit_const = 1;               // coupling weights and grid constants from a __constant__ table
-    int jit_band = 0;                // rows per band of the CTA order (0: group-major)
+    int jit_band = -1;               // rows per band of the CTA order (0: group-major; -1: by slot size)
     bool jit_failed = false;         // AUTO tried the JIT and it was unavailable
     std::string jit_err;
 };

@@ -589,6 +589,22 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
 // kernel over groups [k0, k1) of one phase type: CTA -> (group, row, chunk),
 // then the group's code (inlined, or a call when the groups are compiled
 // separately)
+// Rows per band of the CTA order (0: group-major).  By default group-major
+// order, in which each group streams its sources over the whole grid, is
+// kept while a component slot is under 4 MB: the groups that run at the same
+// time then reuse shared sources in L2.  With larger slots (3D grids) a
+// group's sources no longer stay in L2 for the next group, so the CTAs go
+// band by band, the band sized so that all components' rows of a band take
+// about 48 MB (0.4 of the L2).
+int band_rows(const smg_handle* h) {
+    if (h->jit_band >= 0) return h->jit_band;
+    const double slot = (double)h->g.cs * 8;
+    if (slot < 4.0 * (1 << 20)) return 0;
+    const long long rows = (long long)h->g.B[1] * h->g.B[2];
+    const double row_all = (double)h->n_sys * h->g.s1 * 8;
+    return (int)std::max(1LL, std::min(rows, (long long)(48.0 * (1 << 20) / row_all)));
+}
+
 void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k1, int block, bool inl,
                    const std::string& name, bool rec) {
     const smg::DevGrid& g = h->g;
@@ -602,7 +618,7 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
     // with bands of R rows, band-major (every group of the kernel on R rows,
     // then the next band), so that the source rows a band needs stay in L2
     // while all groups use them
-    const int R = inl ? h->jit_band : 0;
+    const int R = inl ? band_rows(h) : 0;
     const long long rows = (long long)g.B[1] * g.B[2];
     std::string map;
     if (R > 0) {
@@ -1024,7 +1040,7 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         const int step = per > 0 ? per : ng;
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            const int R = h->jit_band;
+            const int R = band_rows(h);
             const long long rows = (long long)g.B[1] * g.B[2];
             const long long ctas = R > 0 ? (long long)(k1 - k0) * ((rows + R - 1) / R) * R * (cta_per_group / rows)
                                          : (long long)(k1 - k0) * cta_per_group;

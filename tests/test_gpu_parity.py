@@ -253,6 +253,30 @@ def test_graph_steps_keep_results(name):
             np.testing.assert_array_equal(outs[0][j], o[j])
 
 
+def test_jit_band_order_keeps_results_3d():
+    """CTA order by bands of rows (the default for component slots of 4 MB and
+    more: here 84^3 cells, about 714-row bands) against group-major order and
+    explicit odd band sizes: bit-identical states."""
+    from starmap_b200 import _lib, configs
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(configs.pointsource3d(n=84, n_mom=9, tfinal=0.1))
+    outs = []
+    for band in (-1, 0, 1, 333):
+        S, fs, solver, T = setup_gpu(par)
+        try:
+            solver.tune(_lib.SMG_TUNE_JIT_BAND, band)
+            solver.set_variant(5)
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.run(4)
+            outs.append(solver.get_state([0, 7, 50, 99]))
+        finally:
+            solver.close()
+    for o in outs[1:]:
+        for j in outs[0]:
+            np.testing.assert_array_equal(outs[0][j], o[j])
+
+
 def test_gpu_pn_equals_spn_boxes():
     from test_cpu_oracle_properties import boxes_prob
     outP = starmap_solver(starmap_init(boxes_prob("P", 9)))
