@@ -1855,14 +1855,17 @@ int jit_family_build(const std::vector<smg_handle*>& inst, int block, int group,
         K.phase = all[i].phase;
         K.fam = fam_idx[i];
         // work items of the kernel's groups over the family's instances:
-        // (member, group, chunk, row), group-major so that CTAs running at
-        // the same time share code
+        // (member, group, chunk, row), instance by instance and within an
+        // instance group by group: the CTAs running at the same time share
+        // a group's code, and the groups of one instance reuse its sources
+        // in L2 (group-major over all members streamed every group's sources
+        // through L2 once per group)
         const int k0 = std::stoi(all[i].name.substr(all[i].name.rfind('_') + 1));
         const int k1 = k0 + (int)all[i].grid;
         std::vector<int4> items;
         const std::vector<int>& mem = S->members[K.fam];
-        for (int grp = k0; grp < k1; ++grp)
-            for (size_t li = 0; li < mem.size(); ++li) {
+        for (size_t li = 0; li < mem.size(); ++li)
+            for (int grp = k0; grp < k1; ++grp) {
                 const smg_handle* h = inst[mem[li]];
                 const int tpr = (h->g.B[0] + 1) / 2;
                 const int nch = (tpr + block - 1) / block;
