@@ -132,9 +132,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(family="jit"):
+def ncu_traffic(family="jit", name=None):
     """DRAM bytes per step of the phase kernels of `family` from the committed ncu summary (or None)."""
-    name = "phase_kernels_jit_lattice_p39.txt" if family == "jit" else "phase_kernels_lattice_p39_350.txt"
+    if name is None:
+        name = "phase_kernels_jit_lattice_p39.txt" if family == "jit" else "phase_kernels_lattice_p39_350.txt"
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
@@ -332,7 +333,8 @@ def bench_3d(steps: int = 96, n: int = 128):
             "ms_per_step": ms / steps, "kernel_family": family, "launches": int(launches), "finite": finite,
             "state_gb": alg["state_bytes"] / 1e9,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": kind, "algorithmic_bytes_per_step": alg["step"]}}
+                         "frac": achieved / peak, "peak_kind": kind, "algorithmic_bytes_per_step": alg["step"],
+                         "traffic": ncu_traffic(name="phase_kernels_jit_pointsource3d_p9.txt") if n == 128 else None}}
 
 
 def host_buffers(S):
