@@ -135,6 +135,27 @@ int smg_set_field(smg_handle* h, int32_t field, const double* data, double scala
  * (starmap_solver.m:267-274, 531-535) at this point. */
 int smg_set_dt(smg_handle* h, double dt);
 
+/* Time of the current state (default 0): the start of the next smg_run when
+ * sources are evaluated on the device (smg_set_source_expr); each step then
+ * advances it by dt, as the reference's loop does (t = t + dt). */
+int smg_set_time(smg_handle* h, double t);
+
+/* Time-dependent source of component `comp` evaluated on the device: before
+ * every step of smg_run the library writes Q_comp = expr at each point of the
+ * component's grid, at the step's t - dt/2 (starmap_solver.m:276-282), then
+ * runs the step; such runs are not fused across steps and use no CUDA graph.
+ * `expr` is a C++ expression (compiled with NVRTC for sm_100a at the next
+ * smg_run; trusted input only) in x, y, z, t and k: the point's coordinates
+ * in the three solver dimensions, the time and the 1-based component number
+ * -- the arguments of the reference's source hook after starmap_init.
+ * x/y/z hold the coordinates of the component's grid along each solver
+ * dimension (its extent there, 1 for a singleton dimension).  The source must
+ * be an array field of its own; expr = NULL returns to the uploaded values.
+ * The reference evaluates a Matlab function on the host instead; this is the
+ * device-evaluable form of that hook. */
+int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const double* x, const double* y,
+                        const double* z);
+
 /* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
  * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
  * handle's stream; steps that move under 1 GB are replayed from captured

@@ -66,6 +66,7 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device);
 void free_device(smg_handle* h) {
     smg_adjoint_free(h);
     smg::jit_free(h);
+    smg::src_free(h, true);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
     cudaFree(h->dU);
@@ -912,6 +913,57 @@ int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {
     return SMG_OK;
 }
 
+int smg_set_time(smg_handle* h, double t) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_time: NULL handle");
+    if (!std::isfinite(t)) return fail(h, SMG_EINVAL, "smg_set_time: t must be finite");
+    h->t = t;
+    return SMG_OK;
+}
+
+int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const double* x, const double* y,
+                        const double* z) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_source_expr: NULL handle");
+    if (comp < 0 || comp >= h->n_sys) return fail(h, SMG_EINVAL, "smg_set_source_expr: component out of range");
+    const int f = h->comps[comp].Q;
+    size_t at = 0;
+    while (at < h->src_expr.size() && h->src_expr[at].comp != comp) ++at;
+    smg::src_free(h, false);   // the kernels are rebuilt at the next smg_run
+    if (!expr) {   // back to the field's uploaded values
+        if (at < h->src_expr.size()) {
+            cudaFree(h->src_expr[at].dC);
+            h->src_expr.erase(h->src_expr.begin() + at);
+        }
+        return SMG_OK;
+    }
+    if (f < 0 || f >= (int)h->fields_host.size() || !h->fields_host[f].p)
+        return fail(h, SMG_EINVAL, "smg_set_source_expr: the component's source must be an array field");
+    for (int j = 0; j < h->n_sys; ++j)
+        if (j != comp && h->comps[j].Q == f)
+            return fail(h, SMG_EINVAL, "smg_set_source_expr: the source field is shared with another component");
+    if (!x || !y || !z) return fail(h, SMG_EINVAL, "smg_set_source_expr: NULL coordinate vector");
+    const size_t len = std::strlen(expr);
+    if (len == 0 || len > 65536) return fail(h, SMG_EINVAL, "smg_set_source_expr: expression empty or over 64 KB");
+    // coordinates of the component's grid per kernel axis, from the
+    // per-solver-dimension vectors
+    const int* E = h->comps[comp].ext;
+    const double* solver[3] = {x, y, z};
+    std::vector<double> c;
+    for (int a = 0; a < 3; ++a) c.insert(c.end(), solver[h->sd[a]], solver[h->sd[a]] + E[a]);
+    double* d = nullptr;
+    SMG_CUDA(h, cudaMalloc(&d, c.size() * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(h, e, "smg_set_source_expr: coordinates");
+    }
+    if (at == h->src_expr.size()) h->src_expr.emplace_back();
+    else cudaFree(h->src_expr[at].dC);
+    h->src_expr[at].comp = comp;
+    h->src_expr[at].expr = expr;
+    h->src_expr[at].dC = d;
+    return SMG_OK;
+}
+
 int smg_set_dt(smg_handle* h, double dt) {
     if (!h) return fail(h, SMG_EINVAL, "smg_set_dt: NULL handle");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, SMG_EINVAL, "smg_set_dt: dt must be finite and > 0");
@@ -1041,6 +1093,28 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
     }
     int64_t left = nsteps;
     int64_t launches = 0, rem = 0;
+    if (!h->src_expr.empty()) {
+        // sources evaluated on the device: before every step Q at the step's
+        // t - dt/2 (starmap_solver.m:276-282), then one unfused step (the
+        // two phase-A passes around a step boundary see different sources);
+        // the time advances as the host loop does, t = t + dt
+        if (!h->src_expr[0].fn) {
+            std::string why;
+            const int rc = smg::src_build(h, why);
+            if (rc != SMG_OK) return fail(h, rc, "source expressions: " + why);
+        }
+        if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+        for (int64_t k = 0; k < nsteps; ++k) {
+            const double t_end = h->t + h->dt;
+            SMG_CUDA(h, smg::launch_src(h, t_end - h->dt / 2, h->stream));
+            SMG_CUDA(h, enqueue_steps(h, 1, h->stream, &rem));
+            launches += rem + (int64_t)h->src_expr.size();
+            h->t = t_end;
+        }
+        if (events) SMG_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+        h->last_launches = events ? launches : h->last_launches + launches;
+        return SMG_OK;
+    }
     if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
     if (kBlock > 0 && left >= kBlock && (!h->graph || h->graph_steps != kBlock)) {
         // the first block goes to the stream as direct launches, so that the

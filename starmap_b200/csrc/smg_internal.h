@@ -70,6 +70,16 @@ struct smg_handle {
     int64_t graph_launches = 0;
     int graph_block = -1;            // steps per captured graph (0: direct launches; -1: by step size)
     std::string err;
+    // sources evaluated on the device every step (smg_set_source_expr)
+    struct SrcExpr {
+        int comp = -1;
+        std::string expr;                // C++ expression in x, y, z (solver dimensions), t, k
+        double* dC = nullptr;            // coordinates per kernel axis, concatenated
+        void* fn = nullptr;              // CUfunction once built
+    };
+    std::vector<SrcExpr> src_expr;
+    void* src_mod = nullptr;             // CUmodule of the source kernels
+    double t = 0.0;                      // time of the current state (smg_set_time)
     // strip-kernel schedules (phase 0 = A, 1 = B); empty if not usable
     struct HostSched {
         std::vector<smg::Stage> stages;
@@ -152,6 +162,9 @@ cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U
 std::string jit_source(const smg_handle* h, int block, int group);
 int jit_compile(const smg_handle* h, int block, int group, std::string& err);   // compile only (no device)
 int jit_launches(const smg_handle* h, int phase);                                 // kernels per phase
+int src_build(smg_handle* h, std::string& err);       // compile the smg_set_source_expr kernels
+void src_free(smg_handle* h, bool coords);            // unload them (and free their coordinates)
+cudaError_t launch_src(const smg_handle* h, double t, cudaStream_t s);
 int create_host(const smg_problem* p, smg_handle** out);   // host tables only (no CUDA call)
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);

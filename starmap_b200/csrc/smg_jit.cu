@@ -1684,6 +1684,90 @@ cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U
 
 int jit_launches(const smg_handle* h, int phase) { return h->jit ? (int)h->jit->k[phase].size() : 0; }
 
+// ---- sources evaluated on the device --------------------------------------
+// One kernel per registered expression writes Q_j at every point of the
+// component's grid: x, y, z are the point's coordinates in the solver
+// dimensions (the reference's hook arguments, starmap_solver.m:278-282),
+// t the evaluation time, k the 1-based component number.
+void src_free(smg_handle* h, bool coords) {
+    if (h->src_mod) api().ModuleUnload(static_cast<CUmodule_t>(h->src_mod));
+    h->src_mod = nullptr;
+    for (auto& e : h->src_expr) {
+        e.fn = nullptr;
+        if (coords) {
+            cudaFree(e.dC);
+            e.dC = nullptr;
+        }
+    }
+}
+
+int src_build(smg_handle* h, std::string& err) {
+    Api& a = api();
+    if (!a.cu_ok) {
+        err = a.cu_why;
+        return SMG_EINVAL;
+    }
+    src_free(h, false);
+    int axis_of[3];
+    for (int ax = 0; ax < 3; ++ax) axis_of[h->sd[ax]] = ax;
+    std::string src;
+    char b[1024];
+    for (size_t i = 0; i < h->src_expr.size(); ++i) {
+        const auto& e = h->src_expr[i];
+        const int* E = h->comps[e.comp].ext;
+        std::snprintf(b, sizeof b,
+                      "extern \"C\" __global__ void smg_src_%d(double* __restrict__ Q, const double* __restrict__ C, "
+                      "double t) {\n"
+                      "    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;\n"
+                      "    if (i0 >= %d) return;\n"
+                      "    for (int r = blockIdx.y; r < %d; r += gridDim.y) {\n"
+                      "        const int i1 = r %% %d, i2 = r / %d;\n"
+                      "        const double a0 = C[i0], a1 = C[%d + i1], a2 = C[%d + i2];\n"
+                      "        const double x = a%d, y = a%d, z = a%d;\n"
+                      "        const int k = %d;\n"
+                      "        (void)x; (void)y; (void)z; (void)k; (void)t;\n"
+                      "        Q[(long long)i2 * %lld + (long long)i1 * %lld + i0] = (double)(\n",
+                      (int)i, E[0], E[1] * E[2], E[1], E[1], E[0], E[0] + E[1], axis_of[0], axis_of[1], axis_of[2],
+                      e.comp + 1, (long long)h->g.s2, (long long)h->g.s1);
+        src += b;
+        src += e.expr + "\n        );\n    }\n}\n";
+    }
+    std::vector<char> cubin;
+    int rc = compile_one(src, 0, false, cubin, err);
+    if (rc != SMG_OK) return rc;
+    CUmodule_t m = nullptr;
+    if (a.ModuleLoadData(&m, cubin.data()) != 0) {
+        err = "cuModuleLoadData failed (source expressions)";
+        return SMG_ECUDA;
+    }
+    h->src_mod = m;
+    for (size_t i = 0; i < h->src_expr.size(); ++i) {
+        CUfunction_t f = nullptr;
+        const std::string name = "smg_src_" + std::to_string(i);
+        if (a.ModuleGetFunction(&f, m, name.c_str()) != 0) {
+            err = "cuModuleGetFunction " + name;
+            src_free(h, false);
+            return SMG_ECUDA;
+        }
+        h->src_expr[i].fn = f;
+    }
+    return SMG_OK;
+}
+
+cudaError_t launch_src(const smg_handle* h, double t, cudaStream_t s) {
+    for (const auto& e : h->src_expr) {
+        const int* E = h->comps[e.comp].ext;
+        double* Q = const_cast<double*>(h->fields_host[h->comps[e.comp].Q].p);
+        const double* C = e.dC;
+        double tt = t;
+        void* args[] = {&Q, &C, &tt};
+        const unsigned gx = (unsigned)((E[0] + 127) / 128), gy = (unsigned)std::min(E[1] * E[2], 4096);
+        if (api().LaunchKernel(static_cast<CUfunction_t>(e.fn), gx, gy, 1, 128, 1, 1, 0, s, args, nullptr) != 0)
+            return cudaErrorLaunchFailure;
+    }
+    return cudaSuccess;
+}
+
 // Generated adjoint kernels (compiled like the forward ones, inline layout).
 int jit_build_adj(smg_handle* h, std::string& err) {
     if (h->jit_adj) return SMG_OK;

@@ -144,6 +144,27 @@ class GpuSolver:
     def set_dt(self, dt):
         check(self._L.smg_set_dt(self.h, float(dt)), self.h)
 
+    def set_time(self, t):
+        """Time of the current state (the start of the next run when sources
+        are evaluated on the device)."""
+        check(self._L.smg_set_time(self.h, float(t)), self.h)
+
+    def set_source_expr(self, j, expr, coords=None):
+        """Evaluate the source of component j on the device every step
+        (``smg_set_source_expr``): ``expr`` is a C++ expression in the solver
+        coordinates x, y, z, the time t and the 1-based component k;
+        ``coords`` the component's coordinate vectors per solver dimension.
+        ``expr=None`` returns to uploaded source values."""
+        if expr is None:
+            check(self._L.smg_set_source_expr(self.h, int(j), None, None, None, None), self.h)
+            return
+        cs = [np.ascontiguousarray(np.asarray(c, dtype=np.float64).ravel()) for c in coords]
+        e = self.extents(j)
+        if any(c.size != e[d] for d, c in enumerate(cs)):
+            raise ValueError(f"coordinate vectors must have the component's extents {e}")
+        check(self._L.smg_set_source_expr(self.h, int(j), expr.encode(), dptr(cs[0]), dptr(cs[1]), dptr(cs[2])),
+              self.h)
+
     def active_variant(self):
         """(kernel family the next run uses, reason AUTO could not use JIT)."""
         v = _lib.C.c_int32()
@@ -601,12 +622,21 @@ def starmap_solver(par: dict):
 
     solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], fs["F"])
     t_gpu0 = time.perf_counter()
+    # a time-dependent source given also as an expression is evaluated on the
+    # device every step instead of on the host
+    dev_src = bool(S.src_td) and bool(par.get("source_expr"))
     try:
         solver.set_state(S.U0)
         solver.set_dt(dt)
+        if dev_src:
+            expr = device_source_expr(par["source_expr"], int(par.get("dim", 3)))
+            for j1 in S.source_ind:
+                g = S.G(j1 - 1)
+                solver.set_source_expr(j1 - 1, expr, [S.xs[g[0] - 1], S.ys[g[1] - 1], S.zs[g[2] - 1]])
+            solver.set_time(0.0)
         t_plot = list(np.atleast_1d(np.asarray(par.get("t_plot", [])))) + [np.inf]
         want_plot = par.get("output", _noop_output) is not _noop_output
-        per_step = td_any or S.src_td or S.filter_td
+        per_step = td_any or (S.src_td and not dev_src) or S.filter_td
         step_count = 0
         t_cur = 0.0
         plot_count = 0
@@ -625,7 +655,7 @@ def starmap_solver(par: dict):
                         solver.set_field(T.index[("sT",) + k], sT1[k])
                         solver.set_field(T.index[("ET",) + k], expm1div(-sT1[k] * dt / 2))
                 tn = t_cur + dt
-                if S.src_td:
+                if S.src_td and not dev_src:
                     for j, q in _sources(S, tn, dt).items():
                         solver.set_field(T.index[("Q", j)], q)
                 if S.filter_td:
@@ -678,6 +708,19 @@ def starmap_solver(par: dict):
         print(f"CPU-times\n advection:{gpu_s:12.2f}s{gpu_s / tot * 100:5.0f}%\n "
               f"absorb/scatter:{cpu_setup:7.2f}s{cpu_setup / tot * 100:5.0f}%\n plotting:{0.0:13.2f}s{0:5.0f}%")
     return _output_struct(S, U)
+
+
+def device_source_expr(expr: str, dim: int) -> str:
+    """The user's source expression, written in the variables of the user's
+    own hook (x, y, t, k in 2D; x, y, z, t, k in 3D; x, t, k in 1D), as an
+    expression in the solver dimensions that ``smg_set_source_expr`` takes:
+    in 2D the user's (x, y) are the solver's second and third dimensions, in
+    1D the user's x is the third (the wrapping of starmap_init.m)."""
+    if dim == 3:
+        return "(" + expr + ")"
+    if dim == 2:
+        return "[&](double x, double y) { return (double)(" + expr + "); }(y, z)"
+    return "[&](double x) { return (double)(" + expr + "); }(z)"
 
 
 def _call_output(S, outfn, par, Uplot, step):
