@@ -156,6 +156,21 @@ int smg_set_time(smg_handle* h, double t);
 int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const double* x, const double* y,
                         const double* z);
 
+/* Time-dependent materials evaluated on the device: before every step of
+ * smg_run the library evaluates sigma_a, sigma_s0 and (expr_sm non-NULL)
+ * sigma_sm at t + dt, forms sigma_t = sigma_a + (sigma_s0 - sigma_sm) per
+ * (grid type, order), averages each with its values at t into the field and
+ * writes its decay factor expm1div(-s dt/2) (starmap_solver.m:214-252,
+ * 267-274); the values at t are taken at the first smg_run after
+ * smg_set_time.  Expressions as for smg_set_source_expr, in x, y, z, t and,
+ * for sigma_sm, the order m.  rows: nrows triples (sigma_t field, its decay
+ * field, order m); sA_field / EA_field: sigma_a on grid 111 and its decay
+ * field; all array fields.  coords: 6 vectors, per solver dimension the
+ * coordinates of grid type 1 then 2.  expr_a = NULL returns to uploaded
+ * values.  The reference evaluates Matlab hooks on the host instead. */
+int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0, const char* expr_sm, int32_t nrows,
+                          const int32_t* rows, int32_t sA_field, int32_t EA_field, const double* const* coords);
+
 /* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
  * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
  * handle's stream; steps that move under 1 GB are replayed from captured

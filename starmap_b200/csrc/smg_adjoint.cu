@@ -807,8 +807,9 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     if (h->filter_mode == SMG_FILTER_FULL)
         return afail(h, SMG_EINVAL, "smg_forward: the adjoint supports f_position '' and 'substep'");
     if (!(h->pair[0].ok && h->pair[1].ok)) return afail(h, SMG_EINVAL, "smg_forward: pair tables unavailable");
-    if (!h->src_expr.empty())
-        return afail(h, SMG_EINVAL, "smg_forward: the adjoint covers autonomous problems (no device-evaluated sources)");
+    if (!h->src_expr.empty() || h->mat.on)
+        return afail(h, SMG_EINVAL,
+                     "smg_forward: the adjoint covers autonomous problems (no device-evaluated sources or materials)");
     const size_t sb = state_bytes(h);
     const int maxdest = (int)std::max(h->destA.size(), h->destB.size());
     const size_t vb = (size_t)h->g.cs * std::max(maxdest, 1) * sizeof(double);

@@ -917,6 +917,56 @@ int smg_set_time(smg_handle* h, double t) {
     if (!h) return fail(h, SMG_EINVAL, "smg_set_time: NULL handle");
     if (!std::isfinite(t)) return fail(h, SMG_EINVAL, "smg_set_time: t must be finite");
     h->t = t;
+    h->mat.init = false;   // materials re-evaluated at t before the next step
+    return SMG_OK;
+}
+
+int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0, const char* expr_sm, int32_t nrows,
+                          const int32_t* rows, int32_t sA_field, int32_t EA_field, const double* const* coords) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL handle");
+    smg::src_free(h, false);
+    cudaFree(h->mat.dC);
+    cudaFree(h->mat.dOld);
+    h->mat = smg_handle::MatExpr{};
+    if (!expr_a) return SMG_OK;   // back to uploaded values
+    if (!expr_s0 || nrows < 0 || (nrows > 0 && !rows) || !coords)
+        return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL argument");
+    for (const char* e : {expr_a, expr_s0, expr_sm})
+        if (e && (std::strlen(e) == 0 || std::strlen(e) > 65536))
+            return fail(h, SMG_EINVAL, "smg_set_material_expr: expression empty or over 64 KB");
+    auto array_field = [&](int f) { return f >= 0 && f < (int)h->fields_host.size() && h->fields_host[f].p; };
+    auto& M = h->mat;
+    for (int r = 0; r < nrows; ++r) {
+        if (!array_field(rows[3 * r]) || !array_field(rows[3 * r + 1]))
+            return fail(h, SMG_EINVAL, "smg_set_material_expr: sigma_t and decay fields must be array fields");
+        M.sT.push_back(rows[3 * r]);
+        M.ET.push_back(rows[3 * r + 1]);
+        M.m.push_back(rows[3 * r + 2]);
+    }
+    if (!array_field(sA_field) || !array_field(EA_field))
+        return fail(h, SMG_EINVAL, "smg_set_material_expr: sigma_a and its decay field must be array fields");
+    M.sA = sA_field;
+    M.EA = EA_field;
+    M.a = expr_a;
+    M.s0 = expr_s0;
+    M.sm = expr_sm ? expr_sm : "";
+    // coordinates: solver dimension d, grid type 1 then 2
+    std::vector<double> c;
+    for (int d = 0; d < 3; ++d) {
+        int a = 0;
+        while (h->sd[a] != d) ++a;
+        for (int gt = 1; gt <= 2; ++gt) {
+            if (!coords[2 * d + gt - 1]) return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL coordinate vector");
+            const int len = (gt == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+            M.off[d][gt - 1] = (int)c.size();
+            c.insert(c.end(), coords[2 * d + gt - 1], coords[2 * d + gt - 1] + len);
+        }
+    }
+    SMG_CUDA(h, cudaMalloc(&M.dC, c.size() * sizeof(double)));
+    SMG_CUDA(h, cudaMemcpy(M.dC, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice));
+    SMG_CUDA(h, cudaMalloc(&M.dOld, (size_t)(nrows + 1) * h->g.cs * sizeof(double)));
+    M.on = true;
+    M.init = false;
     return SMG_OK;
 }
 
@@ -1093,19 +1143,25 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
     }
     int64_t left = nsteps;
     int64_t launches = 0, rem = 0;
-    if (!h->src_expr.empty()) {
-        // sources evaluated on the device: before every step Q at the step's
-        // t - dt/2 (starmap_solver.m:276-282), then one unfused step (the
-        // two phase-A passes around a step boundary see different sources);
-        // the time advances as the host loop does, t = t + dt
-        if (!h->src_expr[0].fn) {
+    if (!h->src_expr.empty() || h->mat.on) {
+        // sources and materials evaluated on the device: before every step
+        // the materials at t + dt averaged with those at t (and their decay
+        // factors), Q at t + dt/2 (starmap_solver.m:214-282), then one
+        // unfused step (the two phase-A passes around a step boundary see
+        // different coefficients); the time advances as the host loop does
+        if ((!h->src_expr.empty() && !h->src_expr[0].fn) || (h->mat.on && h->mat.fn.empty())) {
             std::string why;
             const int rc = smg::src_build(h, why);
-            if (rc != SMG_OK) return fail(h, rc, "source expressions: " + why);
+            if (rc != SMG_OK) return fail(h, rc, "source and material expressions: " + why);
         }
+        if (h->mat.on && !h->mat.init) SMG_CUDA(h, smg::launch_mat(h, h->t, h->dt, true, h->stream));
         if (events) SMG_CUDA(h, cudaEventRecord(h->ev0, h->stream));
         for (int64_t k = 0; k < nsteps; ++k) {
             const double t_end = h->t + h->dt;
+            if (h->mat.on) {
+                SMG_CUDA(h, smg::launch_mat(h, t_end, h->dt, false, h->stream));
+                launches += (int64_t)h->mat.sT.size() + 1;
+            }
             SMG_CUDA(h, smg::launch_src(h, t_end - h->dt / 2, h->stream));
             SMG_CUDA(h, enqueue_steps(h, 1, h->stream, &rem));
             launches += rem + (int64_t)h->src_expr.size();

@@ -1699,7 +1699,66 @@ void src_free(smg_handle* h, bool coords) {
             e.dC = nullptr;
         }
     }
+    h->mat.fn.clear();
+    if (coords) {
+        cudaFree(h->mat.dC);
+        cudaFree(h->mat.dOld);
+        h->mat.dC = h->mat.dOld = nullptr;
+        h->mat.on = false;
+        h->mat.init = false;
+    }
 }
+
+namespace {
+// Per sigma_t row r of the handle's material expressions (and r = rows for
+// sigma_a on grid 111): the new values at t, the average with the previous
+// ones into the field, its decay factor expm1div(-s*dt/2) and the new values
+// kept for the next step (starmap_solver.m:214-252, 267-274); with init only
+// the values at t are stored.
+void emit_mat_kernel(std::string& o, const smg_handle* h, int r) {
+    const auto& M = h->mat;
+    const bool is_a = r == (int)M.sT.size();
+    const int f = is_a ? M.sA : M.sT[r];
+    const int fg = h->field_grid[f];
+    const int gs[3] = {1 + (fg & 1), 1 + ((fg >> 1) & 1), 1 + ((fg >> 2) & 1)};   // solver dimensions
+    int E[3], axis_of[3];
+    for (int a = 0; a < 3; ++a) {
+        const int d = h->sd[a];
+        E[a] = (gs[d] == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+        axis_of[d] = a;
+    }
+    char b[2048];
+    std::snprintf(b, sizeof b,
+                  "extern \"C\" __global__ void smg_mat_%d(double* __restrict__ S1, double* __restrict__ D, "
+                  "double* __restrict__ old, const double* __restrict__ C, double t, double dt, int init) {\n"
+                  "    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;\n"
+                  "    if (i0 >= %d) return;\n"
+                  "    for (int rr = blockIdx.y; rr < %d; rr += gridDim.y) {\n"
+                  "        const int i1 = rr %% %d, i2 = rr / %d;\n"
+                  "        const int ia[3] = {i0, i1, i2};\n"
+                  "        const double x = C[%d + ia[%d]], y = C[%d + ia[%d]], z = C[%d + ia[%d]];\n"
+                  "        const int m = %d;\n"
+                  "        (void)x; (void)y; (void)z; (void)m; (void)t;\n"
+                  "        const long long p = (long long)i2 * %lld + (long long)i1 * %lld + i0;\n",
+                  r, E[0], E[1] * E[2], E[1], E[1], M.off[0][gs[0] - 1], axis_of[0], M.off[1][gs[1] - 1], axis_of[1],
+                  M.off[2][gs[2] - 1], axis_of[2], is_a ? 0 : M.m[r], (long long)h->g.s2, (long long)h->g.s1);
+    o += b;
+    if (is_a) o += "        const double v = (double)(\n" + M.a + "\n        );\n";
+    else {
+        o += "        const double sa = (double)(\n" + M.a + "\n        );\n";
+        o += "        double ss = (double)(\n" + M.s0 + "\n        );\n";
+        if (!M.sm.empty()) o += "        ss = __dsub_rn(ss, (double)(\n" + M.sm + "\n        ));\n";
+        o += "        const double v = __dadd_rn(sa, ss);\n";
+    }
+    o += "        if (init) { old[p] = v; continue; }\n"
+         "        const double s1 = __dmul_rn(__dadd_rn(old[p], v), 0.5);\n"
+         "        const double xx = __dmul_rn(__dmul_rn(-s1, dt), 0.5);\n"
+         "        double e = __dadd_rn(__dadd_rn(1.0, __dmul_rn(xx, 0.5)), __ddiv_rn(__dmul_rn(xx, xx), 6.0));\n"
+         "        if (fabs(xx) > 2e-4) e = __ddiv_rn(__dsub_rn(exp(xx), 1.0), xx);\n"
+         "        S1[p] = s1; D[p] = e; old[p] = v;\n"
+         "    }\n}\n";
+}
+}  // namespace
 
 int src_build(smg_handle* h, std::string& err) {
     Api& a = api();
@@ -1732,15 +1791,27 @@ int src_build(smg_handle* h, std::string& err) {
         src += b;
         src += e.expr + "\n        );\n    }\n}\n";
     }
+    const int nmat = h->mat.on ? (int)h->mat.sT.size() + 1 : 0;
+    for (int r = 0; r < nmat; ++r) emit_mat_kernel(src, h, r);
     std::vector<char> cubin;
     int rc = compile_one(src, 0, false, cubin, err);
     if (rc != SMG_OK) return rc;
     CUmodule_t m = nullptr;
     if (a.ModuleLoadData(&m, cubin.data()) != 0) {
-        err = "cuModuleLoadData failed (source expressions)";
+        err = "cuModuleLoadData failed (source and material expressions)";
         return SMG_ECUDA;
     }
     h->src_mod = m;
+    for (int r = 0; r < nmat; ++r) {
+        CUfunction_t f = nullptr;
+        const std::string name = "smg_mat_" + std::to_string(r);
+        if (a.ModuleGetFunction(&f, m, name.c_str()) != 0) {
+            err = "cuModuleGetFunction " + name;
+            src_free(h, false);
+            return SMG_ECUDA;
+        }
+        h->mat.fn.push_back(f);
+    }
     for (size_t i = 0; i < h->src_expr.size(); ++i) {
         CUfunction_t f = nullptr;
         const std::string name = "smg_src_" + std::to_string(i);
@@ -1752,6 +1823,32 @@ int src_build(smg_handle* h, std::string& err) {
         h->src_expr[i].fn = f;
     }
     return SMG_OK;
+}
+
+cudaError_t launch_mat(smg_handle* h, double t, double dt, bool init, cudaStream_t s) {
+    auto& M = h->mat;
+    const int rows = (int)M.sT.size();
+    for (int r = 0; r <= rows; ++r) {
+        const int f = r == rows ? M.sA : M.sT[r], fd = r == rows ? M.EA : M.ET[r];
+        const int fg = h->field_grid[f];
+        int E[3];
+        for (int a = 0; a < 3; ++a) {
+            const int gd = 1 + ((fg >> h->sd[a]) & 1);
+            E[a] = (gd == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+        }
+        double* S1 = const_cast<double*>(h->fields_host[f].p);
+        double* D = const_cast<double*>(h->fields_host[fd].p);
+        double* old = M.dOld + (size_t)r * h->g.cs;
+        const double* C = M.dC;
+        double tt = t, dd = dt;
+        int in = init ? 1 : 0;
+        void* args[] = {&S1, &D, &old, &C, &tt, &dd, &in};
+        const unsigned gx = (unsigned)((E[0] + 127) / 128), gy = (unsigned)std::min(E[1] * E[2], 4096);
+        if (api().LaunchKernel(static_cast<CUfunction_t>(M.fn[r]), gx, gy, 1, 128, 1, 1, 0, s, args, nullptr) != 0)
+            return cudaErrorLaunchFailure;
+    }
+    if (init) M.init = true;
+    return cudaSuccess;
 }
 
 cudaError_t launch_src(const smg_handle* h, double t, cudaStream_t s) {

@@ -149,6 +149,22 @@ class GpuSolver:
         are evaluated on the device)."""
         check(self._L.smg_set_time(self.h, float(t)), self.h)
 
+    def set_material_expr(self, expr_a, expr_s0, expr_sm, rows, sA_field, EA_field, coords):
+        """Evaluate the materials on the device every step
+        (``smg_set_material_expr``): ``rows`` (sigma_t field, decay field,
+        order m) per (grid type, order); ``coords`` six vectors, per solver
+        dimension the coordinates of grid types 1 and 2.  ``expr_a=None``
+        returns to uploaded values."""
+        if expr_a is None:
+            check(self._L.smg_set_material_expr(self.h, None, None, None, 0, None, -1, -1, None), self.h)
+            return
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1))
+        cs = [np.ascontiguousarray(np.asarray(c, dtype=np.float64).ravel()) for c in coords]
+        ptrs = (_lib.C.POINTER(_lib.C.c_double) * 6)(*[dptr(c) for c in cs])
+        check(self._L.smg_set_material_expr(self.h, expr_a.encode(), expr_s0.encode(),
+                                            expr_sm.encode() if expr_sm else None, len(r) // 3, iptr(r),
+                                            int(sA_field), int(EA_field), ptrs), self.h)
+
     def set_source_expr(self, j, expr, coords=None):
         """Evaluate the source of component j on the device every step
         (``smg_set_source_expr``): ``expr`` is a C++ expression in the solver
@@ -620,11 +636,24 @@ def starmap_solver(par: dict):
     sA, sT, sA1, sT1, dt = fs["sA"], fs["sT"], fs["sA1"], fs["sT1"], fs["dt"]
     cpu_setup = time.perf_counter() - t_start
 
-    solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], fs["F"])
-    t_gpu0 = time.perf_counter()
     # a time-dependent source given also as an expression is evaluated on the
-    # device every step instead of on the host
+    # device every step instead of on the host; so are time-dependent
+    # materials when every material hook has an expression (hyperbolic dt,
+    # filters not time-dependent)
     dev_src = bool(S.src_td) and bool(par.get("source_expr"))
+    dev_mat = (td_any and S.timestep == 0 and not S.filter_td and (dev_src or not S.src_td)
+               and bool(par.get("sigma_a_expr")) and bool(par.get("sigma_s0_expr"))
+               and (bool(par.get("sigma_sm_expr")) or not S.flag_ani))
+    if dev_mat:
+        # the material fields become arrays, written by the device every step
+        shape = lambda g: S.XYZ(g)[0].shape
+        full = lambda v, g: np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), shape(g)))
+        solver, T = _build(S, full(sA1, (1, 1, 1)), {k: full(v, k[:3]) for k, v in sT1.items()},
+                           full(fs["EA"], (1, 1, 1)), {k: full(v, k[:3]) for k, v in fs["ET"].items()},
+                           fs["Q"], fs["F"])
+    else:
+        solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], fs["F"])
+    t_gpu0 = time.perf_counter()
     try:
         solver.set_state(S.U0)
         solver.set_dt(dt)
@@ -634,9 +663,26 @@ def starmap_solver(par: dict):
                 g = S.G(j1 - 1)
                 solver.set_source_expr(j1 - 1, expr, [S.xs[g[0] - 1], S.ys[g[1] - 1], S.zs[g[2] - 1]])
             solver.set_time(0.0)
+        if dev_mat:
+            dim = int(par.get("dim", 3))
+            ex = lambda key: device_source_expr(par[key], dim) if par.get(key) else None
+            rows = [(T.index[("sT",) + row], T.index[("ET",) + row], row[3]) for row in S.sg]
+            solver.set_material_expr(ex("sigma_a_expr"), ex("sigma_s0_expr"),
+                                     ex("sigma_sm_expr") if S.flag_ani else None, rows, T.index[("sA",)],
+                                     T.index[("EA",)], [S.xs[0], S.xs[1], S.ys[0], S.ys[1], S.zs[0], S.zs[1]])
+            solver.set_time(0.0)
+            # dt of every step as the reference chooses it for time-dependent
+            # materials: min(dt_hyp, time left / cn) * cn, the last step shortened
+            sched_t, sched_dt = [], []
+            tt = 0.0
+            while tt < tfinal:
+                d = min(S.dt_hyp, (tfinal - tt) / cn) * cn
+                tt = tt + d
+                sched_t.append(tt)
+                sched_dt.append(d)
         t_plot = list(np.atleast_1d(np.asarray(par.get("t_plot", [])))) + [np.inf]
         want_plot = par.get("output", _noop_output) is not _noop_output
-        per_step = td_any or (S.src_td and not dev_src) or S.filter_td
+        per_step = (td_any and not dev_mat) or (S.src_td and not dev_src) or S.filter_td
         step_count = 0
         t_cur = 0.0
         plot_count = 0
@@ -664,14 +710,23 @@ def starmap_solver(par: dict):
             # how many steps can run before the next plot time
             if per_step:
                 nrun = 1
+            elif dev_mat:
+                ts, dts = sched_t[step_count:], sched_dt[step_count:]
+                if dts[0] != dt:
+                    dt = dts[0]
+                    solver.set_dt(dt)
+                nrun = 1
+                while nrun < len(dts) and dts[nrun] == dts[0]:
+                    nrun += 1
+                ts = ts[:nrun]
             else:
                 ts = step_times(dt, tfinal)[step_count:]
                 nrun = len(ts)
-                if want_plot:
-                    for k, tk in enumerate(ts):
-                        if tk >= t_plot[plot_count] - 1e-14:
-                            nrun = k + 1
-                            break
+            if not per_step and want_plot:
+                for k, tk in enumerate(ts):
+                    if tk >= t_plot[plot_count] - 1e-14:
+                        nrun = k + 1
+                        break
             U0 = None
             if want_plot and nrun >= 1:
                 if nrun > 1:
