@@ -171,6 +171,17 @@ int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const dou
 int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0, const char* expr_sm, int32_t nrows,
                           const int32_t* rows, int32_t sA_field, int32_t EA_field, const double* const* coords);
 
+/* Time-dependent filter evaluated on the device: before every step of
+ * smg_run the library writes, per row, the filter at t - dt/2 into field
+ * rows[3r] and at t into rows[3r+1] ('substep'; rows[3r+1] = -1 for 'full':
+ * at t into rows[3r]), for the row's order k = rows[3r+2]
+ * (starmap_solver.m:283-305).  expr in x, y, z, t, dt and k, as for
+ * smg_set_source_expr; coords as for smg_set_material_expr.  expr = NULL
+ * returns to uploaded values.  The reference evaluates a Matlab hook on the
+ * host instead. */
+int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const int32_t* rows,
+                        const double* const* coords);
+
 /* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
  * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
  * handle's stream; steps that move under 1 GB are replayed from captured

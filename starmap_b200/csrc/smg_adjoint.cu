@@ -807,7 +807,7 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     if (h->filter_mode == SMG_FILTER_FULL)
         return afail(h, SMG_EINVAL, "smg_forward: the adjoint supports f_position '' and 'substep'");
     if (!(h->pair[0].ok && h->pair[1].ok)) return afail(h, SMG_EINVAL, "smg_forward: pair tables unavailable");
-    if (!h->src_expr.empty() || h->mat.on)
+    if (!h->src_expr.empty() || h->mat.on || !h->filt.f1.empty())
         return afail(h, SMG_EINVAL,
                      "smg_forward: the adjoint covers autonomous problems (no device-evaluated sources or materials)");
     const size_t sb = state_bytes(h);

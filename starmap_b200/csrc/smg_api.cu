@@ -921,11 +921,40 @@ int smg_set_time(smg_handle* h, double t) {
     return SMG_OK;
 }
 
+// The coordinate table of the material and filter expressions: per solver
+// dimension d the coordinates of grid types 1 and 2 (coords[2d], coords[2d+1]).
+static int set_coords(smg_handle* h, const double* const* coords, const char* who) {
+    std::vector<double> c;
+    smg_handle::Coords X;
+    for (int d = 0; d < 3; ++d) {
+        int a = 0;
+        while (h->sd[a] != d) ++a;
+        for (int gt = 1; gt <= 2; ++gt) {
+            if (!coords[2 * d + gt - 1]) return fail(h, SMG_EINVAL, std::string(who) + ": NULL coordinate vector");
+            const int len = (gt == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+            X.off[d][gt - 1] = (int)c.size();
+            c.insert(c.end(), coords[2 * d + gt - 1], coords[2 * d + gt - 1] + len);
+        }
+    }
+    SMG_CUDA(h, cudaMalloc(&X.dC, c.size() * sizeof(double)));
+    const cudaError_t e = cudaMemcpy(X.dC, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(X.dC);
+        return cuda_fail(h, e, (std::string(who) + ": coordinates").c_str());
+    }
+    cudaFree(h->xyz.dC);
+    h->xyz = X;
+    return SMG_OK;
+}
+
+static bool array_field(const smg_handle* h, int f) {
+    return f >= 0 && f < (int)h->fields_host.size() && h->fields_host[f].p;
+}
+
 int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0, const char* expr_sm, int32_t nrows,
                           const int32_t* rows, int32_t sA_field, int32_t EA_field, const double* const* coords) {
     if (!h) return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL handle");
     smg::src_free(h, false);
-    cudaFree(h->mat.dC);
     cudaFree(h->mat.dOld);
     h->mat = smg_handle::MatExpr{};
     if (!expr_a) return SMG_OK;   // back to uploaded values
@@ -934,39 +963,54 @@ int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0
     for (const char* e : {expr_a, expr_s0, expr_sm})
         if (e && (std::strlen(e) == 0 || std::strlen(e) > 65536))
             return fail(h, SMG_EINVAL, "smg_set_material_expr: expression empty or over 64 KB");
-    auto array_field = [&](int f) { return f >= 0 && f < (int)h->fields_host.size() && h->fields_host[f].p; };
-    auto& M = h->mat;
+    smg_handle::MatExpr M;
     for (int r = 0; r < nrows; ++r) {
-        if (!array_field(rows[3 * r]) || !array_field(rows[3 * r + 1]))
+        if (!array_field(h, rows[3 * r]) || !array_field(h, rows[3 * r + 1]))
             return fail(h, SMG_EINVAL, "smg_set_material_expr: sigma_t and decay fields must be array fields");
         M.sT.push_back(rows[3 * r]);
         M.ET.push_back(rows[3 * r + 1]);
         M.m.push_back(rows[3 * r + 2]);
     }
-    if (!array_field(sA_field) || !array_field(EA_field))
+    if (!array_field(h, sA_field) || !array_field(h, EA_field))
         return fail(h, SMG_EINVAL, "smg_set_material_expr: sigma_a and its decay field must be array fields");
     M.sA = sA_field;
     M.EA = EA_field;
     M.a = expr_a;
     M.s0 = expr_s0;
     M.sm = expr_sm ? expr_sm : "";
-    // coordinates: solver dimension d, grid type 1 then 2
-    std::vector<double> c;
-    for (int d = 0; d < 3; ++d) {
-        int a = 0;
-        while (h->sd[a] != d) ++a;
-        for (int gt = 1; gt <= 2; ++gt) {
-            if (!coords[2 * d + gt - 1]) return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL coordinate vector");
-            const int len = (gt == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
-            M.off[d][gt - 1] = (int)c.size();
-            c.insert(c.end(), coords[2 * d + gt - 1], coords[2 * d + gt - 1] + len);
-        }
-    }
-    SMG_CUDA(h, cudaMalloc(&M.dC, c.size() * sizeof(double)));
-    SMG_CUDA(h, cudaMemcpy(M.dC, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice));
+    const int rc = set_coords(h, coords, "smg_set_material_expr");
+    if (rc != SMG_OK) return rc;
     SMG_CUDA(h, cudaMalloc(&M.dOld, (size_t)(nrows + 1) * h->g.cs * sizeof(double)));
     M.on = true;
     M.init = false;
+    h->mat = M;
+    return SMG_OK;
+}
+
+int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const int32_t* rows,
+                        const double* const* coords) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_set_filter_expr: NULL handle");
+    smg::src_free(h, false);
+    h->filt = smg_handle::FiltExpr{};
+    if (!expr) return SMG_OK;   // back to uploaded values
+    if (nrows < 1 || !rows || !coords) return fail(h, SMG_EINVAL, "smg_set_filter_expr: NULL argument or no rows");
+    if (std::strlen(expr) == 0 || std::strlen(expr) > 65536)
+        return fail(h, SMG_EINVAL, "smg_set_filter_expr: expression empty or over 64 KB");
+    smg_handle::FiltExpr F;
+    F.expr = expr;
+    for (int r = 0; r < nrows; ++r) {
+        const int f1 = rows[3 * r], f2 = rows[3 * r + 1];
+        if (!array_field(h, f1) || (f2 >= 0 && !array_field(h, f2)))
+            return fail(h, SMG_EINVAL, "smg_set_filter_expr: filter fields must be array fields");
+        if (f2 >= 0 && h->field_grid[f2] != h->field_grid[f1])
+            return fail(h, SMG_EINVAL, "smg_set_filter_expr: a row's two fields must share a grid");
+        F.f1.push_back(f1);
+        F.f2.push_back(f2);
+        F.k.push_back(rows[3 * r + 2]);
+    }
+    const int rc = set_coords(h, coords, "smg_set_filter_expr");
+    if (rc != SMG_OK) return rc;
+    h->filt = F;
     return SMG_OK;
 }
 
@@ -1143,13 +1187,14 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
     }
     int64_t left = nsteps;
     int64_t launches = 0, rem = 0;
-    if (!h->src_expr.empty() || h->mat.on) {
+    if (!h->src_expr.empty() || h->mat.on || !h->filt.f1.empty()) {
         // sources and materials evaluated on the device: before every step
         // the materials at t + dt averaged with those at t (and their decay
         // factors), Q at t + dt/2 (starmap_solver.m:214-282), then one
         // unfused step (the two phase-A passes around a step boundary see
         // different coefficients); the time advances as the host loop does
-        if ((!h->src_expr.empty() && !h->src_expr[0].fn) || (h->mat.on && h->mat.fn.empty())) {
+        if ((!h->src_expr.empty() && !h->src_expr[0].fn) || (h->mat.on && h->mat.fn.empty()) ||
+            (!h->filt.f1.empty() && h->filt.fn.empty())) {
             std::string why;
             const int rc = smg::src_build(h, why);
             if (rc != SMG_OK) return fail(h, rc, "source and material expressions: " + why);
@@ -1163,6 +1208,8 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
                 launches += (int64_t)h->mat.sT.size() + 1;
             }
             SMG_CUDA(h, smg::launch_src(h, t_end - h->dt / 2, h->stream));
+            SMG_CUDA(h, smg::launch_filt(h, t_end, h->dt, h->stream));
+            launches += (int64_t)h->filt.f1.size();
             SMG_CUDA(h, enqueue_steps(h, 1, h->stream, &rem));
             launches += rem + (int64_t)h->src_expr.size();
             h->t = t_end;

@@ -78,19 +78,29 @@ struct smg_handle {
         void* fn = nullptr;              // CUfunction once built
     };
     std::vector<SrcExpr> src_expr;
+    // grid coordinates of the material and filter expressions: per solver
+    // dimension, grid types 1 and 2 (offsets into dC)
+    struct Coords {
+        double* dC = nullptr;
+        int off[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    } xyz;
     // materials evaluated on the device every step (smg_set_material_expr)
     struct MatExpr {
         bool on = false;
         std::string a, s0, sm;           // sigma_a, sigma_s0, sigma_sm (sm empty: isotropic)
         std::vector<int> sT, ET, m;      // per sigma_t field: its decay field and moment order
         int sA = -1, EA = -1;
-        double* dC = nullptr;            // coordinates: per solver dimension, grid types 1 and 2
-        int off[3][2] = {{0, 0}, {0, 0}, {0, 0}};
         double* dOld = nullptr;          // the values at the previous time (sT rows, then sigma_a)
         std::vector<void*> fn;           // CUfunction per sigma_t row, then sigma_a
         bool init = false;               // dOld holds the values at h->t
     } mat;
-    void* src_mod = nullptr;             // CUmodule of the source and material kernels
+    // filters evaluated on the device every step (smg_set_filter_expr)
+    struct FiltExpr {
+        std::string expr;                // in x, y, z, t, dt and the order k
+        std::vector<int> f1, f2, k;      // per row: fields at t - dt/2 and t (substep; f2 = -1 for 'full')
+        std::vector<void*> fn;
+    } filt;
+    void* src_mod = nullptr;             // CUmodule of the source, material and filter kernels
     double t = 0.0;                      // time of the current state (smg_set_time)
     // strip-kernel schedules (phase 0 = A, 1 = B); empty if not usable
     struct HostSched {
@@ -178,6 +188,7 @@ int src_build(smg_handle* h, std::string& err);       // compile the smg_set_sou
 void src_free(smg_handle* h, bool coords);            // unload them (and free their coordinates)
 cudaError_t launch_src(const smg_handle* h, double t, cudaStream_t s);
 cudaError_t launch_mat(smg_handle* h, double t, double dt, bool init, cudaStream_t s);
+cudaError_t launch_filt(const smg_handle* h, double t, double dt, cudaStream_t s);
 int create_host(const smg_problem* p, smg_handle** out);   // host tables only (no CUDA call)
 cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long len, double* partial, double* out,
                          cudaStream_t s);

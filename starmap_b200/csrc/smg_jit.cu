@@ -1700,12 +1700,15 @@ void src_free(smg_handle* h, bool coords) {
         }
     }
     h->mat.fn.clear();
+    h->filt.fn.clear();
     if (coords) {
-        cudaFree(h->mat.dC);
+        cudaFree(h->xyz.dC);
         cudaFree(h->mat.dOld);
-        h->mat.dC = h->mat.dOld = nullptr;
+        h->xyz.dC = nullptr;
+        h->mat.dOld = nullptr;
         h->mat.on = false;
         h->mat.init = false;
+        h->filt = smg_handle::FiltExpr{};
     }
 }
 
@@ -1740,8 +1743,8 @@ void emit_mat_kernel(std::string& o, const smg_handle* h, int r) {
                   "        const int m = %d;\n"
                   "        (void)x; (void)y; (void)z; (void)m; (void)t;\n"
                   "        const long long p = (long long)i2 * %lld + (long long)i1 * %lld + i0;\n",
-                  r, E[0], E[1] * E[2], E[1], E[1], M.off[0][gs[0] - 1], axis_of[0], M.off[1][gs[1] - 1], axis_of[1],
-                  M.off[2][gs[2] - 1], axis_of[2], is_a ? 0 : M.m[r], (long long)h->g.s2, (long long)h->g.s1);
+                  r, E[0], E[1] * E[2], E[1], E[1], h->xyz.off[0][gs[0] - 1], axis_of[0], h->xyz.off[1][gs[1] - 1], axis_of[1],
+                  h->xyz.off[2][gs[2] - 1], axis_of[2], is_a ? 0 : M.m[r], (long long)h->g.s2, (long long)h->g.s1);
     o += b;
     if (is_a) o += "        const double v = (double)(\n" + M.a + "\n        );\n";
     else {
@@ -1757,6 +1760,45 @@ void emit_mat_kernel(std::string& o, const smg_handle* h, int r) {
          "        if (fabs(xx) > 2e-4) e = __ddiv_rn(__dsub_rn(exp(xx), 1.0), xx);\n"
          "        S1[p] = s1; D[p] = e; old[p] = v;\n"
          "    }\n}\n";
+}
+
+// Filter row r (smg_set_filter_expr): the filter of the row's (grid type,
+// order k) at t - dt/2 into field f1 and at t into f2 ('substep'), or at t
+// into f1 ('full') (starmap_solver.m:283-305).  The coordinates are the
+// material expressions' table.
+void emit_filt_kernel(std::string& o, const smg_handle* h, int r) {
+    const auto& Fl = h->filt;
+    const int fg = h->field_grid[Fl.f1[r]];
+    const int gs[3] = {1 + (fg & 1), 1 + ((fg >> 1) & 1), 1 + ((fg >> 2) & 1)};
+    int E[3], axis_of[3];
+    for (int a = 0; a < 3; ++a) {
+        const int d = h->sd[a];
+        E[a] = (gs[d] == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+        axis_of[d] = a;
+    }
+    const bool two = Fl.f2[r] >= 0;
+    char b[2048];
+    std::snprintf(b, sizeof b,
+                  "extern \"C\" __global__ void smg_filt_%d(double* __restrict__ F1, double* __restrict__ F2, "
+                  "const double* __restrict__ C, double tq, double dt) {\n"
+                  "    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;\n"
+                  "    if (i0 >= %d) return;\n"
+                  "    for (int rr = blockIdx.y; rr < %d; rr += gridDim.y) {\n"
+                  "        const int i1 = rr %% %d, i2 = rr / %d;\n"
+                  "        const int ia[3] = {i0, i1, i2};\n"
+                  "        const double x = C[%d + ia[%d]], y = C[%d + ia[%d]], z = C[%d + ia[%d]];\n"
+                  "        const int k = %d;\n"
+                  "        (void)x; (void)y; (void)z; (void)k;\n"
+                  "        const long long p = (long long)i2 * %lld + (long long)i1 * %lld + i0;\n",
+                  r, E[0], E[1] * E[2], E[1], E[1], h->xyz.off[0][gs[0] - 1], axis_of[0], h->xyz.off[1][gs[1] - 1], axis_of[1],
+                  h->xyz.off[2][gs[2] - 1], axis_of[2], Fl.k[r], (long long)h->g.s2, (long long)h->g.s1);
+    o += b;
+    if (two)
+        o += "        { const double t = tq - dt / 2; F1[p] = (double)(\n" + Fl.expr + "\n        ); }\n"
+             "        { const double t = tq; F2[p] = (double)(\n" + Fl.expr + "\n        ); }\n";
+    else
+        o += "        { const double t = tq; F1[p] = (double)(\n" + Fl.expr + "\n        ); }\n";
+    o += "        (void)F2;\n    }\n}\n";
 }
 }  // namespace
 
@@ -1793,6 +1835,8 @@ int src_build(smg_handle* h, std::string& err) {
     }
     const int nmat = h->mat.on ? (int)h->mat.sT.size() + 1 : 0;
     for (int r = 0; r < nmat; ++r) emit_mat_kernel(src, h, r);
+    const int nfilt = (int)h->filt.f1.size();
+    for (int r = 0; r < nfilt; ++r) emit_filt_kernel(src, h, r);
     std::vector<char> cubin;
     int rc = compile_one(src, 0, false, cubin, err);
     if (rc != SMG_OK) return rc;
@@ -1811,6 +1855,16 @@ int src_build(smg_handle* h, std::string& err) {
             return SMG_ECUDA;
         }
         h->mat.fn.push_back(f);
+    }
+    for (int r = 0; r < nfilt; ++r) {
+        CUfunction_t f = nullptr;
+        const std::string name = "smg_filt_" + std::to_string(r);
+        if (a.ModuleGetFunction(&f, m, name.c_str()) != 0) {
+            err = "cuModuleGetFunction " + name;
+            src_free(h, false);
+            return SMG_ECUDA;
+        }
+        h->filt.fn.push_back(f);
     }
     for (size_t i = 0; i < h->src_expr.size(); ++i) {
         CUfunction_t f = nullptr;
@@ -1839,7 +1893,7 @@ cudaError_t launch_mat(smg_handle* h, double t, double dt, bool init, cudaStream
         double* S1 = const_cast<double*>(h->fields_host[f].p);
         double* D = const_cast<double*>(h->fields_host[fd].p);
         double* old = M.dOld + (size_t)r * h->g.cs;
-        const double* C = M.dC;
+        const double* C = h->xyz.dC;
         double tt = t, dd = dt;
         int in = init ? 1 : 0;
         void* args[] = {&S1, &D, &old, &C, &tt, &dd, &in};
@@ -1848,6 +1902,27 @@ cudaError_t launch_mat(smg_handle* h, double t, double dt, bool init, cudaStream
             return cudaErrorLaunchFailure;
     }
     if (init) M.init = true;
+    return cudaSuccess;
+}
+
+cudaError_t launch_filt(const smg_handle* h, double t, double dt, cudaStream_t s) {
+    const auto& Fl = h->filt;
+    for (size_t r = 0; r < Fl.f1.size(); ++r) {
+        const int fg = h->field_grid[Fl.f1[r]];
+        int E[3];
+        for (int a = 0; a < 3; ++a) {
+            const int gd = 1 + ((fg >> h->sd[a]) & 1);
+            E[a] = (gd == 2 && h->g.bc[a] == 1) ? h->g.n[a] + 1 : h->g.n[a];
+        }
+        double* F1 = const_cast<double*>(h->fields_host[Fl.f1[r]].p);
+        double* F2 = Fl.f2[r] >= 0 ? const_cast<double*>(h->fields_host[Fl.f2[r]].p) : F1;
+        const double* C = h->xyz.dC;
+        double tt = t, dd = dt;
+        void* args[] = {&F1, &F2, &C, &tt, &dd};
+        const unsigned gx = (unsigned)((E[0] + 127) / 128), gy = (unsigned)std::min(E[1] * E[2], 4096);
+        if (api().LaunchKernel(static_cast<CUfunction_t>(Fl.fn[r]), gx, gy, 1, 128, 1, 1, 0, s, args, nullptr) != 0)
+            return cudaErrorLaunchFailure;
+    }
     return cudaSuccess;
 }
 

@@ -165,6 +165,19 @@ class GpuSolver:
                                             expr_sm.encode() if expr_sm else None, len(r) // 3, iptr(r),
                                             int(sA_field), int(EA_field), ptrs), self.h)
 
+    def set_filter_expr(self, expr, rows, coords):
+        """Evaluate the filter on the device every step (``smg_set_filter_expr``):
+        ``rows`` (field at t - dt/2, field at t or -1, order k) per (grid type,
+        order); ``coords`` as for :meth:`set_material_expr`.  ``expr=None``
+        returns to uploaded values."""
+        if expr is None:
+            check(self._L.smg_set_filter_expr(self.h, None, 0, None, None), self.h)
+            return
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1))
+        cs = [np.ascontiguousarray(np.asarray(c, dtype=np.float64).ravel()) for c in coords]
+        ptrs = (_lib.C.POINTER(_lib.C.c_double) * 6)(*[dptr(c) for c in cs])
+        check(self._L.smg_set_filter_expr(self.h, expr.encode(), len(r) // 3, iptr(r), ptrs), self.h)
+
     def set_source_expr(self, j, expr, coords=None):
         """Evaluate the source of component j on the device every step
         (``smg_set_source_expr``): ``expr`` is a C++ expression in the solver
@@ -641,18 +654,20 @@ def starmap_solver(par: dict):
     # materials when every material hook has an expression (hyperbolic dt,
     # filters not time-dependent)
     dev_src = bool(S.src_td) and bool(par.get("source_expr"))
-    dev_mat = (td_any and S.timestep == 0 and not S.filter_td and (dev_src or not S.src_td)
+    dev_filt = bool(S.filter_td) and bool(par.get("filterfunction_expr"))
+    dev_mat = (td_any and S.timestep == 0 and (dev_filt or not S.filter_td) and (dev_src or not S.src_td)
                and bool(par.get("sigma_a_expr")) and bool(par.get("sigma_s0_expr"))
                and (bool(par.get("sigma_sm_expr")) or not S.flag_ani))
+    # fields written by the device every step become arrays
+    shape = lambda g: S.XYZ(g)[0].shape
+    full = lambda v, g: np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), shape(g)))
+    Fv = {k: full(v, k[:3]) for k, v in fs["F"].items()} if dev_filt else fs["F"]
     if dev_mat:
-        # the material fields become arrays, written by the device every step
-        shape = lambda g: S.XYZ(g)[0].shape
-        full = lambda v, g: np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), shape(g)))
         solver, T = _build(S, full(sA1, (1, 1, 1)), {k: full(v, k[:3]) for k, v in sT1.items()},
                            full(fs["EA"], (1, 1, 1)), {k: full(v, k[:3]) for k, v in fs["ET"].items()},
-                           fs["Q"], fs["F"])
+                           fs["Q"], Fv)
     else:
-        solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], fs["F"])
+        solver, T = _build(S, sA1, sT1, fs["EA"], fs["ET"], fs["Q"], Fv)
     t_gpu0 = time.perf_counter()
     try:
         solver.set_state(S.U0)
@@ -662,6 +677,15 @@ def starmap_solver(par: dict):
             for j1 in S.source_ind:
                 g = S.G(j1 - 1)
                 solver.set_source_expr(j1 - 1, expr, [S.xs[g[0] - 1], S.ys[g[1] - 1], S.zs[g[2] - 1]])
+            solver.set_time(0.0)
+        coords6 = [S.xs[0], S.xs[1], S.ys[0], S.ys[1], S.zs[0], S.zs[1]]
+        if dev_filt:
+            if S.f_position == "substep":
+                frows = [(T.index[("F",) + row + (1,)], T.index[("F",) + row + (2,)], row[3]) for row in S.f_sg]
+            else:
+                frows = [(T.index[("F",) + row], -1, row[3]) for row in S.f_sg]
+            solver.set_filter_expr(device_source_expr(par["filterfunction_expr"], int(par.get("dim", 3))),
+                                   frows, coords6)
             solver.set_time(0.0)
         if dev_mat:
             dim = int(par.get("dim", 3))
@@ -682,7 +706,7 @@ def starmap_solver(par: dict):
                 sched_dt.append(d)
         t_plot = list(np.atleast_1d(np.asarray(par.get("t_plot", [])))) + [np.inf]
         want_plot = par.get("output", _noop_output) is not _noop_output
-        per_step = (td_any and not dev_mat) or (S.src_td and not dev_src) or S.filter_td
+        per_step = (td_any and not dev_mat) or (S.src_td and not dev_src) or (S.filter_td and not dev_filt)
         step_count = 0
         t_cur = 0.0
         plot_count = 0
@@ -704,7 +728,7 @@ def starmap_solver(par: dict):
                 if S.src_td and not dev_src:
                     for j, q in _sources(S, tn, dt).items():
                         solver.set_field(T.index[("Q", j)], q)
-                if S.filter_td:
+                if S.filter_td and not dev_filt:
                     for key, val in _filters(S, dt, tn).items():
                         solver.set_field(T.index[("F",) + key], val)
             # how many steps can run before the next plot time

@@ -148,3 +148,23 @@ def test_material_expressions_fall_back_without_every_hook():
     prob.pop("sigma_s0_expr")
     par = starmap_init(prob)
     compare(starmap_solver(par), O.starmap_solver(par).output, 1e-12)
+
+
+@pytest.mark.parametrize("position", ["substep", "full"])
+def test_time_dependent_filter_on_the_device(position):
+    """A filter hook taking t (re-evaluated every step: at t - dt/2 and t for
+    'substep', at t for 'full'), on the device against the host hook."""
+    prob = boxes(lambda x, y, t: (2 + 0.5 * t * t) * MASK_PY(x, y), "(2 + 0.5 * t * t) * " + MASK_C, n_mom=4,
+                 filterfunction=lambda par, dt, k, x, y, t: np.exp(-(0.5 + t + 0.1 * x) * dt * (k / 4.0) * (k / 4.0)),
+                 filterfunction_expr="exp(-(0.5 + t + 0.1 * x) * dt * (k / 4.0) * (k / 4.0))", f_position=position)
+    par = starmap_init(prob)
+    compare(starmap_solver(par), O.starmap_solver(par).output, 1e-12)
+
+
+def test_everything_time_dependent_on_the_device():
+    prob = td_materials(n_mom=4, source=lambda x, y, t: (1 + t) * ((x < 0.2) & (y < 0.2)).astype(np.float64),
+                        source_expr="(1 + t) * (((x < 0.2) && (y < 0.2)) ? 1.0 : 0.0)",
+                        filterfunction=lambda par, dt, k, x, y, t: np.exp(-(1 + t) * dt * (k / 4.0) * (k / 4.0)),
+                        filterfunction_expr="exp(-(1 + t) * dt * (k / 4.0) * (k / 4.0))", f_position="substep")
+    par = starmap_init(prob)
+    compare(starmap_solver(par), O.starmap_solver(par).output, 1e-12)
