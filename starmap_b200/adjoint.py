@@ -29,7 +29,7 @@ import numpy as np
 from .batch import _tables
 from .solver import GpuSolver, first_step, handle_tables, prepare
 
-__all__ = ["MisfitAdjoint"]
+__all__ = ["MisfitAdjoint", "batched_gradients"]
 
 
 class MisfitAdjoint:
@@ -85,3 +85,30 @@ class MisfitAdjoint:
             self.close()
         except Exception:
             pass
+
+
+def batched_gradients(pars, obs, nsteps: int, ckpt_every: int = 20, threads: int = 8):
+    """Misfit gradients of many independent problems (e.g. an ensemble of
+    inverse problems) in one call: one :class:`MisfitAdjoint` per problem,
+    their forward and backward sweeps issued from ``threads`` host threads so
+    that the instances' kernels (each handle has its own CUDA stream) overlap
+    on the GPU.  ``obs[i]`` is problem i's observation.  Returns the list of
+    gradient dicts and the wall seconds of the forward and backward stages.
+    ``ckpt_every`` must be > 0: with 0 every instance would size its
+    recording to the whole free memory."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+    if ckpt_every < 1:
+        raise ValueError("batched gradients need an explicit checkpoint interval (ckpt_every >= 1)")
+    adjs = [MisfitAdjoint(p, ckpt_every=ckpt_every) for p in pars]
+    try:
+        with ThreadPoolExecutor(max_workers=max(1, int(threads))) as ex:
+            t0 = time.perf_counter()
+            list(ex.map(lambda ao: ao[0].forward(ao[1], nsteps), zip(adjs, obs)))
+            t1 = time.perf_counter()
+            grads = list(ex.map(lambda a: a.backward(), adjs))
+            t2 = time.perf_counter()
+        return grads, t1 - t0, t2 - t1
+    finally:
+        for a in adjs:
+            a.close()
