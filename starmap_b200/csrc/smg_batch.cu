@@ -433,6 +433,10 @@ int smg_batch_run(smg_batch* b, int64_t nsteps) {
     for (size_t i = 0; i < b->inst.size(); ++i) {
         if (!b->inst[i]->dt_set) return bfail(b, SMG_ESTATE, "smg_batch_run: dt not set");
         if (!b->inst[i]->state_set) return bfail(b, SMG_ESTATE, "smg_batch_run: state not set");
+        const smg_handle* h = b->inst[i];
+        if (!h->src_expr.empty() || h->mat.on || !h->filt.f1.empty())
+            return bfail(b, SMG_EINVAL,
+                         "smg_batch_run: device-evaluated sources, materials or filters are not supported in a batch");
         B_CUDA(b, cudaStreamSynchronize(b->inst[i]->stream));
     }
     B_CUDA(b, cudaMemsetAsync(b->d_bar, 0, sizeof(BarrierState), b->stream));

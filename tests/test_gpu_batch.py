@@ -130,3 +130,26 @@ def test_batch_autotune_restores_state():
                 np.testing.assert_array_equal(got[j], ref[j])
     finally:
         batch.close()
+
+
+def test_batch_refuses_device_expressions():
+    """A batch advances its instances with its own kernels, which do not
+    evaluate smg_set_source_expr expressions: such an instance is refused."""
+    from starmap_b200 import _lib
+    probs = configs.batched_sweep(n_inst=2, seed=5, edges=(16,), orders=(1,))
+    for p in probs:
+        p["source"] = lambda x, y: 0.1 * x   # an array source field on component 1
+    pars = [starmap_init(p) for p in probs]
+    setups, batch = setup_batch(pars)
+    try:
+        batch.set_states([S.U0 for S, _ in setups])
+        batch.set_dt([fs["dt"] for _, fs in setups])
+        S0 = setups[0][0]
+        g = S0.G(0)
+        batch.inst[0].set_source_expr(0, "t", [S0.xs[g[0] - 1], S0.ys[g[1] - 1], S0.zs[g[2] - 1]])
+        with pytest.raises(_lib.SmgError):
+            batch.run(2)
+        batch.inst[0].set_source_expr(0, None)
+        batch.run(2)
+    finally:
+        batch.close()
