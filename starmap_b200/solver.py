@@ -695,15 +695,7 @@ def starmap_solver(par: dict):
                                      ex("sigma_sm_expr") if S.flag_ani else None, rows, T.index[("sA",)],
                                      T.index[("EA",)], [S.xs[0], S.xs[1], S.ys[0], S.ys[1], S.zs[0], S.zs[1]])
             solver.set_time(0.0)
-            # dt of every step as the reference chooses it for time-dependent
-            # materials: min(dt_hyp, time left / cn) * cn, the last step shortened
-            sched_t, sched_dt = [], []
-            tt = 0.0
-            while tt < tfinal:
-                d = min(S.dt_hyp, (tfinal - tt) / cn) * cn
-                tt = tt + d
-                sched_t.append(tt)
-                sched_dt.append(d)
+            sched_t, sched_dt = td_schedule(S.dt_hyp, tfinal, cn)
         t_plot = list(np.atleast_1d(np.asarray(par.get("t_plot", [])))) + [np.inf]
         want_plot = par.get("output", _noop_output) is not _noop_output
         per_step = (td_any and not dev_mat) or (S.src_td and not dev_src) or (S.filter_td and not dev_filt)
@@ -787,6 +779,21 @@ def starmap_solver(par: dict):
         print(f"CPU-times\n advection:{gpu_s:12.2f}s{gpu_s / tot * 100:5.0f}%\n "
               f"absorb/scatter:{cpu_setup:7.2f}s{cpu_setup / tot * 100:5.0f}%\n plotting:{0.0:13.2f}s{0:5.0f}%")
     return _output_struct(S, U)
+
+
+def td_schedule(dt_hyp: float, tfinal: float, cn: float):
+    """Times after each step and the dt of each step as the reference chooses
+    them for time-dependent materials with the hyperbolic step
+    (starmap_solver.m:165-209): dt = min(dt_hyp, time left / cn) * cn, so the
+    last step is shortened to end at tfinal, and t = t + dt."""
+    ts, dts = [], []
+    t = 0.0
+    while t < tfinal:
+        d = min(dt_hyp, (tfinal - t) / cn) * cn
+        t = t + d
+        ts.append(t)
+        dts.append(d)
+    return ts, dts
 
 
 def device_source_expr(expr: str, dim: int) -> str:
