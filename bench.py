@@ -43,29 +43,33 @@ def dist_env():
 
 
 class Dist:
-    """Barrier and max-over-ranks; torch.distributed only when WORLD_SIZE > 1."""
+    """Barrier and max-over-ranks; torch.distributed only when WORLD_SIZE > 1
+    (NCCL on the GPUs; gloo on host tensors, which the CPU tests use)."""
 
     def __init__(self, world, local_rank, backend="nccl"):
         self.world = world
         self.torch = None
+        self.cuda = backend == "nccl"
         if world > 1:
             import datetime
 
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local_rank)
+            if self.cuda:
+                torch.cuda.set_device(local_rank)
             td.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
             self.torch, self.td = torch, td
 
     def barrier(self):
         if self.torch is not None:
             self.td.barrier()
-            self.torch.cuda.synchronize()
+            if self.cuda:
+                self.torch.cuda.synchronize()
 
     def max(self, v: float) -> float:
         if self.torch is None:
             return v
-        t = self.torch.tensor([float(v)], device="cuda", dtype=self.torch.float64)
+        t = self.torch.tensor([float(v)], device="cuda" if self.cuda else "cpu", dtype=self.torch.float64)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
@@ -121,6 +125,13 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows
                                                         if r[3].replace(".", "").isdigit())}
+
+
+def aggregate_rate(units_per_step: float, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job rate of N replicas (weak scaling): every rank advances its
+    own copy of the workload, so the job's units are N times one rank's, over
+    the slowest rank's time."""
+    return units_per_step * steps * world / (ms_max / 1e3)
 
 
 def measured_peak():
@@ -476,7 +487,7 @@ def main():
     achieved = alg["step"] / t_step / 1e9
     traffic = ncu_traffic(family)
     line = {
-        "metric": METRIC, "value": upd_step * args.steps * world / (ms_max / 1e3), "unit": UNIT,
+        "metric": METRIC, "value": aggregate_rate(upd_step, args.steps, world, ms_max), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",

@@ -44,6 +44,7 @@
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -116,9 +117,23 @@ void* open_first(std::initializer_list<const char*> names) {
     return nullptr;
 }
 
+// The CUDA toolkit's copy of a library by absolute path ($CUDA_HOME, then
+// /usr/local/cuda), before the bare name: a process may already hold another
+// release under the same name (PyTorch bundles its own NVRTC and nvJitLink),
+// which dlopen by name would return.
+void* open_toolkit(const char* lib, std::initializer_list<const char*> names) {
+    const char* roots[] = {std::getenv("CUDA_HOME"), "/usr/local/cuda"};
+    for (const char* root : roots) {
+        if (!root || !*root) continue;
+        const std::string path = std::string(root) + "/lib64/" + lib;
+        if (void* p = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL)) return p;
+    }
+    return open_first(names);
+}
+
 void load_api() {
     Api& a = g_api;
-    void* nv = open_first({"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"});
+    void* nv = open_toolkit("libnvrtc.so.12", {"libnvrtc.so.12", "libnvrtc.so"});
     if (!nv) {
         a.why = "NVRTC (libnvrtc.so.12) not found";
     } else if (sym(nv, "nvrtcCreateProgram", a.CreateProgram) && sym(nv, "nvrtcCompileProgram", a.CompileProgram) &&
@@ -131,7 +146,7 @@ void load_api() {
         a.why = "NVRTC entry points missing";
     }
     // nvJitLink exports versioned names (nvJitLink.h maps the API onto them)
-    void* jl = open_first({"libnvJitLink.so.12", "libnvJitLink.so", "/usr/local/cuda/lib64/libnvJitLink.so.12"});
+    void* jl = open_toolkit("libnvJitLink.so.12", {"libnvJitLink.so.12", "libnvJitLink.so"});
     if (!jl) {
         a.link_why = "nvJitLink (libnvJitLink.so.12) not found";
     } else if (sym(jl, "__nvJitLinkCreate_12_9", a.LinkCreate) && sym(jl, "__nvJitLinkDestroy_12_9", a.LinkDestroy) &&
