@@ -182,6 +182,18 @@ int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0
 int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const int32_t* rows,
                         const double* const* coords);
 
+/* Keep a copy of the current state on the device for smg_get_interp (the
+ * first call allocates it; it is freed with the handle).  The reference keeps
+ * that copy on the host (U0 before the last step of an output interval,
+ * starmap_solver.m:425-430). */
+int smg_snapshot(smg_handle* h);
+
+/* The components j with U[j] non-NULL of (1 - lambda) * snapshot +
+ * lambda * state, computed on the device in the reference's operation order
+ * and written to host arrays as smg_get_state does: the linear interpolation
+ * to an output time inside the last step (starmap_solver.m:431-473). */
+int smg_get_interp(smg_handle* h, double lambda, double* const* U);
+
 /* Advance `nsteps` full Strang steps A(dt/2) B(dt) A(dt/2) [+ full filter]
  * (starmap_solver.m:307-421) with the current dt.  Asynchronous on the
  * handle's stream; steps that move under 1 GB are replayed from captured

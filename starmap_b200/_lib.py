@@ -89,6 +89,8 @@ SIGNATURES = {
     "smg_set_field": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_double]),
     "smg_set_dt": (C.c_int, [C.c_void_p, C.c_double]),
     "smg_set_time": (C.c_int, [C.c_void_p, C.c_double]),
+    "smg_snapshot": (C.c_int, [C.c_void_p]),
+    "smg_get_interp": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.POINTER(C.c_double))]),
     "smg_set_filter_expr": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(C.c_int32),
                                       C.POINTER(C.POINTER(C.c_double))]),
     "smg_set_material_expr": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int32,

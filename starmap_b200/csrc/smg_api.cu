@@ -70,6 +70,9 @@ void free_device(smg_handle* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
     cudaFree(h->dU);
+    cudaFree(h->dSnap);
+    h->dSnap = nullptr;
+    h->snap_set = false;
     cudaFree(h->dStage);
     h->dStage = nullptr;
     h->stage_bytes = 0;
@@ -105,23 +108,27 @@ void free_device(smg_handle* h) {
     h->stream = nullptr;
 }
 
-// State transfers go through a staging buffer: each component of a chunk is
-// one linear copy (the copy engines move padded rows of a few KB several
-// times slower than contiguous data), and one kernel scatters the chunk into
-// (or gathers it from) the padded slots.  A component larger than the
-// staging buffer takes the pitched copy below.
+// State transfers go through a staging buffer: each component (in pieces of
+// whole rows where it exceeds the buffer) is one linear copy -- the copy
+// engines move padded rows of a few KB several times slower than contiguous
+// data -- and one kernel scatters a chunk into (or gathers it from) the
+// padded slots.
 constexpr size_t kStageBytes = 64u << 20;
 constexpr int kXferMax = 64;   // components per chunk (kernel parameter space)
 
 struct XferChunk {
     int n;
-    int e0[kXferMax], rows[kXferMax], e1[kXferMax];
+    int e0[kXferMax], e1[kXferMax], row0[kXferMax], rows[kXferMax];
     long long stage_off[kXferMax], slot_off[kXferMax];
 };
 
-// to_slots: stage -> padded slots, else slots -> stage.  blockIdx.z is the
-// component of the chunk, x runs along rows, blockIdx.y strides over rows.
-__global__ void k_xfer(XferChunk c, double* __restrict__ stage, double* __restrict__ U, long long s1, long long s2,
+// Entry k of a chunk: rows row0 .. row0+rows-1 (row = y + e1*z) of one
+// component, compact in the staging buffer.  to_slots: stage -> padded
+// slots; else slots -> stage, or with snap the interpolation
+// wa*snap + wb*U (the output-time interpolation, starmap_solver.m:425-473).
+// blockIdx.z is the entry, x runs along rows, blockIdx.y strides over rows.
+__global__ void k_xfer(XferChunk c, double* __restrict__ stage, double* __restrict__ U,
+                       const double* __restrict__ snap, double wa, double wb, long long s1, long long s2,
                        int to_slots) {
     const int k = blockIdx.z;
     if (k >= c.n) return;
@@ -131,41 +138,91 @@ __global__ void k_xfer(XferChunk c, double* __restrict__ stage, double* __restri
     double* st = stage + c.stage_off[k];
     double* sl = U + c.slot_off[k];
     for (int r = blockIdx.y; r < c.rows[k]; r += gridDim.y) {
-        const long long d = (long long)(r / e1) * s2 + (long long)(r % e1) * s1 + x;
+        const int row = c.row0[k] + r;
+        const long long d = (long long)(row / e1) * s2 + (long long)(row % e1) * s1 + x;
         const long long q = (long long)r * e0 + x;
         if (to_slots) sl[d] = st[q];
+        else if (snap) st[q] = __dadd_rn(__dmul_rn(wa, snap[c.slot_off[k] + d]), __dmul_rn(wb, sl[d]));
         else st[q] = sl[d];
     }
 }
 
-cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, bool to_slots) {
+cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, bool to_slots, const double* snap = nullptr,
+                        double wa = 0.0, double wb = 0.0) {
     int e0max = 1, rows_max = 1;
     for (int k = 0; k < c.n; ++k) {
         e0max = std::max(e0max, c.e0[k]);
         rows_max = std::max(rows_max, c.rows[k]);
     }
     dim3 grid((unsigned)((e0max + 127) / 128), (unsigned)std::min(rows_max, 4096), (unsigned)c.n);
-    k_xfer<<<grid, 128, 0, h->stream>>>(c, h->dStage, h->dU, h->g.s1, h->g.s2, to_slots ? 1 : 0);
+    k_xfer<<<grid, 128, 0, h->stream>>>(c, h->dStage, h->dU, snap, wa, wb, h->g.s1, h->g.s2, to_slots ? 1 : 0);
     return cudaGetLastError();
 }
 
+// The staged transfer of the components with non-NULL host pointers: each
+// component in pieces of whole rows that fit the staging buffer (a piece is
+// one contiguous range of the column-major host array), up to kXferMax
+// pieces per kernel launch.  Upload: copy the pieces in, then scatter.
+// Download: gather (or interpolate with snap), then copy the pieces out.
+int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double* const* Uout,
+                    const double* snap, double wa, double wb) {
+    XferChunk c;
+    c.n = 0;
+    size_t used = 0;
+    struct Piece { int j; size_t host_off, stage_off, bytes; };
+    std::vector<Piece> pend;
+    auto flush = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        if (c.n) e = xfer_launch(h, c, upload, snap, wa, wb);
+        if (!upload)
+            for (size_t i = 0; i < pend.size() && e == cudaSuccess; ++i)
+                e = cudaMemcpyAsync(reinterpret_cast<char*>(Uout[pend[i].j]) + pend[i].host_off,
+                                    reinterpret_cast<const char*>(h->dStage) + pend[i].stage_off, pend[i].bytes,
+                                    cudaMemcpyDeviceToHost, h->stream);
+        c.n = 0;
+        used = 0;
+        pend.clear();
+        return e;
+    };
+    for (int j = 0; j < h->n_sys; ++j) {
+        if (upload ? !Uin[j] : !Uout[j]) continue;
+        const int* e = h->comps[j].ext;
+        const size_t row_bytes = (size_t)e[0] * 8;
+        const int rows = e[1] * e[2];
+        const int max_rows = (int)std::max<size_t>(1, h->stage_bytes / row_bytes);
+        if (row_bytes > h->stage_bytes) return fail(h, SMG_EINVAL, "state transfer: a row exceeds the staging buffer");
+        for (int r0 = 0; r0 < rows; r0 += max_rows) {
+            const int nr = std::min(max_rows, rows - r0);
+            const size_t bytes = (size_t)nr * row_bytes;
+            if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
+            if (upload)
+                SMG_CUDA(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->dStage) + used,
+                                            reinterpret_cast<const char*>(Uin[j]) + (size_t)r0 * row_bytes, bytes,
+                                            cudaMemcpyHostToDevice, h->stream));
+            c.e0[c.n] = e[0];
+            c.e1[c.n] = e[1];
+            c.row0[c.n] = r0;
+            c.rows[c.n] = nr;
+            c.stage_off[c.n] = (long long)(used / 8);
+            c.slot_off[c.n] = (long long)j * h->g.cs;
+            ++c.n;
+            if (!upload) pend.push_back({j, (size_t)r0 * row_bytes, used, bytes});
+            used += (bytes + 255) / 256 * 256;
+        }
+    }
+    SMG_CUDA(h, flush());
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
 // Copy a column-major host array with extents e[] (kernel axes) into a
-// padded device slot (and back).
+// padded device slot (field uploads).
 cudaError_t put_slot(const smg_handle* h, double* dst, const double* src, const int e[3]) {
     cudaMemcpy3DParms p{};
     p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
     p.dstPtr = make_cudaPitchedPtr(dst, (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
     p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
     p.kind = cudaMemcpyHostToDevice;
-    return cudaMemcpy3DAsync(&p, h->stream);
-}
-
-cudaError_t get_slot(const smg_handle* h, double* dst, const double* src, const int e[3]) {
-    cudaMemcpy3DParms p{};
-    p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)h->g.s1 * 8, (size_t)h->g.s1, (size_t)h->g.B[1]);
-    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)e[0] * 8, (size_t)e[0], (size_t)e[1]);
-    p.extent = make_cudaExtent((size_t)e[0] * 8, (size_t)e[1], (size_t)e[2]);
-    p.kind = cudaMemcpyDeviceToHost;
     return cudaMemcpy3DAsync(&p, h->stream);
 }
 
@@ -815,81 +872,35 @@ int smg_set_state(smg_handle* h, const double* const* U) {
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_set_state: NULL argument");
     for (int j = 0; j < h->n_sys; ++j)
         if (!U[j]) return fail(h, SMG_EINVAL, "smg_set_state: NULL component pointer");
-    XferChunk c;
-    c.n = 0;
-    size_t used = 0;
-    auto flush = [&]() -> cudaError_t {
-        cudaError_t e = c.n ? xfer_launch(h, c, true) : cudaSuccess;
-        c.n = 0;
-        used = 0;
-        return e;
-    };
-    for (int j = 0; j < h->n_sys; ++j) {
-        const int* e = h->comps[j].ext;
-        const size_t bytes = (size_t)e[0] * e[1] * e[2] * 8;
-        if (bytes > h->stage_bytes) {
-            SMG_CUDA(h, put_slot(h, h->dU + (size_t)j * h->g.cs, U[j], e));
-            continue;
-        }
-        if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
-        SMG_CUDA(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->dStage) + used, U[j], bytes, cudaMemcpyHostToDevice,
-                                    h->stream));
-        c.e0[c.n] = e[0];
-        c.e1[c.n] = e[1];
-        c.rows[c.n] = e[1] * e[2];
-        c.stage_off[c.n] = (long long)(used / 8);
-        c.slot_off[c.n] = (long long)j * h->g.cs;
-        ++c.n;
-        used += (bytes + 255) / 256 * 256;
-    }
-    SMG_CUDA(h, flush());
-    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    const int rc = staged_transfer(h, true, U, nullptr, nullptr, 0.0, 0.0);
+    if (rc != SMG_OK) return rc;
     h->state_set = true;
     return SMG_OK;
 }
 
 int smg_get_state(smg_handle* h, double* const* U) {
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_state: NULL argument");
-    // per chunk: gather into the staging buffer, then one linear copy per
-    // component (the next chunk's gather waits for these on the stream)
-    XferChunk c;
-    c.n = 0;
-    size_t used = 0;
-    std::vector<std::pair<int, size_t>> pend;   // (component, staging byte offset)
-    auto flush = [&]() -> cudaError_t {
-        cudaError_t e = cudaSuccess;
-        if (c.n) e = xfer_launch(h, c, false);
-        for (size_t i = 0; i < pend.size() && e == cudaSuccess; ++i) {
-            const int* x = h->comps[pend[i].first].ext;
-            e = cudaMemcpyAsync(U[pend[i].first], reinterpret_cast<const char*>(h->dStage) + pend[i].second,
-                                (size_t)x[0] * x[1] * x[2] * 8, cudaMemcpyDeviceToHost, h->stream);
-        }
-        c.n = 0;
-        used = 0;
-        pend.clear();
-        return e;
-    };
-    for (int j = 0; j < h->n_sys; ++j) {
-        if (!U[j]) continue;
-        const int* e = h->comps[j].ext;
-        const size_t bytes = (size_t)e[0] * e[1] * e[2] * 8;
-        if (bytes > h->stage_bytes) {
-            SMG_CUDA(h, get_slot(h, U[j], h->dU + (size_t)j * h->g.cs, e));
-            continue;
-        }
-        if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
-        c.e0[c.n] = e[0];
-        c.e1[c.n] = e[1];
-        c.rows[c.n] = e[1] * e[2];
-        c.stage_off[c.n] = (long long)(used / 8);
-        c.slot_off[c.n] = (long long)j * h->g.cs;
-        ++c.n;
-        pend.push_back({j, used});
-        used += (bytes + 255) / 256 * 256;
+    return staged_transfer(h, false, nullptr, U, nullptr, 0.0, 0.0);
+}
+
+int smg_snapshot(smg_handle* h) {
+    if (!h) return fail(h, SMG_EINVAL, "smg_snapshot: NULL handle");
+    if (!h->state_set) return fail(h, SMG_ESTATE, "smg_snapshot: smg_set_state has not been called");
+    const size_t bytes = (size_t)h->g.cs * h->n_sys * sizeof(double);
+    if (!h->dSnap) {
+        SMG_CUDA(h, cudaMalloc(&h->dSnap, bytes));
+        h->bytes += bytes;
     }
-    SMG_CUDA(h, flush());
-    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    SMG_CUDA(h, cudaMemcpyAsync(h->dSnap, h->dU, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    h->snap_set = true;
     return SMG_OK;
+}
+
+int smg_get_interp(smg_handle* h, double lambda, double* const* U) {
+    if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_interp: NULL argument");
+    if (!h->snap_set) return fail(h, SMG_ESTATE, "smg_get_interp: smg_snapshot has not been called");
+    if (!std::isfinite(lambda)) return fail(h, SMG_EINVAL, "smg_get_interp: lambda must be finite");
+    return staged_transfer(h, false, nullptr, U, h->dSnap, 1.0 - lambda, lambda);
 }
 
 int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {

@@ -47,6 +47,8 @@ struct smg_handle {
     // device memory
     double* dU = nullptr;
     double* dStage = nullptr;        // staging for state transfers (linear copies, then a scatter kernel)
+    double* dSnap = nullptr;         // copy of the state for output-time interpolation (smg_snapshot)
+    bool snap_set = false;
     size_t stage_bytes = 0;
     double* dFields = nullptr;       // slots for array fields
     smg::DevComp* dComps = nullptr;

@@ -116,6 +116,18 @@ class GpuSolver:
         """Components ``which`` (default all) as arrays of their extents.  With
         ``out`` ({j: float64 buffer of the component's size}, e.g. in pinned
         host memory) the values are written there."""
+        return self._download(lambda ptrs: self._L.smg_get_state(self.h, ptrs), which, out)
+
+    def snapshot(self):
+        """Keep a device copy of the current state (for :meth:`get_interp`)."""
+        check(self._L.smg_snapshot(self.h), self.h)
+
+    def get_interp(self, lam, which=None, out=None):
+        """Components ``which`` of ``(1 - lam) * snapshot + lam * state``,
+        computed on the device (the output-time interpolation)."""
+        return self._download(lambda ptrs: self._L.smg_get_interp(self.h, float(lam), ptrs), which, out)
+
+    def _download(self, call, which, out):
         which = range(self.n_sys) if which is None else which
         res = {}
         ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
@@ -129,7 +141,7 @@ class GpuSolver:
                 buf = np.empty(int(np.prod(e)), dtype=np.float64)
             res[j] = (buf, e)
             ptrs[j] = dptr(buf)
-        check(self._L.smg_get_state(self.h, ptrs), self.h)
+        check(call(ptrs), self.h)
         return {j: buf.reshape(e, order="F") for j, (buf, e) in res.items()}
 
     def set_field(self, k, val):
@@ -743,7 +755,6 @@ def starmap_solver(par: dict):
                     if tk >= t_plot[plot_count] - 1e-14:
                         nrun = k + 1
                         break
-            U0 = None
             if want_plot and nrun >= 1:
                 if nrun > 1:
                     solver.run(nrun - 1)
@@ -751,16 +762,17 @@ def starmap_solver(par: dict):
                         t_cur = t_cur + dt
                     step_count += nrun - 1
                     nrun = 1
-                U0 = solver.get_state([j - 1 for j in S.mom_output])
+                solver.snapshot()   # the state before the last step, kept on the device
             solver.run(nrun)
             for _ in range(nrun):
                 t_cur = t_cur + dt
             step_count += nrun
             if want_plot:
-                Un = solver.get_state([j - 1 for j in S.mom_output])
                 while t_cur >= t_plot[plot_count] - 1e-14:
                     lam = (t_plot[plot_count] - t_cur + dt) / dt
-                    Uplot = [(1 - lam) * U0[j - 1] + lam * Un[j - 1] for j in S.mom_output]
+                    # (1 - lam) * U0 + lam * Un on the device, downloaded once
+                    Ud = solver.get_interp(lam, [j - 1 for j in S.mom_output])
+                    Uplot = [Ud[j - 1] for j in S.mom_output]
                     ret = _call_output(S, outfn, par, Uplot, plot_count + 1)
                     if isinstance(ret, dict):
                         par = ret
