@@ -49,7 +49,8 @@ def test_linesource_xy_symmetry():
     assert np.abs(U - U.T).max() <= 1e-13 * np.abs(U).max()
 
 
-@pytest.mark.parametrize("name", ["lattice_p5_substep", "box3d_bc1_p2_full", "td_sigma", "spn_3d"])
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "box3d_bc1_p2_full", "td_sigma", "spn_3d",
+                                  "parabolic_homog", "parabolic_td", "boxes_td_source"])
 def test_numpy_and_c_restatements_agree(name):
     par = starmap_init(cases.ALL[name]())
     a = O.starmap_solver(par)
