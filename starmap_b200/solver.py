@@ -447,7 +447,11 @@ def prepare(par: dict) -> _Setup:
 
     def XYZ(g):
         if g not in grids:
-            grids[g] = np.meshgrid(xs[g[0] - 1], ys[g[1] - 1], zs[g[2] - 1], indexing="ij")
+            # column-major (the reference's layout): hook results computed
+            # elementwise on these grids are column-major too, so the state
+            # and field uploads need no transposing copy
+            grids[g] = [np.asfortranarray(a) for a in
+                        np.meshgrid(xs[g[0] - 1], ys[g[1] - 1], zs[g[2] - 1], indexing="ij")]
         return grids[g]
 
     S.par, S.n_sys, S.Mx, S.My, S.Mz = par, n_sys, Mx, My, Mz
