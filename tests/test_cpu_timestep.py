@@ -97,3 +97,24 @@ def test_3d_field_with_planes_is_rejected():
     prob["sigma_s0"] = lambda x, y, z: 1.0 + 0.1 * z
     with pytest.raises(ValueError):
         first_step(prepare(starmap_init(prob)))
+
+
+def test_search_with_zero_cross_sections_and_little_time_left():
+    """sigma = 0: below the stability limit the growth factor is 1, so the
+    search lowers its threshold to 1 and still brackets the limit; with less
+    time left than a step, the lower end stops at or past the time left."""
+    prob = cases.parabolic_homog()
+    prob["sigma_a"] = lambda x, y: 0.0
+    prob["sigma_s0"] = lambda x, y: 0.0
+    S = prepare(starmap_init(prob))
+    decay = np.zeros(S.n_sys)
+    dt_b, la0 = timestep.search(S.M_sym, S.even, S.odd, decay, 0.0, S.dt_hyp, 1e9, 1)
+    assert 0 < dt_b < 1e9
+    assert timestep.growth_factor(S.M_sym, S.even, S.odd, decay, dt_b, 1) < la0
+    # the hyperbolic step is stable, so with less time left than it the
+    # bracket never moves: its lower end stays at dt_hyp (the caller then
+    # takes min(dt, time left) * cn)
+    small = 0.1 * S.dt_hyp
+    dt_s, _ = timestep.search(S.M_sym, S.even, S.odd, decay, 0.0, S.dt_hyp, small, 1)
+    assert dt_s == S.dt_hyp
+    assert dt_b >= S.dt_hyp
