@@ -64,3 +64,34 @@ def test_step_count_overshoot_quirk():
     par = starmap_init(configs.linesource(n=100, n_mom=7, tfinal=1.0))
     r = O.starmap_solver(par, max_steps=None)
     assert r.step_count == 67 and r.t > 1.0
+
+
+def _staggered_l2(U, n, h):
+    """Squared discrete L2 norm of one 2D component with the weights of
+    starmap_2d_ex_l2norm.m:93-99 (for each axis: a component on the n cell
+    centres has end weights 1/2, one on the n+1 faces end weights 0)."""
+    U = np.squeeze(np.asarray(U))
+    s = [U.shape[d] == n[d] for d in range(2)]
+    w1 = np.ones(n[0] + 1 - s[0])
+    w1[[0, -1]] = s[0] / 2
+    w2 = np.ones(n[1] + 1 - s[1])
+    w2[[0, -1]] = s[1] / 2
+    return np.prod(h) * w1 @ (U ** 2) @ w2
+
+
+@pytest.mark.parametrize("bc", [1, 0])
+def test_discrete_energy_does_not_grow_in_void(bc):
+    """The expanding Gaussian of starmap_2d_ex_l2norm.m (void, all moments at
+    output times): the staggered L2 energy never increases and stays within
+    2% of its start by t = 0.5."""
+    n = 24
+    prob = dict(name="gauss", closure="P", n_mom=3, ax=[-1, 1, -1, 1], n=[n, n], bc=[bc, bc],
+                ic=lambda x, y, k: (1 / (4 * np.pi * 1e-2)) * np.exp(-(x ** 2 + y ** 2) / (4 * 1e-2)) * (k == 1),
+                t_plot=list(np.linspace(0, 0.5, 11)), mom_output="all", output=lambda *a: None, tfinal=0.5,
+                quiet=True)
+    r = O.starmap_solver(starmap_init(prob), capture_snapshots=True)
+    h = [2 / n, 2 / n]
+    E = np.array([np.sqrt(sum(_staggered_l2(u, [n, n], h) for u in Us)) for _, Us in r.snapshots])
+    assert len(E) == 11
+    assert np.all(np.diff(E) <= 1e-14 * E[0])
+    assert E[-1] >= 0.98 * E[0]
