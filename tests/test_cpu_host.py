@@ -123,3 +123,17 @@ def test_init_wraps_2d_hooks_and_defaults():
         starmap_init(dict(closure="P", n_mom=3, ax=[0, 1, 0, 2], n=[4]))
     with pytest.raises(ValueError):
         starmap_init(dict(closure="P", n_mom=3, ax=[0, 1, 0, 1], ic=lambda x: x))
+
+
+@pytest.mark.parametrize("prob", [
+    dict(closure="P", n_mom=3),                                            # none of ax, n, bc
+    dict(closure="P", n_mom=3, ax=[0, 1, 0, 1], bc=[1, 1, 1]),             # ax and bc disagree
+    dict(closure="P", n_mom=3, n=[4, 4], bc=[0, 0, 0]),                    # n and bc disagree
+    dict(closure="P", n_mom=3, ax=[0, 1, 0, 1], n=[4, 4], sigma_a=lambda a, b, c, d, e: a),   # hook arity
+    dict(closure="P", n_mom=3, ax=[0, 1, 0, 1], n=[4, 4], source=lambda: 1.0),                # hook arity
+])
+def test_init_rejects_inconsistent_problems(prob):
+    """starmap_init.m:36-60 and the hook-arity checks: inconsistent ax/n/bc
+    and hooks of an unsupported number of arguments are errors."""
+    with pytest.raises(ValueError):
+        starmap_init(prob)

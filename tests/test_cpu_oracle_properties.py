@@ -49,6 +49,16 @@ def test_linesource_xy_symmetry():
     assert np.abs(U - U.T).max() <= 1e-13 * np.abs(U).max()
 
 
+def test_linesource_reflection_symmetry():
+    """The line source is symmetric under x -> -x and y -> -y: the zeroth
+    moment (cell centres, symmetric about 0) is mirrored in both axes."""
+    r = O.starmap_solver(starmap_init(configs.linesource(n=30, n_mom=5, tfinal=1.0)))
+    U = np.asarray(r.output[0]["U"])
+    scale = np.abs(U).max()
+    assert np.abs(U - U[::-1, :]).max() <= 1e-12 * scale
+    assert np.abs(U - U[:, ::-1]).max() <= 1e-12 * scale
+
+
 @pytest.mark.parametrize("name", ["lattice_p5_substep", "box3d_bc1_p2_full", "td_sigma", "spn_3d",
                                   "parabolic_homog", "parabolic_td", "boxes_td_source"])
 def test_numpy_and_c_restatements_agree(name):
