@@ -1,0 +1,47 @@
+"""Randomised agreement of the two independent restatements of the
+reference loop (numpy, and the OpenMP C loop used as the CPU baseline):
+hypothesis draws small 2D and 3D problems -- closure and order, cell counts
+(odd and unequal), boundary conditions per axis, material and source fields,
+filter position -- and both must give the same bits."""
+import numpy as np
+from hypothesis import HealthCheck, given, settings, strategies as st
+
+from oracle import c_oracle
+from oracle import solver_np as O
+from starmap_b200 import configs, starmap_init
+
+
+@st.composite
+def problems(draw):
+    dim = draw(st.sampled_from([2, 3]))
+    closure = draw(st.sampled_from(["P", "SP"]))
+    n_mom = draw(st.integers(1, 4 if dim == 2 else 2))
+    n = [draw(st.integers(3, 9)) for _ in range(dim)]
+    bc = [draw(st.integers(0, 1)) for _ in range(dim)]
+    fpos = draw(st.sampled_from(["", "substep", "full"]))
+    a0, a1 = draw(st.floats(0.0, 2.0)), draw(st.floats(-0.5, 0.5))
+    s0 = draw(st.floats(0.0, 2.0))
+    q = draw(st.floats(0.0, 1.0))
+    if dim == 2:
+        prob = dict(ax=[-1.0, 1.0, -0.5, 1.5], ic=lambda x, y: np.exp(-4 * (x ** 2 + y ** 2)),
+                    sigma_a=lambda x, y: a0 + a1 * np.sin(x + 2 * y), sigma_s0=lambda x, y: s0 + 0 * x,
+                    source=lambda x, y: q * np.exp(-3 * ((x - 0.2) ** 2 + y ** 2)))
+    else:
+        prob = dict(ax=[-1.0, 1.0, -1.0, 1.0, -0.5, 1.0], ic=lambda x, y, z: np.exp(-4 * (x ** 2 + y ** 2 + z ** 2)),
+                    sigma_a=lambda x, y, z: a0 + a1 * np.sin(x + 2 * y - z), sigma_s0=lambda x, y, z: s0 + 0 * x,
+                    source=lambda x, y, z: q * np.exp(-3 * ((x - 0.2) ** 2 + y ** 2 + z ** 2)))
+    prob.update(closure=closure, n_mom=n_mom, n=n, bc=bc, tfinal=0.3, quiet=True)
+    if fpos:
+        prob.update(filterfunction=configs.exp_filter(2, 2.0), f_position=fpos)
+    return prob
+
+
+@settings(max_examples=25, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(problems())
+def test_numpy_and_c_restatements_agree_on_random_problems(prob):
+    par = starmap_init(prob)
+    a = O.starmap_solver(par)
+    b = c_oracle.run(par, nthreads=2)
+    assert a.step_count == b.step_count
+    for u, v in zip(a.output, b.output):
+        np.testing.assert_array_equal(u["U"], v["U"])
