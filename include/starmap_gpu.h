@@ -335,6 +335,8 @@ typedef struct smg_batch smg_batch;
 #define SMG_BATCH_JIT              8  /* 1: kernels generated per family of equal-structure instances (default;
                                          built on the first run, NVRTC needed), 0: the precompiled kernels */
 
+/* Instances with f_position 'full' (SMG_FILTER_FULL) are refused (SMG_EINVAL):
+ * the batch kernels do not apply the full-step filter. */
 int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch** out);
 void smg_batch_destroy(smg_batch* b);
 const char* smg_batch_last_error(const smg_batch* b);

@@ -362,6 +362,14 @@ extern "C" {
 int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch** out) {
     if (!out || n_inst < 1 || !probs) return bfail(nullptr, SMG_EINVAL, "smg_batch_create: bad arguments");
     *out = nullptr;
+    // the batch kernels apply no full-step filter (f_position 'full',
+    // starmap_solver.m:417-421): refuse such instances rather than skip it
+    for (int i = 0; i < n_inst; ++i)
+        if (!probs[i] || probs[i]->filter_mode == SMG_FILTER_FULL)
+            return bfail(nullptr, SMG_EINVAL,
+                         "smg_batch_create: instance " + std::to_string(i) +
+                             (probs[i] ? " uses f_position 'full', which the batched solver does not apply"
+                                       : " is NULL"));
     smg_batch* b = new smg_batch();
     for (int i = 0; i < n_inst; ++i) {
         smg_handle* h = nullptr;

@@ -137,3 +137,14 @@ def test_init_rejects_inconsistent_problems(prob):
     and hooks of an unsupported number of arguments are errors."""
     with pytest.raises(ValueError):
         starmap_init(prob)
+
+
+def test_batch_refuses_full_filter_before_device_work():
+    """The batched solver does not apply the full-step filter, so an instance
+    with f_position 'full' is refused at creation (before any device work)."""
+    from starmap_b200 import _lib, configs
+    from starmap_b200.batch import setup_batch
+    probs = configs.batched_sweep(n_inst=2, seed=5, edges=(16,), orders=(1,))
+    probs[1].update(filterfunction=configs.exp_filter(2, 2.0), f_position="full")
+    with pytest.raises(_lib.SmgError, match="full"):
+        setup_batch([starmap_init(p) for p in probs])
