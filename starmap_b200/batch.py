@@ -109,9 +109,17 @@ class GpuBatch:
 
 
 def setup_batch(pars):
-    """Host setup of every ``par`` and the batch handle (states/dt not yet set)."""
+    """Host setup of every ``par`` and the batch handle (states/dt not yet set).
+
+    A batch advances every instance with the coefficients of its first step
+    and a fixed dt, so it takes autonomous problems only: materials, sources
+    and filters whose hooks depend on t are refused (they need the per-step
+    path of ``starmap_solver``, starmap_solver.m:165-305)."""
     setups = []
-    for par in pars:
+    for i, par in enumerate(pars):
         S = prepare(par)
+        if S.time_dependent.any() or S.src_td or S.filter_td:
+            raise ValueError(f"batch instance {i}: time-dependent materials, sources or filters are not "
+                             "supported by the batched solver (run it through starmap_solver)")
         setups.append((S, first_step(S)))
     return setups, GpuBatch(setups)

@@ -148,3 +148,15 @@ def test_batch_refuses_full_filter_before_device_work():
     probs[1].update(filterfunction=configs.exp_filter(2, 2.0), f_position="full")
     with pytest.raises(_lib.SmgError, match="full"):
         setup_batch([starmap_init(p) for p in probs])
+
+
+def test_batch_refuses_time_dependent_problems():
+    """A batch keeps each instance's first-step coefficients and dt, so
+    time-dependent hooks are refused at set-up (on the host)."""
+    import cases
+    from starmap_b200 import configs
+    from starmap_b200.batch import setup_batch
+    good = starmap_init(configs.batched_sweep(n_inst=1, seed=5, edges=(16,), orders=(1,))[0])
+    for bad in (cases.td_sigma(), cases.boxes_td_source()):
+        with pytest.raises(ValueError, match="time-dependent"):
+            setup_batch([good, starmap_init(bad)])
