@@ -118,3 +118,22 @@ def test_search_with_zero_cross_sections_and_little_time_left():
     dt_s, _ = timestep.search(S.M_sym, S.even, S.odd, decay, 0.0, S.dt_hyp, small, 1)
     assert dt_s == S.dt_hyp
     assert dt_b >= S.dt_hyp
+
+
+from hypothesis import HealthCheck, given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=12, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(ts=st.sampled_from([0, 1, 2]), n=st.integers(4, 8), a0=st.floats(0.5, 4.0), a1=st.floats(0.0, 2.0),
+       w=st.floats(0.5, 8.0), s0=st.floats(0.0, 4.0), tfinal=st.floats(0.05, 0.4))
+def test_host_dt_sequence_matches_oracle_on_random_td_problems(ts, n, a0, a1, w, s0, tfinal):
+    """Time-dependent absorption with the hyperbolic or a parabolic step: the
+    host loop's dt of every step equals the oracle's."""
+    prob = dict(name="td", closure="P", n_mom=2, timestep=ts, ax=[0, 1, 0, 1], n=[n, n + 1], bc=[0, 1],
+                ic=lambda x, y: np.exp(-10 * ((x - .5) ** 2 + (y - .5) ** 2)),
+                sigma_a=lambda x, y, t: a0 + a1 * np.sin(w * t) + 0 * x, sigma_s0=lambda x, y: s0 + 0 * x,
+                tfinal=tfinal, quiet=True)
+    par = starmap_init(prob)
+    ref = O.starmap_solver(par)
+    _, dts = host_dts(par)
+    assert dts == [float(d) for d in ref.dts]
