@@ -13,7 +13,7 @@ from test_cpu_jit import _nvrtc_available
 from test_cpu_oracle_random import problems
 
 
-@settings(max_examples=8, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=8, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(problems())
 def test_generated_kernels_compile_for_random_problems(prob):
     if not _nvrtc_available():

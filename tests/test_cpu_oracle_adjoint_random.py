@@ -17,7 +17,7 @@ def _final(par, nsteps, U0):
     return O.starmap_solver(par, max_steps=nsteps, advance=rec).U
 
 
-@settings(max_examples=10, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=10, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(problems())
 def test_oracle_adjoint_dot_product_on_random_problems(prob):
     assume(prob.get("f_position", "") != "full")

@@ -15,7 +15,7 @@ from test_gpu_adjoint import make_solver
 pytestmark = pytest.mark.gpu
 
 
-@settings(max_examples=8, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=8, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(problems())
 def test_gpu_adjoint_matches_cpu_adjoint_on_random_problems(prob):
     assume(prob.get("f_position", "") != "full")

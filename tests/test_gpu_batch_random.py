@@ -19,7 +19,7 @@ def _two_d(prob):
     return len(prob["n"]) == 2 and prob.get("f_position", "") != "full"
 
 
-@settings(max_examples=6, deadline=None, suppress_health_check=[HealthCheck.too_slow, HealthCheck.filter_too_much])
+@settings(max_examples=6, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow, HealthCheck.filter_too_much])
 @given(st.lists(problems().filter(_two_d), min_size=2, max_size=5))
 def test_batch_matches_plain_runs_on_random_sets(probs):
     pars = [starmap_init(dict(p, tfinal=1e9)) for p in probs]

@@ -15,7 +15,7 @@ from test_cpu_oracle_random import problems
 pytestmark = pytest.mark.gpu
 
 
-@settings(max_examples=12, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=12, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(problems())
 def test_gpu_matches_oracle_on_random_problems(prob):
     par = starmap_init(prob)
