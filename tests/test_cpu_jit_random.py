@@ -26,3 +26,22 @@ def test_generated_kernels_compile_for_random_problems(prob):
     # every component is updated once per phase in the plain kernels
     plain = src.split("// ---- program (smg_fam_")[0]
     assert plain.count("double* Uj = U + pt + ") == S.n_sys
+
+
+@settings(max_examples=6, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
+@given(problems())
+def test_generated_adjoint_kernels_compile_for_random_problems(prob):
+    """The adjoint's recording and backward-phase kernels (filters '' and
+    'substep', the adjoint's scope) compile for drawn structures too."""
+    if not _nvrtc_available():
+        pytest.skip("NVRTC library not present")
+    if prob.get("f_position", "") == "full":
+        prob = dict(prob)
+        prob.pop("f_position")
+        prob.pop("filterfunction")
+    S = prepare(starmap_init(prob))
+    fs = first_step(S)
+    T = _tables(S, fs)
+    src = jit_source(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T), compile=2,
+                     tune={_lib.SMG_TUNE_JIT_GROUP: 4, _lib.SMG_TUNE_JIT_SPLIT: 3})
+    assert "smg_adj_p1_0(" in src and "smg_adj_s1_0(" in src
