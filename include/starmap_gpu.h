@@ -110,7 +110,10 @@ int smg_set_device(int32_t device);
 
 /* Validate the descriptor, build the coupling tables (the Ix/Iy/Iz lists of
  * starmap_solver.m:77-79 in sumcell order, starmap_solver.m:350-351/398-399),
- * allocate device memory and upload the coefficient fields.
+ * allocate device memory and upload the coefficient fields. Limits: n[d] <=
+ * 2^30, and one component's padded slot (the points of the first kernel axis
+ * rounded up to 8, times those of the other two, faces included) below 2^31
+ * points, since the kernels index a point with 32 bits; else SMG_EINVAL.
  * Replaces: starmap_solver.m:136-157 (field allocation) on the device side. */
 int smg_create(const smg_problem* p, smg_handle** out);
 

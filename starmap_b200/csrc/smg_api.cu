@@ -625,7 +625,7 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device) {
     if (p->filter_mode != 0 && !p->filter1) return fail(nullptr, SMG_EINVAL, "filter1 table required");
     if (p->filter_mode == 1 && !p->filter2) return fail(nullptr, SMG_EINVAL, "filter2 table required for substep");
     for (int d = 0; d < 3; ++d) {
-        if (p->n[d] < 1) return fail(nullptr, SMG_EINVAL, "n[d] must be >= 1");
+        if (p->n[d] < 1 || p->n[d] > (1 << 30)) return fail(nullptr, SMG_EINVAL, "n[d] must be in [1, 2^30]");
         if (p->bc[d] != 0 && p->bc[d] != 1) return fail(nullptr, SMG_EINVAL, "bc[d] must be 0 or 1");
         if (!(p->h[d] > 0.0) || !std::isfinite(p->h[d])) return fail(nullptr, SMG_EINVAL, "h[d] must be finite and > 0");
     }
@@ -670,6 +670,11 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device) {
         h->g.bc[k] = p->bc[d];
         h->g.h[k] = p->h[d];
         h->g.B[k] = p->n[d] + ((p->bc[d] == 1 && gt2[d]) ? 1 : 0);
+    }
+    // the kernels index a point inside one component with 32-bit integers
+    if (std::ceil(h->g.B[0] / 8.0) * 8.0 * h->g.B[1] * h->g.B[2] + 31.0 >= 2147483648.0) {
+        delete h;
+        return fail(nullptr, SMG_EINVAL, "grid too large: one component must hold fewer than 2^31 padded points");
     }
     h->g.s1 = ((long long)h->g.B[0] + 7) / 8 * 8;
     h->g.s2 = h->g.s1 * h->g.B[1];

@@ -40,6 +40,32 @@ def test_create_rejects_bad_descriptor():
     assert L.smg_create(None, ctypes.byref(h)) == _lib.SMG_EINVAL
 
 
+@pytest.mark.parametrize("n,msg", [((1, 65536, 32768), b"2^31"), ((1, 1, (1 << 30) + 1), b"n[d]")])
+def test_create_refuses_grids_beyond_32bit_point_index(n, msg):
+    """A component whose padded slot holds 2^31 points or more is refused
+    before any device work (the kernels index a point with 32 bits)."""
+    L = _lib.lib()
+    p = _lib.smg_problem()
+    p.n_sys = 1
+    p.n[:] = n
+    p.bc[:] = (0, 0, 0)
+    p.h[:] = (1.0, 1e-3, 1e-3)
+    gt = (ctypes.c_int32 * 3)(1, 1, 1)
+    M = (ctypes.c_double * 1)(0.0)
+    tab = (ctypes.c_int32 * 1)(-1)
+    f = (_lib.smg_field * 1)()
+    f[0].scalar = 1.0
+    f[0].grid[:] = (1, 1, 1)
+    p.gt, p.Mx, p.My, p.Mz = gt, M, M, M
+    p.n_fields, p.fields = 1, f
+    p.sigma_t, p.source = tab, tab
+    p.sigma_a, p.decay_a, p.filter_mode = 0, -1, 0
+    h = ctypes.c_void_p()
+    assert L.smg_create(ctypes.byref(p), ctypes.byref(h)) == _lib.SMG_EINVAL
+    assert msg in L.smg_last_error(None)
+    assert not h.value
+
+
 @pytest.mark.parametrize("N,lam", [(7, 0.960290), (39, 0.998238), (15, 0.989401)])
 def test_pn2d_eigenvalue_pins(N, lam):
     # largest |eigenvalue| of Mz equals the largest root of the Legendre
