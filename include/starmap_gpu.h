@@ -222,7 +222,9 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
  * NUL-terminated copy.  compile = 1 also compiles it with NVRTC for sm_100a
  * (no GPU needed); compile = 2 adds (to the source and the compilation) the
  * adjoint's recording and backward-phase kernels, compile = 3 the batched
- * solver's family kernels.  No reference counterpart. */
+ * solver's family kernels.  SMG_EINVAL for a problem whose state holds 2^31
+ * doubles or more (the generated kernels use 32-bit element offsets).  No
+ * reference counterpart. */
 int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune, int32_t compile,
                    char* buf, int64_t cap, int64_t* len);
 

@@ -2250,6 +2250,11 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
     smg_handle* h = nullptr;
     int rc = smg::create_host(p, &h);
     if (rc != SMG_OK) return rc;
+    if (!(h->pair[0].ok && h->pair[1].ok)) {   // the generator reads the pair tables
+        delete h;
+        smg::set_global_error("smg_jit_source: the problem exceeds 32-bit element offsets");
+        return SMG_EINVAL;
+    }
     for (int i = 0; i < ntune; ++i) {
         if (keys[i] < SMG_TUNE_JIT_BLOCK) {
             rc = SMG_EINVAL;

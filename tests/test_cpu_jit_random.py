@@ -45,3 +45,18 @@ def test_generated_adjoint_kernels_compile_for_random_problems(prob):
     src = jit_source(S.n, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T), compile=2,
                      tune={_lib.SMG_TUNE_JIT_GROUP: 4, _lib.SMG_TUNE_JIT_SPLIT: 3})
     assert "smg_adj_p1_0(" in src and "smg_adj_s1_0(" in src
+
+
+def test_generator_refuses_state_beyond_32bit_offsets():
+    """A 2D P7 problem on 7800 x 7800 cells holds 36 slots of about 61e6
+    points, over 2^31 doubles in all: the generated kernels address
+    components through 32-bit element offsets, so the generator refuses it
+    on the host instead of reading wrapped offsets."""
+    from starmap_b200 import configs
+    from starmap_b200.solver import SmgError
+    S = prepare(starmap_init(configs.linesource(n=20, n_mom=7, tfinal=0.1)))
+    T = _tables(S, first_step(S))
+    assert all(getattr(v, "ndim", 0) == 0 for v, _ in T.fields)
+    big = [1, 7800, 7800]
+    with pytest.raises(SmgError, match="32-bit element offsets"):
+        jit_source(big, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
