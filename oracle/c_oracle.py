@@ -9,7 +9,6 @@ arrays.  Use ``run(par, nthreads)`` for a full solve.
 from __future__ import annotations
 
 import ctypes as C
-import os
 import time
 
 import numpy as np

@@ -25,7 +25,7 @@ import time
 import numpy as np
 
 from . import _lib
-from ._lib import FILTER_FULL, FILTER_NONE, FILTER_SUBSTEP, SmgError, check, dptr, iptr
+from ._lib import FILTER_FULL, FILTER_NONE, FILTER_SUBSTEP, check, dptr, iptr
 from . import timestep
 from .init import _noop_output, capargs, nargin, zero
 
@@ -543,7 +543,6 @@ class _Tables:
 
 
 def _build(S, sA1, sT1, EA, ET, Q, F):
-    n_sys = S.n_sys
     T = _Tables()
     for row in S.sg:
         T.add(("sT",) + row, sT1[row], row[:3])

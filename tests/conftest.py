@@ -1,8 +1,6 @@
 import os
 import sys
 
-import pytest
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
@@ -11,9 +9,3 @@ if ROOT not in sys.path:
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: long-running CPU test")
-
-
-def pytest_collection_modifyitems(config, items):
-    # GPU tests fail loudly (no fallback) when no device is present; that is
-    # the point of the gpu marker, so they are not skipped here.
-    pass

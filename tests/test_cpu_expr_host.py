@@ -1,7 +1,6 @@
 """Host side of the device-evaluated hooks: the time-dependent dt schedule
 against the oracle's steps, and the mapping of a user expression's
 variables onto the solver dimensions the generated kernels use."""
-import numpy as np
 import pytest
 
 import cases

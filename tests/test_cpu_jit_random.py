@@ -53,10 +53,9 @@ def test_generator_refuses_state_beyond_32bit_offsets():
     components through 32-bit element offsets, so the generator refuses it
     on the host instead of reading wrapped offsets."""
     from starmap_b200 import configs
-    from starmap_b200.solver import SmgError
     S = prepare(starmap_init(configs.linesource(n=20, n_mom=7, tfinal=0.1)))
     T = _tables(S, first_step(S))
     assert all(getattr(v, "ndim", 0) == 0 for v, _ in T.fields)
     big = [1, 7800, 7800]
-    with pytest.raises(SmgError, match="32-bit element offsets"):
+    with pytest.raises(_lib.SmgError, match="32-bit element offsets"):
         jit_source(big, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
