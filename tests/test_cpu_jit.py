@@ -81,3 +81,14 @@ def test_family_kernels_compile(name):
     # one block per destination in the family kernels too
     fam = src[src.index("// ---- program (smg_fam_"):]
     assert fam.count("double* Uj = U + pt + ") == S.n_sys
+
+
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "pt3d_p3", "spn_3d"])
+def test_generated_source_is_deterministic(name):
+    """The per-process compile cache is keyed by source text, so the
+    generator gives the same text for the same problem, also after another
+    problem was generated in between."""
+    _, a = _source(name, split=16)
+    _source("odd_mixed_bc", split=4)
+    _, b = _source(name, split=16)
+    assert a == b
