@@ -30,6 +30,24 @@ def test_library_loads_and_exports_every_header_symbol():
     assert _lib.lib().smg_device_count() >= 0
 
 
+def test_ctypes_signatures_match_header_prototypes():
+    """Every prototype of include/starmap_gpu.h has a ctypes binding with the
+    same number of parameters, pointer parameters bound as pointers, and
+    void returns as None."""
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "starmap_gpu.h")).read(), flags=re.S)
+    protos = re.findall(r"^\s*((?:const\s+)?\w+\s*\**)\s*(smg_\w+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.M)
+    assert {p[1] for p in protos} == set(_lib.SIGNATURES)
+    for ret, name, args in protos:
+        restype, argtypes = _lib.SIGNATURES[name]
+        assert (ret.strip() == "void") == (restype is None), name
+        params = [] if args.strip() in ("", "void") else args.split(",")
+        assert len(params) == len(argtypes), name
+        for param, ct in zip(params, argtypes):
+            is_ptr = "*" in param or "[" in param
+            ct_ptr = ct in (ctypes.c_void_p, ctypes.c_char_p) or issubclass(ct, ctypes._Pointer)
+            assert is_ptr == ct_ptr, (name, param)
+
+
 def test_create_rejects_bad_descriptor():
     L = _lib.lib()
     p = _lib.smg_problem()
