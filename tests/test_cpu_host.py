@@ -48,6 +48,27 @@ def test_ctypes_signatures_match_header_prototypes():
             assert is_ptr == ct_ptr, (name, param)
 
 
+def test_ctypes_struct_layouts_match_the_c_compiler():
+    """smg_field and smg_problem: size and every member offset of the ctypes
+    mirror agree with the C compiler's layout of the header (static
+    assertions checked by gcc -fsyntax-only; nothing is written)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not present")
+    lines = ["#include <stddef.h>", '#include "starmap_gpu.h"']
+    for st in (_lib.smg_field, _lib.smg_problem):
+        name = st.__name__
+        lines.append(f'_Static_assert(sizeof({name}) == {ctypes.sizeof(st)}, "sizeof {name}");')
+        for fname, _ in st._fields_:
+            off = getattr(st, fname).offset
+            lines.append(f'_Static_assert(offsetof({name}, {fname}) == {off}, "{name}.{fname}");')
+    r = subprocess.run([gcc, "-fsyntax-only", "-x", "c", "-I", os.path.join(ROOT, "include"), "-"],
+                       input="\n".join(lines) + "\n", capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_create_rejects_bad_descriptor():
     L = _lib.lib()
     p = _lib.smg_problem()
