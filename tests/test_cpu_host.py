@@ -69,6 +69,20 @@ def test_ctypes_struct_layouts_match_the_c_compiler():
     assert r.returncode == 0, r.stderr
 
 
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
+def test_header_compiles_standalone(lang, std):
+    """A MEX gateway in plain C or any C++ host includes the header alone."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("compiler not present")
+    r = subprocess.run([cc, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-x", lang,
+                        "-I", os.path.join(ROOT, "include"), "-"],
+                       input='#include "starmap_gpu.h"\n', capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_create_rejects_bad_descriptor():
     L = _lib.lib()
     p = _lib.smg_problem()
