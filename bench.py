@@ -395,8 +395,8 @@ def run_reference(args, rank, world):
         "config": {"workload": WORKLOAD_NAME, "n_sys": n_sys, "cells": cells, "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"first {steps} of 321 steps after {warm} warm-up step(s); "
-                                   "GNU Octave (the reference runtime) is absent on this box, so the "
-                                   "oracle's C restatement of starmap_solver.m stands in"},
+                                   "the oracle's C restatement of starmap_solver.m stands in for the "
+                                   "reference, which is MATLAB/GNU Octave code this arm does not run"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
