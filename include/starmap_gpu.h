@@ -284,7 +284,11 @@ int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t 
 
 /* Grid-type classification of starmap_solver.m:76-98 from the sparsity of
  * par.Mx/My/Mz (column-major n_sys x n_sys): writes gt_out[3*j+d] in {1,2}.
- * Host-only helper for callers that do not classify themselves. */
+ * SMG_EINVAL when a component is not reached from component 1 (the
+ * reference's loop never ends there) or when a coupling along axis d joins
+ * components whose grid types differ in more than axis d (the reference would
+ * put a component on two grids).  Host-only helper for callers that do not
+ * classify themselves. */
 int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz,
                  int32_t* gt_out);
 

@@ -581,6 +581,18 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
     }
     if (assigned < n_sys)
         return fail(nullptr, SMG_EINVAL, "smg_classify: components not connected to component 1");
+    // every coupling along d must join grids that differ in axis d alone; the
+    // reference's set unions would put such a component on two grids at once
+    for (int j = 0; j < n_sys; ++j)
+        for (int d = 0; d < 3; ++d)
+            for (int i : I[d][j])
+                if (cls[i] != (cls[j] ^ (1 << d))) {
+                    char buf[160];
+                    std::snprintf(buf, sizeof buf,
+                                  "smg_classify: M%c(%d,%d) couples components that admit no staggered grid types",
+                                  "xyz"[d], j + 1, i + 1);
+                    return fail(nullptr, SMG_EINVAL, buf);
+                }
     for (int j = 0; j < n_sys; ++j)
         for (int d = 0; d < 3; ++d) gt_out[3 * j + d] = 1 + ((cls[j] >> d) & 1);
     return SMG_OK;

@@ -150,6 +150,19 @@ def test_native_classification_matches_oracle(cl, N, dim):
     np.testing.assert_array_equal(gt, np.stack([gx, gy, gz], 1))
 
 
+def test_classification_refuses_unstaggerable_couplings():
+    """Component 3 reached from component 1 along y (grid 1,2) and, through
+    component 2, along x twice (grid 1,1): no staggered grid types exist, and
+    the classification says so instead of picking one."""
+    Mx = np.array([[0., 1, 0], [1, 0, 1], [0, 1, 0]])
+    My = np.array([[0., 0, 1], [0, 0, 0], [1, 0, 0]])
+    Mz = np.zeros((3, 3))
+    with pytest.raises(_lib.SmgError, match="admit no staggered grid types"):
+        _lib.classify(Mx, My, Mz)
+    with pytest.raises(_lib.SmgError, match="not connected"):
+        _lib.classify(np.zeros((2, 2)), np.zeros((2, 2)), np.zeros((2, 2)))
+
+
 def test_phase_partition_counts():
     # component sets of the benchmark configurations
     def counts(N, dim):
