@@ -114,6 +114,8 @@ int smg_set_device(int32_t device);
  * 2^30, and one component's padded slot (the points of the first kernel axis
  * rounded up to 8, times those of the other two, faces included) below 2^31
  * points, since the kernels index a point with 32 bits; else SMG_EINVAL.
+ * Every coupling M_d(j,i) != 0 must join grid types that differ in axis d
+ * alone (as smg_classify assigns them); else SMG_EINVAL.
  * Replaces: starmap_solver.m:136-157 (field allocation) on the device side. */
 int smg_create(const smg_problem* p, smg_handle** out);
 

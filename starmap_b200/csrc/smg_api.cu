@@ -710,6 +710,13 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device) {
                 int eD[3];
                 int gflip[3] = {p->gt[3 * i], p->gt[3 * i + 1], p->gt[3 * i + 2]};
                 gflip[d] = 3 - gi;
+                if (gflip[0] != p->gt[3 * j] || gflip[1] != p->gt[3 * j + 1] || gflip[2] != p->gt[3 * j + 2]) {
+                    delete h;
+                    char buf[160];
+                    std::snprintf(buf, sizeof buf, "gt: coupling M%c(%d,%d) needs grids that differ in axis %c alone",
+                                  "xyz"[d], j + 1, i + 1, "xyz"[d]);
+                    return fail(nullptr, SMG_EINVAL, buf);
+                }
                 grid_extents(h, gflip, eD);
                 if (eD[0] != c.ext[0] || eD[1] != c.ext[1] || eD[2] != c.ext[2]) {
                     delete h;

@@ -59,3 +59,16 @@ def test_generator_refuses_state_beyond_32bit_offsets():
     big = [1, 7800, 7800]
     with pytest.raises(_lib.SmgError, match="32-bit element offsets"):
         jit_source(big, S.bc, S.h, S.gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
+
+
+def test_create_refuses_grid_types_inconsistent_with_the_couplings():
+    """With periodic boundaries every grid has the same extents, so only the
+    grid types show a wrong gt: a component moved to another grid is refused."""
+    import numpy as np
+    from starmap_b200 import configs
+    S = prepare(starmap_init(configs.linesource(n=20, n_mom=3, tfinal=0.1)))
+    T = _tables(S, first_step(S))
+    gt = np.array(S.gt, dtype=np.int32).reshape(S.n_sys, 3).copy()
+    gt[1, 2] = 3 - gt[1, 2]
+    with pytest.raises(_lib.SmgError, match="differ in axis"):
+        jit_source(S.n, S.bc, S.h, gt, S.Mx, S.My, S.Mz, T.fields, **handle_tables(S, T))
