@@ -1,8 +1,10 @@
 """The generated kernels compile for every problem structure: hypothesis
 draws small problems (closure and order, odd and unequal sizes, per-axis
 boundary conditions, field or scalar coefficients, filter position) and the
-generated source -- plain and family (batched) forms -- must compile with
-NVRTC for sm_100a (no GPU needed)."""
+generated source -- plain, family (batched) and adjoint forms -- must compile
+with NVRTC for sm_100a (no GPU needed).  Descriptors the generator cannot
+serve (state beyond 32-bit offsets, grid types inconsistent with the
+couplings) are refused on the host."""
 import pytest
 from hypothesis import HealthCheck, given, settings
 
