@@ -15,7 +15,9 @@
  * Conventions
  *   - Every entry point returns SMG_OK (0) or a negative SMG_E* code; the
  *     message of the last failure on a handle is smg_last_error(handle), and
- *     of a failed smg_create / handle-less call smg_last_error(NULL).
+ *     of a failed smg_create / handle-less call smg_last_error(NULL).  The
+ *     handle-less message is kept per host thread: the pointer stays valid
+ *     until the same thread's next handle-less failure.
  *   - Arrays follow MATLAB's column-major order.  Component j lives on the
  *     staggered grid gt[3*j+d] (1 = cell centres, 2 = staggered points) and
  *     has extent n[d] along solver dimension d, or n[d]+1 when gt == 2 and
@@ -277,8 +279,10 @@ int smg_state_sumsq(smg_handle* h, double* sumsq);
  * cudaStream_t (NULL: the default stream).  The partial sums live in a fixed
  * 256 KB array inside the library, resident on every GPU that loads it, so
  * ncomp is limited to 1024 (larger requests return SMG_EINVAL).  The first
- * call on a device looks up that array's device address, so make it before
- * any stream capture on that device.  All calls share the array: calls whose
+ * call on a device looks up that array's device address, and so does the
+ * first call after the device's context was reset (cudaDeviceReset, MATLAB's
+ * reset(gpuDevice)), since the array may then live elsewhere: make those
+ * calls before any stream capture on that device.  All calls share the array: calls whose
  * GPU work overlaps (different streams or threads) race on it.  The message
  * of a failed call is smg_last_error(NULL). */
 int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t len, double* d_out,

@@ -12,7 +12,6 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -25,16 +24,14 @@ using smg::DevField;
 
 namespace {
 
-std::mutex g_err_mu;
-std::string g_err;   // last handle-less failure
+// last handle-less failure of the calling thread: smg_last_error(NULL)
+// returns a pointer into it that stays valid until that thread's next
+// handle-less failure, whatever other threads do meanwhile
+thread_local std::string g_err;
 
 int fail(smg_handle* h, int code, const std::string& msg) {
-    if (h) {
-        h->err = msg;
-    } else {
-        std::lock_guard<std::mutex> lk(g_err_mu);
-        g_err = msg;
-    }
+    if (h) h->err = msg;
+    else g_err = msg;
     return code;
 }
 
@@ -532,7 +529,6 @@ const char* smg_version(void) { return "starmap_b200 0.1 (sm_100a, fp64)"; }
 
 const char* smg_last_error(const smg_handle* h) {
     if (h) return h->err.c_str();
-    std::lock_guard<std::mutex> lk(g_err_mu);
     return g_err.c_str();
 }
 

@@ -95,11 +95,46 @@ static __device__ __align__(256) double g_sumsq_scratch[kNoAllocScratch];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
+// per device: the array's address and the context it belongs to.  A device
+// reset (cudaDeviceReset, MATLAB's reset(gpuDevice)) destroys the context and
+// unloads the module; the next context loads it again, possibly at another
+// address, so the address is looked up again whenever the context changes.
 double* g_scratch_addr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};
 
 int noalloc_fail(int code, const std::string& m) {
     smg::set_global_error(m);   // read back with smg_last_error(NULL)
     return code;
+}
+
+// Unique id of the calling thread's current context (cuCtxGetId, reached
+// through the runtime's driver entry points, so the library needs no link to
+// libcuda); 0 when there is none yet or the driver lacks the call.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+
+unsigned long long current_ctx_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {   // under g_scratch_mu
+        looked = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+            get_id = reinterpret_cast<CtxGetIdFn>(f2);
+        }
+    }
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx) return 0;
+    if (get_id(ctx, &id) != 0) return 0;
+    return id;
 }
 
 }  // namespace
@@ -119,15 +154,20 @@ extern "C" int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t strid
     if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: device index too large");
     double* scratch;
     {
-        // first call on this device (with it current): look up the device
-        // address of the static array; host code cannot use the symbol itself
+        // first call on this device, or in a new context of it (with it
+        // current): look up the device address of the static array; host code
+        // cannot use the symbol itself.  Without a context id (no current
+        // context yet, or a driver without cuCtxGetId) it is looked up on
+        // every call.
         std::lock_guard<std::mutex> lk(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
+        const unsigned long long ctx = current_ctx_id();
+        if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_sumsq_scratch);
             if (e != cudaSuccess)
                 return noalloc_fail(SMG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             g_scratch_addr[dev] = static_cast<double*>(p);
+            g_scratch_ctx[dev] = ctx ? ctx : current_ctx_id();   // the lookup may have created the context
         }
         scratch = g_scratch_addr[dev];
     }

@@ -4,9 +4,10 @@ Such a host (for example a MATLAB MEX gateway that only holds gpuArray buffers
 owned by MATLAB's allocator) passes its own device input and output buffers;
 the library keeps the partial sums in a fixed array of its own instead of
 allocating.  The result must equal the ordinary, allocating reduction
-(smg_state_sumsq) on the same data, on consecutive calls that reuse the
-array.  Device buffers for the test are made with torch; the entry point
-itself allocates nothing."""
+(smg_state_sumsq) on the same data, and numpy's sum of squares on the host for
+vectors with gaps between them, on consecutive calls that reuse the array.
+Device buffers for the test are made with torch; the entry point itself
+allocates nothing."""
 import ctypes
 
 import numpy as np
@@ -60,6 +61,30 @@ def test_noalloc_sumsq_matches_allocating_reduction():
             assert np.all(np.abs(got - ref) <= REL_TOL * np.abs(ref)), (call, got, ref)
     finally:
         solver.close()
+
+
+def test_noalloc_sumsq_strided_vs_host_sum():
+    """Vectors with gaps between them (stride > len): only the first len values
+    of each vector count.  The gaps hold NaN and huge values, which would show
+    in the result if they were read.  Checked against numpy's sum of squares on
+    the host, on two calls in a row with different sizes."""
+    torch = pytest.importorskip("torch")
+    L = _lib.lib()
+    rng = np.random.default_rng(9)
+    for call, (ncomp, length, stride) in enumerate(((37, 5001, 5120), (1024, 777, 800))):
+        host = np.full((ncomp, stride), np.nan)
+        host[:, length + 1:] = 1e300
+        host[:, :length] = rng.standard_normal((ncomp, length)) * (call + 1)
+        x = torch.from_numpy(host).to("cuda")
+        out = torch.full((ncomp,), float("nan"), dtype=torch.float64, device="cuda")
+        rc = L.smg_sumsq_noalloc(ctypes.c_void_p(x.data_ptr()), ncomp, stride, length,
+                                 ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == _lib.SMG_OK, L.smg_last_error(None)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        ref = np.sum(host[:, :length] * host[:, :length], axis=1)
+        assert np.all(np.isfinite(got)), call
+        assert np.all(np.abs(got - ref) <= REL_TOL * ref), (call, np.max(np.abs(got - ref) / ref))
 
 
 def test_noalloc_sumsq_rejects_too_many_components():
