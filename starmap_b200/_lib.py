@@ -37,6 +37,10 @@ SMG_TUNE_JIT_PREFETCH = 12
 SMG_TUNE_JIT_BAND = 13
 SMG_TUNE_JIT_CONST = 14
 SMG_TUNE_GRAPH_STEPS = 15
+SMG_TUNE_JIT_STAGED = 16
+SMG_TUNE_JIT_SLICES = 17
+SMG_TUNE_JIT_STAGES = 18
+SMG_TUNE_JIT_ROWS = 19
 
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1

@@ -900,7 +900,11 @@ int smg_set_state(smg_handle* h, const double* const* U) {
 
 int smg_get_state(smg_handle* h, double* const* U) {
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_state: NULL argument");
-    return staged_transfer(h, false, nullptr, U, nullptr, 0.0, 0.0);
+    const int rc = staged_transfer(h, false, nullptr, U, nullptr, 0.0, 0.0);
+    if (rc == SMG_OK && smg::jit_status(h) == SMG_ETIMEOUT)
+        return fail(h, SMG_ETIMEOUT,
+                    "smg_get_state: a staged kernel's shared-memory pipeline wait ran out (state undefined)");
+    return rc;
 }
 
 int smg_snapshot(smg_handle* h) {
@@ -1358,6 +1362,30 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             smg::jit_free(h);
             h->jit_failed = false;
             break;
+        case SMG_TUNE_JIT_STAGED:
+            if (value < -1 || value > 1) return fail(h, SMG_EINVAL, "smg_tune: jit staged must be -1, 0 or 1");
+            h->jit_staged = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_SLICES:
+            if (value < 1 || value > 16) return fail(h, SMG_EINVAL, "smg_tune: jit slices must be 1..16");
+            h->jit_slices = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_STAGES:
+            if (value < 2 || value > 6) return fail(h, SMG_EINVAL, "smg_tune: jit stages must be 2..6");
+            h->jit_stages = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
+        case SMG_TUNE_JIT_ROWS:
+            if (value < 0 || value > (1 << 30)) return fail(h, SMG_EINVAL, "smg_tune: jit rows must be 0..2^30");
+            h->jit_rows = value;
+            smg::jit_free(h);
+            h->jit_failed = false;
+            break;
         case SMG_TUNE_GRAPH_STEPS:
             if (value < -1 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: graph steps must be -1..4096");
             h->graph_block = value;
@@ -1387,8 +1415,12 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap) 
     else v = SMG_VARIANT_GENERIC;
     *variant = v;
     if (why && cap > 0) {
-        const size_t n = std::min<size_t>((size_t)cap - 1, h->jit_err.size());
-        std::memcpy(why, h->jit_err.data(), n);
+        // with the generated kernels active: their form; otherwise why AUTO could not use them
+        const std::string m = v == SMG_VARIANT_JIT
+                                  ? (smg::jit_staged_active(h) ? "bulk-staged" : "register")
+                                  : h->jit_err;
+        const size_t n = std::min<size_t>((size_t)cap - 1, m.size());
+        std::memcpy(why, m.data(), n);
         why[n] = '\0';
     }
     return SMG_OK;
@@ -1420,6 +1452,8 @@ int smg_set_variant(smg_handle* h, int32_t variant) {
 int smg_sync(smg_handle* h) {
     if (!h) return fail(h, SMG_EINVAL, "smg_sync: NULL handle");
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (smg::jit_status(h) == SMG_ETIMEOUT)
+        return fail(h, SMG_ETIMEOUT, "smg_sync: a staged kernel's shared-memory pipeline wait ran out (state undefined)");
     return SMG_OK;
 }
 

@@ -98,7 +98,9 @@ struct Api {
     CUresult_t (*ModuleGetFunction)(CUfunction_t*, CUmodule_t, const char*) = nullptr;
     CUresult_t (*LaunchKernel)(CUfunction_t, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                cudaStream_t, void**, void**) = nullptr;
+    CUresult_t (*FuncSetAttribute)(CUfunction_t, int, int) = nullptr;
 };
+constexpr int kFuncAttrMaxDynamicSmem = 8;   // CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES
 
 Api g_api;
 std::once_flag g_api_once;
@@ -164,7 +166,8 @@ void load_api() {
     if (!cu) {
         a.cu_why = "CUDA driver library (libcuda.so.1) not found";
     } else if (sym(cu, "cuModuleLoadData", a.ModuleLoadData) && sym(cu, "cuModuleUnload", a.ModuleUnload) &&
-               sym(cu, "cuModuleGetFunction", a.ModuleGetFunction) && sym(cu, "cuLaunchKernel", a.LaunchKernel)) {
+               sym(cu, "cuModuleGetFunction", a.ModuleGetFunction) && sym(cu, "cuLaunchKernel", a.LaunchKernel) &&
+               sym(cu, "cuFuncSetAttribute", a.FuncSetAttribute)) {
         a.cu_ok = true;
     } else {
         a.cu_why = "CUDA driver entry points missing";
@@ -299,6 +302,64 @@ static __device__ __forceinline__ double dwdu(int M, double s, double E, double 
     if (M == 1) return F1 * hdt * E;
     const double r = 1.0 - hdt * s * E;
     return F2 * hdt * E * (r * F1 + 1.0);
+}
+)";
+
+// Helpers of the bulk-staged kernels: mbarriers in shared memory, the bulk
+// copy engine (cp.async.bulk, global -> this CTA's shared memory, completion
+// counted in bytes on an mbarrier; no cluster multicast), and bounded waits.
+const char* kStagePrelude = R"(
+static __device__ __forceinline__ unsigned sa(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+static __device__ __forceinline__ void mb_init(unsigned long long* b, unsigned n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(sa(b)), "r"(n) : "memory");
+}
+static __device__ __forceinline__ void mb_expect(unsigned long long* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(sa(b)), "r"(bytes) : "memory");
+}
+static __device__ __forceinline__ void mb_arrive(unsigned long long* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(sa(b)) : "memory");
+}
+static __device__ __forceinline__ bool mb_try(unsigned long long* b, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(sa(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+static __device__ __forceinline__ unsigned long long gtime() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// wait for the phase of parity `parity` to complete; false after 4 s (the
+// caller records the failure in the error flag and stops)
+static __device__ __forceinline__ bool mb_wait(unsigned long long* b, unsigned parity) {
+    if (mb_try(b, parity)) return true;
+    const unsigned long long t0 = gtime();
+    for (unsigned n = 1;; ++n) {
+        if (mb_try(b, parity)) return true;
+        if ((n & 255u) == 0 && gtime() - t0 > 4000000000ull) return false;
+    }
+}
+static __device__ __forceinline__ void bulk_ld(double* dst, const double* src, unsigned bytes, unsigned long long* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(sa(dst)), "l"(src), "r"(bytes), "r"(sa(b)) : "memory");
+}
+static __device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+// the four values of an x difference for a point pair: from two aligned
+// 128-bit shared loads in the interior (pattern A: stencil (p, p-1), B:
+// (p+1, p)), from shared memory at the stencil offsets where the stencil
+// clamps, or from global memory where it wraps out of the staged window
+static __device__ __forceinline__ void xvals(int patA, const double* s, const double* g, bool xf, bool xw, int h0,
+                                             int l0, int h1, int l1, double& a0, double& b0, double& a1, double& b1) {
+    if (xf) {
+        const double2 P = lds2(s);
+        if (patA) { const double2 Q = lds2(s - 2); a0 = P.x; b0 = Q.y; a1 = P.y; b1 = P.x; }
+        else { const double2 R = lds2(s + 2); a0 = P.y; b0 = P.x; a1 = R.x; b1 = P.y; }
+    } else if (xw) {
+        a0 = s[h0]; b0 = s[l0]; a1 = s[h1]; b1 = s[l1];
+    } else {
+        a0 = __ldg(g + h0); b0 = __ldg(g + l0); a1 = __ldg(g + h1); b1 = __ldg(g + l1);
+    }
 }
 )";
 
@@ -1004,11 +1065,399 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
     o += "    }\n}\n";
 }
 
-// One generated kernel: its program, phase type, name and CTA count.
+// ---- bulk-staged kernels -----------------------------------------------------
+// The register form above loads every source value with a global load at its
+// first use, so each warp waits on DRAM several times per group and the loads
+// in flight are bounded by the registers that hold them.  In the staged form a
+// CTA owns one group, a 64-point chunk of a row and a band of rows; one
+// producer thread copies, for each row of the band, every row segment the
+// group reads (its destinations, the array coefficients, the x sources with
+// two points either side, both neighbouring rows of every y/z source) into a
+// ring of shared-memory stages with the bulk copy engine (cp.async.bulk,
+// completion counted in bytes on an mbarrier), up to `stages` rows ahead of
+// the consumers; consumer warps (the group's destinations split into slices,
+// one warp per slice, a lane per point pair) fold the couplings from shared
+// memory with the register form's arithmetic and store their destinations.
+// Copies are in flight without holding registers, and the register budget is
+// no longer split with the loads.  All waits are bounded (4 s): a wait that
+// runs out sets the kernel's error flag and ends the CTA.
+constexpr int kStW = 64;      // points of a row per CTA: 32 lanes x 2
+constexpr int kStSlot = 68;   // doubles per staged row segment: the chunk and 2 points either side
+
+struct StagedRows {
+    std::vector<int> coefs;                     // array fields read by the group
+    std::vector<std::pair<int, int>> xs;        // (source, g2) of x differences
+    std::vector<std::tuple<int, int, int>> yz;  // (axis, source, g2): two slots (hi row, lo row)
+    int nd = 0;                                 // destinations (slots 0..nd-1)
+    int slot_coef(int f) const { return nd + (int)(std::find(coefs.begin(), coefs.end(), f) - coefs.begin()); }
+    int slot_x(int src) const {
+        for (size_t i = 0; i < xs.size(); ++i)
+            if (xs[i].first == src) return nd + (int)coefs.size() + (int)i;
+        return -1;
+    }
+    int slot_yz(int a, int src) const {
+        for (size_t i = 0; i < yz.size(); ++i)
+            if (std::get<0>(yz[i]) == a && std::get<1>(yz[i]) == src)
+                return nd + (int)coefs.size() + (int)xs.size() + 2 * (int)i;
+        return -1;
+    }
+    int nslots() const { return nd + (int)coefs.size() + (int)xs.size() + 2 * (int)yz.size(); }
+};
+
+StagedRows staged_rows(const smg_handle* h, int phase, const std::vector<int>& D, const std::vector<int>& P) {
+    StagedRows R;
+    R.nd = (int)P.size();
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    for (int p : P) {
+        const Coefs f = coefs_of(h, phase, D[p]);
+        std::vector<int> fl = {f.q, f.s, f.E};
+        if (filt) fl.insert(fl.end(), {f.F1, f.F2});
+        for (int fi : fl)
+            if (is_array(h, fi) && std::find(R.coefs.begin(), R.coefs.end(), fi) == R.coefs.end())
+                R.coefs.push_back(fi);
+    }
+    for (int p : P) {
+        const smg::DevComp& c = h->comps[D[p]];
+        for (int q = c.cbeg; q < c.cend; ++q) {
+            const smg::DevCoup& cp = h->coups[q];
+            const int a = cp.code >> 1, g2 = cp.code & 1;
+            if (a == 0) {
+                if (R.slot_x(cp.src) < 0) R.xs.push_back({cp.src, g2});
+            } else if (R.slot_yz(a, cp.src) < 0) {
+                R.yz.push_back(std::make_tuple(a, cp.src, g2));
+            }
+        }
+    }
+    return R;
+}
+
+std::string staged_group_name(int phase, int k) { return "smg_s" + std::to_string(phase) + "_" + std::to_string(k); }
+
+// One group of the staged form: producer and consumers over the rows of the
+// CTA's band.  P: positions into the phase's destination list; ns consumer
+// warps (slices); st ring stages of `stage` doubles; rb rows per band.
+void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, int ns,
+                       int st, int rb, long long stage) {
+    const smg::DevGrid& g = h->g;
+    const std::vector<int> D = phase_dests(h, phase);
+    const StagedRows R = staged_rows(h, phase, D, P);
+    const smg::DevComp& c0 = h->comps[D[P[0]]];
+    const int E0 = c0.ext[0], E1 = c0.ext[1], E2 = c0.ext[2];
+    const long long nrows = (long long)E1 * E2;
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    const char* an[3] = {"x", "y", "z"};
+    char b[4096];
+    bool used_g2[3][2] = {{false, false}, {false, false}, {false, false}};
+    for (int p : P)
+        for (int q = h->comps[D[p]].cbeg; q < h->comps[D[p]].cend; ++q)
+            used_g2[h->coups[q].code >> 1][h->coups[q].code & 1] = true;
+    std::snprintf(b, sizeof b,
+                  "static __device__ __forceinline__ void %s(double* __restrict__ U, const DevField* __restrict__ F, "
+                  "double hdt, int kf, int mode, int* err, double* smem, int chunk, int band) {\n"
+                  "    (void)hdt; (void)kf; (void)mode; (void)F;\n"
+                  "    const int c0 = chunk * %d;\n"
+                  "    if (c0 >= %d) return;\n"
+                  "    const int q0 = band * %d;\n"
+                  "    if (q0 >= %lld) return;\n"
+                  "    const int q1 = q0 + %d < %lld ? q0 + %d : %lld;\n"
+                  "    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);\n"
+                  "    double* sm = smem + 16;\n"
+                  "    if (threadIdx.x == 0) {\n"
+                  "        for (int s = 0; s < %d; ++s) { mb_init(&bar[s], 1); mb_init(&bar[%d + s], %d); }\n"
+                  "        asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\");\n"
+                  "        asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
+                  "    }\n"
+                  "    __syncthreads();\n"
+                  "    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);\n",
+                  staged_group_name(phase, k).c_str(), kStW, E0, rb, nrows, rb, nrows, rb, nrows, st, st, ns);
+    o += b;
+    // ---- producer: one thread
+    const int nx = (int)R.xs.size();
+    const int nother = R.nd + (int)R.coefs.size() + 2 * (int)R.yz.size();
+    std::snprintf(b, sizeof b,
+                  "    if (warp == %d) {\n"
+                  "        if (lane != 0) return;\n"
+                  "        const int xl = c0 - 2 < 0 ? 0 : c0 - 2, xr = c0 + %d < %lld ? c0 + %d : %lld;\n"
+                  "        const unsigned xb = (unsigned)(xr - xl) * 8u;\n"
+                  "        const int xo = xl - (c0 - 2);\n"
+                  "        const unsigned db = (unsigned)((c0 + %d < %lld ? c0 + %d : %lld) - c0) * 8u;\n"
+                  "        const unsigned tx = %du * xb + %du * db;\n"
+                  "        (void)xo; (void)xb;\n"
+                  "        for (int q = q0, it = 0; q < q1; ++q, ++it) {\n"
+                  "            const int s = it %% %d;\n"
+                  "            if (it >= %d && !mb_wait(&bar[%d + s], ((it / %d) & 1) ^ 1)) { atomicExch(err, 1); return; }\n"
+                  "            const int y = q %% %d, z = q / %d;\n"
+                  "            const double* Ur = U + ((long long)z * %lld + (long long)y * %lld);\n"
+                  "            double* stg = sm + (long long)s * %lld;\n",
+                  ns, kStW + 2, (long long)g.s1, kStW + 2, (long long)g.s1, kStW, (long long)g.s1, kStW,
+                  (long long)g.s1, nx, nother, st, st, st, st, E1, E1, (long long)g.s2, (long long)g.s1, stage);
+    o += b;
+    for (int a = 1; a < 3; ++a)
+        for (int g2 = 0; g2 < 2; ++g2) {
+            if (!used_g2[a][g2]) continue;
+            const long long stv = a == 1 ? g.s1 : g.s2;
+            const char* pv = a == 1 ? "y" : "z";
+            std::snprintf(b, sizeof b,
+                          "            long long h%s_%d, l%s_%d;\n"
+                          "            { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); h%s_%d = (long long)(hi - %s) * %lld; "
+                          "l%s_%d = (long long)(lo - %s) * %lld; }\n",
+                          an[a], g2, an[a], g2, pv, g.n[a], g.bc[a], g2, an[a], g2, pv, stv, an[a], g2, pv, stv);
+            o += b;
+        }
+    o += "            mb_expect(&bar[s], tx);\n";
+    for (int i = 0; i < R.nd; ++i) {
+        std::snprintf(b, sizeof b, "            bulk_ld(stg + %d, Ur + %lld + c0, db, &bar[s]);\n", i * kStSlot + 2,
+                      (long long)D[P[i]] * g.cs);
+        o += b;
+    }
+    for (size_t i = 0; i < R.coefs.size(); ++i) {
+        std::snprintf(b, sizeof b, "            bulk_ld(stg + %d, fp(F, %d) + (Ur - U) + c0, db, &bar[s]);\n",
+                      R.slot_coef(R.coefs[i]) * kStSlot + 2, R.coefs[i]);
+        o += b;
+    }
+    for (const auto& xsrc : R.xs) {
+        std::snprintf(b, sizeof b, "            bulk_ld(stg + %d + xo, Ur + %lld + xl, xb, &bar[s]);\n",
+                      R.slot_x(xsrc.first) * kStSlot, (long long)xsrc.first * g.cs);
+        o += b;
+    }
+    for (const auto& t : R.yz) {
+        const int a = std::get<0>(t), src = std::get<1>(t), g2 = std::get<2>(t);
+        const int sl = R.slot_yz(a, src);
+        std::snprintf(b, sizeof b,
+                      "            bulk_ld(stg + %d, Ur + %lld + h%s_%d + c0, db, &bar[s]);\n"
+                      "            bulk_ld(stg + %d, Ur + %lld + l%s_%d + c0, db, &bar[s]);\n",
+                      sl * kStSlot + 2, (long long)src * g.cs, an[a], g2, (sl + 1) * kStSlot + 2,
+                      (long long)src * g.cs, an[a], g2);
+        o += b;
+    }
+    o += "        }\n        return;\n    }\n";
+    // ---- consumers: per-thread x stencil offsets, fixed over the band
+    std::snprintf(b, sizeof b,
+                  "    const int x0 = c0 + 2 * lane, x1 = x0 + 1;\n"
+                  "    const bool act = x0 < %d, v1 = x1 < %d;\n"
+                  "    (void)v1;\n",
+                  E0, E0);
+    o += b;
+    for (int g2 = 0; g2 < 2; ++g2) {
+        if (!used_g2[0][g2]) continue;
+        const bool pa = xpattern_a(g2, g.bc[0]);
+        std::snprintf(b, sizeof b,
+                      "    int hx0_%d = 0, lx0_%d = 0, hx1_%d = 0, lx1_%d = 0;\n"
+                      "    if (act) {\n"
+                      "        int hi, lo; stencil(x0, %d, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
+                      "        if (v1) { stencil(x1, %d, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n"
+                      "    }\n"
+                      "    const bool xf_%d = act && v1 && hx0_%d == %d && lx0_%d == %d && hx1_%d == %d && lx1_%d == %d;\n"
+                      "    const bool xw_%d = hx0_%d >= -2 && hx0_%d <= 3 && lx0_%d >= -2 && lx0_%d <= 3 && "
+                      "hx1_%d >= -2 && hx1_%d <= 3 && lx1_%d >= -2 && lx1_%d <= 3;\n",
+                      g2, g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2, g2, g2, pa ? 0 : 1, g2,
+                      pa ? -1 : 0, g2, pa ? 1 : 2, g2, pa ? 0 : 1, g2, g2, g2, g2, g2, g2, g2, g2, g2);
+        o += b;
+    }
+    std::snprintf(b, sizeof b,
+                  "    for (int q = q0, it = 0; q < q1; ++q, ++it) {\n"
+                  "        const int s = it %% %d;\n"
+                  "        if (!mb_wait(&bar[s], (it / %d) & 1)) { atomicExch(err, 1); return; }\n"
+                  "        const int y = q %% %d, z = q / %d;\n"
+                  "        const int pt = z * %lld + y * %lld + x0;\n"
+                  "        const double* st = sm + (long long)s * %lld + 2 + 2 * lane;\n"
+                  "        (void)pt;\n"
+                  "        if (act) {\n"
+                  "        switch (warp) {\n",
+                  st, st, E1, E1, (long long)g.s2, (long long)g.s1, stage);
+    o += b;
+    // slices: contiguous runs of the group's destinations (the group order
+    // puts destinations that share sources next to each other)
+    const int G = (int)P.size();
+    for (int w = 0; w < ns; ++w) {
+        const int p0 = (int)((long long)G * w / ns), p1 = (int)((long long)G * (w + 1) / ns);
+        if (p0 >= p1) continue;
+        o += "        case " + std::to_string(w) + ": {\n";
+        std::set<int> coef_done;
+        std::set<std::pair<int, int>> val_done;
+        auto coef = [&](int f) {
+            const std::string n = "C" + std::to_string(f);
+            if (coef_done.insert(f).second) {
+                if (is_array(h, f)) std::snprintf(b, sizeof b, "            const double2 %s = lds2(st + %d);\n", n.c_str(),
+                                                  R.slot_coef(f) * kStSlot);
+                else std::snprintf(b, sizeof b, "            const double %s = fs(F, %d);\n", n.c_str(), f);
+                o += b;
+            }
+            return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
+        };
+        for (int pi = p0; pi < p1; ++pi) {
+            const int j = D[P[pi]];
+            const smg::DevComp& c = h->comps[j];
+            const Coefs f = coefs_of(h, phase, j);
+            const auto q = coef(f.q), sv = coef(f.s), E = coef(f.E);
+            std::pair<std::string, std::string> k1{"1.0", "1.0"}, k2{"1.0", "1.0"};
+            if (filt) {
+                k1 = coef(f.F1);
+                k2 = coef(f.F2);
+            }
+            for (int qq = c.cbeg; qq < c.cend; ++qq) {
+                const smg::DevCoup& cp = h->coups[qq];
+                const int a = cp.code >> 1, g2 = cp.code & 1;
+                if (!val_done.insert({a, cp.src}).second) continue;
+                if (a == 0)
+                    std::snprintf(b, sizeof b,
+                                  "            double X%d_a0, X%d_b0, X%d_a1, X%d_b1;\n"
+                                  "            xvals(%d, st + %d, U + pt + %lld, xf_%d, xw_%d, hx0_%d, lx0_%d, hx1_%d, "
+                                  "lx1_%d, X%d_a0, X%d_b0, X%d_a1, X%d_b1);\n",
+                                  cp.src, cp.src, cp.src, cp.src, xpattern_a(g2, g.bc[0]) ? 1 : 0,
+                                  R.slot_x(cp.src) * kStSlot, (long long)cp.src * g.cs, g2, g2, g2, g2, g2, g2, cp.src,
+                                  cp.src, cp.src, cp.src);
+                else
+                    std::snprintf(b, sizeof b, "            const double2 %c%d_h = lds2(st + %d), %c%d_l = lds2(st + %d);\n",
+                                  a == 1 ? 'Y' : 'Z', cp.src, R.slot_yz(a, cp.src) * kStSlot, a == 1 ? 'Y' : 'Z', cp.src,
+                                  (R.slot_yz(a, cp.src) + 1) * kStSlot);
+                o += b;
+            }
+            std::snprintf(b, sizeof b,
+                          "            {\n"
+                          "                const double2 u = lds2(st + %d);\n"
+                          "                double SA = 0.0, SB = 0.0;\n",
+                          pi * kStSlot);
+            o += b;
+            bool first = true;
+            for (int qq = c.cbeg; qq < c.cend; ++qq) {
+                const smg::DevCoup& cp = h->coups[qq];
+                const int a = cp.code >> 1;
+                const int mode_div = h->exact_recip[a];
+                const std::string H = clit(g.h[a]), RH = clit(h->rh[a]), W = clit(cp.w);
+                const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
+                const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
+                first = false;
+                std::string dA, dB;
+                if (a == 0) {
+                    dA = "__dsub_rn(X" + std::to_string(cp.src) + "_a0, X" + std::to_string(cp.src) + "_b0)";
+                    dB = "__dsub_rn(X" + std::to_string(cp.src) + "_a1, X" + std::to_string(cp.src) + "_b1)";
+                } else {
+                    const std::string n = std::string(1, a == 1 ? 'Y' : 'Z') + std::to_string(cp.src);
+                    dA = "__dsub_rn(" + n + "_h.x, " + n + "_l.x)";
+                    dB = "__dsub_rn(" + n + "_h.y, " + n + "_l.y)";
+                }
+                std::snprintf(b, sizeof b,
+                              "                { const double tA = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                              "                  const double tB = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                              "                  %s }\n",
+                              dv, dA.c_str(), H.c_str(), RH.c_str(), W.c_str(), dv, dB.c_str(), H.c_str(), RH.c_str(),
+                              W.c_str(), fold);
+                o += b;
+            }
+            o += "                double u0 = u.x, u1 = u.y;\n";
+            auto sub = [&]() {
+                std::snprintf(b, sizeof b, "u0 = upd(u0, -SA, %s, %s, %s, hdt); u1 = upd(u1, -SB, %s, %s, %s, hdt);",
+                              q.first.c_str(), sv.first.c_str(), E.first.c_str(), q.second.c_str(), sv.second.c_str(),
+                              E.second.c_str());
+                return std::string(b);
+            };
+            auto fl = [&](const std::pair<std::string, std::string>& Fp) {
+                return filt ? " u0 = __dmul_rn(u0, " + Fp.first + "); u1 = __dmul_rn(u1, " + Fp.second + ");"
+                            : std::string();
+            };
+            if (phase == 0) {
+                const std::string one =
+                    "                " + sub() +
+                    (filt ? " u0 = __dmul_rn(u0, kf == 1 ? " + k1.first + " : " + k2.first +
+                                "); u1 = __dmul_rn(u1, kf == 1 ? " + k1.second + " : " + k2.second + ");"
+                          : std::string()) +
+                    "\n";
+                const std::string two = "                " + sub() + fl(k2) + "\n                " + sub() + fl(k1) + "\n";
+                if (h->filter_mode == SMG_FILTER_FULL) o += one;
+                else o += "                if (mode == 0) {\n" + one + "                } else {\n" + two + "                }\n";
+            } else {
+                o += "                " + sub() + fl(k1) + "\n                " + sub() + fl(k2) + "\n";
+            }
+            std::snprintf(b, sizeof b,
+                          "                double* Uj = U + pt + %lld;\n"
+                          "                if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1); else *Uj = u0;\n"
+                          "            }\n",
+                          (long long)j * g.cs);
+            o += b;
+        }
+        o += "        } break;\n";
+    }
+    o += "        default: break;\n        }\n        }\n"
+         "        __syncwarp();\n"
+         "        if (lane == 0) mb_arrive(&bar[" + std::to_string(st) + " + s]);\n"
+         "    }\n}\n";
+}
+
+// Shape of the staged kernels of a handle.
+struct StagedShape {
+    int ns, st, nch, rb;
+    long long nb;
+};
+
+StagedShape staged_shape(const smg_handle* h, int ngroups_phase) {
+    const smg::DevGrid& g = h->g;
+    StagedShape S;
+    S.ns = h->jit_slices;
+    S.st = h->jit_stages;
+    S.nch = (g.B[0] + kStW - 1) / kStW;
+    const long long rows = (long long)g.B[1] * g.B[2];
+    if (h->jit_rows > 0) {
+        S.rb = (int)std::min<long long>(h->jit_rows, rows);
+    } else {
+        // about eight waves of two CTAs per SM over the phase's (group, chunk) columns
+        const long long cols = std::max(1LL, (long long)ngroups_phase * S.nch);
+        S.rb = (int)std::max(1LL, std::min(rows, (rows * cols + 2367) / 2368));
+    }
+    S.nb = (rows + S.rb - 1) / S.rb;
+    return S;
+}
+
+// Whether the plain kernels take the staged form: SMG_TUNE_JIT_STAGED 1, or
+// -1 (default) for 2D problems; never with separately compiled groups, and
+// only when every group's ring fits in one CTA's shared memory.
+bool staged_form(const smg_handle* h) {
+    const int want = h->jit_staged;
+    if (want == 0 || h->jit_calls) return false;
+    if (want < 0 && !(h->g.B[2] == 1 && h->g.B[1] > 1)) return false;
+    for (int phase = 0; phase < 2; ++phase) {
+        const std::vector<int> D = phase_dests(h, phase);
+        if (D.empty()) continue;
+        for (const auto& P : shared_groups(h, phase, h->jit_group)) {
+            const long long smem = (16 + (long long)h->jit_stages * staged_rows(h, phase, D, P).nslots() * kStSlot) * 8;
+            if (smem > 227LL * 1024) return false;
+        }
+    }
+    return true;
+}
+
+// Kernel over staged groups [k0, k1) of one phase: CTA -> (band, group,
+// chunk), band-major, so that the CTAs running at one time cover the same
+// rows of every group and the sources they share are read from L2.
+void emit_staged_dispatch(std::string& o, int phase, int k0, int k1, const StagedShape& S, int minb,
+                          const std::string& name) {
+    char b[1024];
+    const int ngk = k1 - k0;
+    std::snprintf(b, sizeof b,
+                  "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s(double* __restrict__ U, "
+                  "const DevField* __restrict__ F, double hdt, int kf, int mode, double* WR, double* PR, int* err) {\n"
+                  "    extern __shared__ __align__(128) double smem_st[];\n"
+                  "    (void)WR; (void)PR;\n"
+                  "    const int bid = (int)blockIdx.x;\n"
+                  "    const int band = bid / %d, rest = bid - band * %d;\n"
+                  "    const int grp = %d + rest / %d, chunk = rest %% %d;\n"
+                  "    switch (grp) {\n",
+                  32 * (S.ns + 1), minb, name.c_str(), ngk * S.nch, ngk * S.nch, k0, S.nch, S.nch);
+    o += b;
+    for (int k = k0; k < k1; ++k)
+        o += "    case " + std::to_string(k) + ": " + staged_group_name(phase, k) +
+             "(U, F, hdt, kf, mode, err, smem_st, chunk, band); break;\n";
+    o += "    default: break;\n    }\n}\n";
+}
+
+// One generated kernel: its program, phase type, name, CTA count and, for the
+// staged form, CTA size and dynamic shared memory (0: the register form's).
 struct KernelSrc {
     std::string src, name;
     int phase;
     long long grid;
+    int block = 0;
+    int smem = 0;
 };
 
 // The generated code of one handle.
@@ -1053,6 +1502,31 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         const std::vector<std::vector<int>> G = shared_groups(h, phase, group);
         const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
+        if (!rec && staged_form(h)) {
+            const StagedShape S = staged_shape(h, ng);
+            for (int k0 = 0; k0 < ng; k0 += step) {
+                const int k1 = std::min(ng, k0 + step);
+                int slots = 1;
+                for (int j = k0; j < k1; ++j) slots = std::max(slots, staged_rows(h, phase, D, G[j]).nslots());
+                const long long stage = (long long)slots * kStSlot;
+                const long long smem = (16 + S.st * stage) * 8;
+                const int minb = (int)std::max(1LL, std::min(4LL, (227LL * 1024) / (smem + 1024)));
+                KernelSrc k{std::string(kPrelude) + kStagePrelude,
+                            "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
+                            S.nb * (k1 - k0) * S.nch};
+                k.block = 32 * (S.ns + 1);
+                k.smem = (int)smem;
+                ConstTable tab;
+                std::string body;
+                g_ctab = h->jit_const ? &tab : nullptr;
+                for (int j = k0; j < k1; ++j) emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage);
+                g_ctab = nullptr;
+                k.src += ctab_decl(tab) + body;
+                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name);
+                P.push_back(std::move(k));
+            }
+            continue;
+        }
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
             const int R = band_rows(h);
@@ -1537,12 +2011,15 @@ namespace smg {
 struct JitKernel {
     CUfunction_t fn = nullptr;
     long long grid = 0;
+    int block = 0;   // CTA size (0: the state's)
+    int smem = 0;    // dynamic shared memory (staged form)
 };
 
 struct JitState {
     std::vector<CUmodule_t> mods;
     std::vector<JitKernel> k[4];           // kernels of each phase type (adjoint: 2, 3 the steady forms)
     int block = 64;
+    int* dErr = nullptr;                   // error flag of the staged kernels (a bounded wait ran out)
     std::vector<cudaStream_t> side;        // concurrent kernels of a phase (inline layout)
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
@@ -1566,6 +2043,7 @@ void free_state(JitState*& J) {
     for (cudaStream_t st : J->side) cudaStreamDestroy(st);
     if (J->fork) cudaEventDestroy(J->fork);
     for (cudaEvent_t e : J->join) cudaEventDestroy(e);
+    if (J->dErr) cudaFree(J->dErr);
     if (api().cu_ok)
         for (CUmodule_t m : J->mods) api().ModuleUnload(m);
     delete J;
@@ -1625,8 +2103,16 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
         for (size_t i = 0; i < P.size(); ++i) {
             JitKernel k;
             k.grid = P[i].grid;
+            k.block = P[i].block;
+            k.smem = P[i].smem;
             if (a.ModuleGetFunction(&k.fn, J->mods[i], P[i].name.c_str()) != 0)
                 return fail("cuModuleGetFunction " + P[i].name);
+            if (k.smem > 48 * 1024 && a.FuncSetAttribute(k.fn, kFuncAttrMaxDynamicSmem, k.smem) != 0)
+                return fail("cuFuncSetAttribute " + P[i].name + " (" + std::to_string(k.smem) + " bytes of shared memory)");
+            if (k.smem > 0 && !J->dErr) {
+                if (cudaMalloc(&J->dErr, sizeof(int)) != cudaSuccess) return fail("cudaMalloc (staged kernels' flag)");
+                if (cudaMemset(J->dErr, 0, sizeof(int)) != cudaSuccess) return fail("cudaMemset");
+            }
             J->k[P[i].phase].push_back(k);
         }
     }
@@ -1658,9 +2144,11 @@ cudaError_t launch_state(const smg_handle* h, JitState* J, double* U, int mode, 
     double hdt = h->hdt;
     int kf = kfilter;
     int md = mode;
-    void* args[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec};
+    int* err = J->dErr;
+    void* args[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec, &err};
     auto go = [&](const JitKernel& k, cudaStream_t st) {
-        return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, (unsigned)J->block, 1, 1, 0, st, args, nullptr) == 0
+        const unsigned blk = (unsigned)(k.block > 0 ? k.block : J->block);
+        return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, blk, 1, 1, (unsigned)k.smem, st, args, nullptr) == 0
                    ? cudaSuccess
                    : cudaErrorLaunchFailure;
     };
@@ -1698,6 +2186,25 @@ cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U
 }
 
 int jit_launches(const smg_handle* h, int phase) { return h->jit ? (int)h->jit->k[phase].size() : 0; }
+
+// SMG_ETIMEOUT when a staged kernel's bounded wait ran out since the last
+// check (the flag is cleared); call after the handle's stream is idle.
+int jit_status(smg_handle* h) {
+    if (!h->jit || !h->jit->dErr) return SMG_OK;
+    int v = 0;
+    if (cudaMemcpy(&v, h->jit->dErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SMG_ECUDA;
+    if (!v) return SMG_OK;
+    cudaMemset(h->jit->dErr, 0, sizeof(int));
+    return SMG_ETIMEOUT;
+}
+
+bool jit_staged_active(const smg_handle* h) {
+    if (!h->jit) return false;
+    for (int p = 0; p < 2; ++p)
+        for (const JitKernel& k : h->jit->k[p])
+            if (k.smem > 0) return true;
+    return false;
+}
 
 // ---- sources evaluated on the device --------------------------------------
 // One kernel per registered expression writes Q_j at every point of the

@@ -207,7 +207,9 @@ class GpuSolver:
               self.h)
 
     def active_variant(self):
-        """(kernel family the next run uses, reason AUTO could not use JIT)."""
+        """(kernel family the next run uses, text): with the generated kernels
+        active the text names their form ("bulk-staged" or "register"), else
+        the reason AUTO could not use them."""
         v = _lib.C.c_int32()
         why = _lib.C.create_string_buffer(512)
         check(self._L.smg_active_variant(self.h, _lib.C.byref(v), why, 512), self.h)
