@@ -32,7 +32,7 @@ def _nvrtc_available():
 
 @pytest.mark.parametrize("name", sorted(cases.ALL))
 def test_generated_source_structure(name):
-    S, src = _source(name, split=4, calls=0)
+    S, src = _source(name, split=4, calls=0, staged=0)
     n_a = sum(1 for j in range(S.n_sys) if int(np.sum(np.asarray(S.gt[j]) == 2)) % 2 == 1)
     assert "smg_jit_p1_0(" in src
     assert ("smg_jit_p0_0(" in src) == (n_a > 0)
@@ -46,8 +46,34 @@ def test_generated_source_structure(name):
     assert src.count("__global__") == (ga + 3) // 4 + (gb + 3) // 4
 
 
+@pytest.mark.parametrize("name", sorted(cases.ALL))
+def test_staged_source_structure(name):
+    """The bulk-staged form: one producer/consumer function per group, one
+    block per destination, bulk copies into the ring, every copy counted in
+    the bytes the stage expects."""
+    import re
+    S, src = _source(name, split=4, calls=0, staged=1, slices=3)
+    n_a = sum(1 for j in range(S.n_sys) if int(np.sum(np.asarray(S.gt[j]) == 2)) % 2 == 1)
+    assert src.count("double* Uj = U + pt + ") == S.n_sys
+    ga = len(set(re.findall(r"void (smg_s0_\d+)\(", src)))
+    gb = len(set(re.findall(r"void (smg_s1_\d+)\(", src)))
+    assert (n_a + 7) // 8 <= ga <= n_a and (S.n_sys - n_a + 7) // 8 <= gb <= S.n_sys - n_a
+    assert src.count("__global__") == (ga + 3) // 4 + (gb + 3) // 4
+    assert "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes" in src
+    assert "multicast" not in src
+    # per group: the expected bytes name as many copies as the producer issues
+    for body in src.split("static __device__ __forceinline__ void smg_s")[1:]:
+        body = body.split("\n}\n")[0]
+        m = re.search(r"const unsigned tx = (\d+)u \* xb \+ (\d+)u \* db;", body)
+        assert m, body[:200]
+        assert body.count("bulk_ld(stg") == int(m.group(1)) + int(m.group(2))
+        assert body.count(", xb, &bar[s]);") == int(m.group(1))
+
+
 @pytest.mark.parametrize("name", ["lin_p7_periodic", "odd_mixed_bc", "pt3d_p3", "lattice_p4_full", "spn_3d"])
 @pytest.mark.parametrize("layout", [dict(calls=0, split=4, xpair=0), dict(calls=1, split=2, xpair=1),
+                                    dict(calls=0, split=16, staged=0),
+                                    dict(calls=0, split=4, staged=1, slices=3, stages=2, rows=7),
                                     dict(calls=0, split=0, xpair=1), dict(calls=0, split=16, prefetch=1),
                                     dict(calls=0, split=16, xpair=2), dict(calls=0, split=16, band=5),
                                     dict(calls=0, split=16, const=1)])
