@@ -218,7 +218,7 @@ int smg_set_variant(smg_handle* h, int32_t variant);
 /* The kernel family the next smg_run uses (AUTO resolved; JIT only after it
  * was compiled: by smg_set_variant(JIT) or by AUTO's first smg_run) and, in
  * `why` (cap bytes, may be NULL), the form of the generated kernels when JIT
- * is active ("bulk-staged" or "register", SMG_TUNE_JIT_STAGED), else the
+ * is active ("bulk-staged", "async-staged" or "register", SMG_TUNE_JIT_STAGED), else the
  * reason AUTO could not use JIT. */
 int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
 
@@ -255,8 +255,9 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
 #define SMG_TUNE_JIT_CONST  14   /* 1 (default): coupling weights and grid constants read from a __constant__ table; 0: immediates */
 #define SMG_TUNE_GRAPH_STEPS 15  /* steps per captured CUDA graph of smg_run: 0 direct launches, no graph; -1 (default)
                                     direct launches when a step moves 1 GB or more, else 64 */
-#define SMG_TUNE_JIT_STAGED 16   /* generated kernels that stage each row's segments in shared memory with the bulk
-                                    copy engine: 1 on, 0 off (loads to registers), -1 (default) on for 2D problems */
+#define SMG_TUNE_JIT_STAGED 16   /* generated kernels that stage each row's segments in a shared-memory ring: 0 off
+                                    (loads to registers), 1 bulk copies (cp.async.bulk) by a producer thread, 2 16-byte
+                                    asynchronous copies by the consumer warps, -1 (default): 2 for 2D problems */
 #define SMG_TUNE_JIT_SLICES 17   /* staged kernels: consumer warps per CTA, each taking a slice of a group (1..16) */
 #define SMG_TUNE_JIT_STAGES 18   /* staged kernels: shared-memory ring depth in rows (2..6) */
 #define SMG_TUNE_JIT_ROWS   19   /* staged kernels: rows per CTA (0: about eight waves of CTAs per phase) */

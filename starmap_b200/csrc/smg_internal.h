@@ -148,7 +148,7 @@ struct smg_handle {
     int jit_prefetch = 0;            // L2 prefetch of a group's rows before its loads
     int jit_const = 1;               // coupling weights and grid constants from a __constant__ table
     int jit_band = -1;               // rows per band of the CTA order (0: group-major; -1: by slot size)
-    int jit_staged = -1;             // bulk-staged kernels: 1 on, 0 off, -1 for 2D problems
+    int jit_staged = -1;             // staged kernels: 0 off, 1 bulk copies, 2 async copies, -1 (2 for 2D problems)
     int jit_slices = 4;              // consumer warps (destination slices) per staged CTA
     int jit_stages = 3;              // shared-memory ring stages of the staged kernels
     int jit_rows = 0;                // rows per staged CTA (0: about eight waves per phase)
@@ -191,7 +191,7 @@ std::string jit_source(const smg_handle* h, int block, int group);
 int jit_compile(const smg_handle* h, int block, int group, std::string& err);   // compile only (no device)
 int jit_launches(const smg_handle* h, int phase);                                 // kernels per phase
 int jit_status(smg_handle* h);              // SMG_ETIMEOUT if a staged kernel's bounded wait ran out (clears it)
-bool jit_staged_active(const smg_handle* h);  // the loaded plain kernels are the bulk-staged form
+int jit_form(const smg_handle* h);   // form of the loaded plain kernels: 0 register, 1/2 staged (bulk / async copies)
 int src_build(smg_handle* h, std::string& err);       // compile the smg_set_source_expr kernels
 void src_free(smg_handle* h, bool coords);            // unload them (and free their coordinates)
 cudaError_t launch_src(const smg_handle* h, double t, cudaStream_t s);

@@ -345,6 +345,15 @@ static __device__ __forceinline__ void bulk_ld(double* dst, const double* src, u
                  :: "r"(sa(dst)), "l"(src), "r"(bytes), "r"(sa(b)) : "memory");
 }
 static __device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+// 16-byte asynchronous copy global -> shared (cached in L2 only), its group
+// commit and the wait for all but the newest N groups of this thread
+static __device__ __forceinline__ void cpa(double* dst, const double* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(sa(dst)), "l"(src) : "memory");
+}
+static __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> static __device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
 // the four values of an x difference for a point pair: from two aligned
 // 128-bit shared loads in the interior (pattern A: stencil (p, p-1), B:
 // (p+1, p)), from shared memory at the stencil offsets where the stencil
@@ -1133,11 +1142,15 @@ StagedRows staged_rows(const smg_handle* h, int phase, const std::vector<int>& D
 
 std::string staged_group_name(int phase, int k) { return "smg_s" + std::to_string(phase) + "_" + std::to_string(k); }
 
-// One group of the staged form: producer and consumers over the rows of the
-// CTA's band.  P: positions into the phase's destination list; ns consumer
-// warps (slices); st ring stages of `stage` doubles; rb rows per band.
+// One group of the staged form over the rows of the CTA's band.  P:
+// positions into the phase's destination list; ns consumer warps (slices); st
+// ring stages of `stage` doubles; rb rows per band.  loader 1: a producer
+// thread issues bulk copies completing on mbarriers; loader 2: the consumer
+// warps copy the segments themselves with 16-byte asynchronous copies (one
+// warp instruction per 64-point segment), `st - 1` rows ahead, with one CTA
+// barrier per row and no spin waits.
 void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, int ns,
-                       int st, int rb, long long stage) {
+                       int st, int rb, long long stage, int loader) {
     const smg::DevGrid& g = h->g;
     const std::vector<int> D = phase_dests(h, phase);
     const StagedRows R = staged_rows(h, phase, D, P);
@@ -1160,19 +1173,27 @@ void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, co
                   "    const int q0 = band * %d;\n"
                   "    if (q0 >= %lld) return;\n"
                   "    const int q1 = q0 + %d < %lld ? q0 + %d : %lld;\n"
-                  "    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);\n"
                   "    double* sm = smem + 16;\n"
-                  "    if (threadIdx.x == 0) {\n"
-                  "        for (int s = 0; s < %d; ++s) { mb_init(&bar[s], 1); mb_init(&bar[%d + s], %d); }\n"
-                  "        asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\");\n"
-                  "        asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
-                  "    }\n"
-                  "    __syncthreads();\n"
                   "    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);\n",
-                  staged_group_name(phase, k).c_str(), kStW, E0, rb, nrows, rb, nrows, rb, nrows, st, st, ns);
+                  staged_group_name(phase, k).c_str(), kStW, E0, rb, nrows, rb, nrows, rb, nrows);
     o += b;
-    // ---- producer: one thread
+    if (loader == 1) {
+        std::snprintf(b, sizeof b,
+                      "    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);\n"
+                      "    if (threadIdx.x == 0) {\n"
+                      "        for (int s = 0; s < %d; ++s) { mb_init(&bar[s], 1); mb_init(&bar[%d + s], %d); }\n"
+                      "        asm volatile(\"fence.mbarrier_init.release.cluster;\" ::: \"memory\");\n"
+                      "        asm volatile(\"fence.proxy.async.shared::cta;\" ::: \"memory\");\n"
+                      "    }\n"
+                      "    __syncthreads();\n",
+                      st, st, ns);
+        o += b;
+    } else {
+        o += "    (void)err;\n";
+    }
+    // ---- producer: one thread (loader 1)
     const int nx = (int)R.xs.size();
+    if (loader == 1) {
     const int nother = R.nd + (int)R.coefs.size() + 2 * (int)R.yz.size();
     std::snprintf(b, sizeof b,
                   "    if (warp == %d) {\n"
@@ -1231,6 +1252,7 @@ void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, co
         o += b;
     }
     o += "        }\n        return;\n    }\n";
+    }
     // ---- consumers: per-thread x stencil offsets, fixed over the band
     std::snprintf(b, sizeof b,
                   "    const int x0 = c0 + 2 * lane, x1 = x0 + 1;\n"
@@ -1254,17 +1276,99 @@ void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, co
                       pa ? -1 : 0, g2, pa ? 1 : 2, g2, pa ? 0 : 1, g2, g2, g2, g2, g2, g2, g2, g2, g2);
         o += b;
     }
+    if (loader == 2) {
+        // the copies of one row: main 64-point segments (a warp instruction
+        // each, lane l the 16 bytes at c0 + 2l) spread over the warps, and
+        // the two 2-point halos of every x source (lanes 0 and 1)
+        std::vector<std::pair<int, std::string>> cp;   // (slot, source row pointer expression)
+        for (int i = 0; i < R.nd; ++i) cp.push_back({i, "Ur + " + std::to_string((long long)D[P[i]] * g.cs)});
+        for (int f : R.coefs) cp.push_back({R.slot_coef(f), "fp(F, " + std::to_string(f) + ") + (Ur - U)"});
+        for (const auto& xsrc : R.xs) cp.push_back({R.slot_x(xsrc.first), "Ur + " + std::to_string((long long)xsrc.first * g.cs)});
+        for (const auto& t : R.yz) {
+            const int a = std::get<0>(t), src = std::get<1>(t), g2 = std::get<2>(t);
+            const int sl = R.slot_yz(a, src);
+            const std::string base = "Ur + " + std::to_string((long long)src * g.cs) + " + ";
+            cp.push_back({sl, base + "h" + an[a] + "_" + std::to_string(g2)});
+            cp.push_back({sl + 1, base + "l" + an[a] + "_" + std::to_string(g2)});
+        }
+        std::snprintf(b, sizeof b,
+                      "    auto issue = [&](int i) {\n"
+                      "        const int qq = q0 + i;\n"
+                      "        if (qq >= q1) return;\n"
+                      "        const int y = qq %% %d, z = qq / %d;\n"
+                      "        const double* Ur = U + ((long long)z * %lld + (long long)y * %lld);\n"
+                      "        double* stg = sm + (long long)(i %% %d) * %lld;\n",
+                      E1, E1, (long long)g.s2, (long long)g.s1, st, stage);
+        o += b;
+        for (int a = 1; a < 3; ++a)
+            for (int g2 = 0; g2 < 2; ++g2) {
+                if (!used_g2[a][g2]) continue;
+                const long long stv = a == 1 ? g.s1 : g.s2;
+                const char* pv = a == 1 ? "y" : "z";
+                std::snprintf(b, sizeof b,
+                              "        long long h%s_%d, l%s_%d;\n"
+                              "        { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); h%s_%d = (long long)(hi - %s) * %lld; "
+                              "l%s_%d = (long long)(lo - %s) * %lld; }\n",
+                              an[a], g2, an[a], g2, pv, g.n[a], g.bc[a], g2, an[a], g2, pv, stv, an[a], g2, pv, stv);
+                o += b;
+            }
+        std::snprintf(b, sizeof b, "        const int xo = c0 + 2 * lane;\n        if (xo < %lld) {\n        switch (warp) {\n",
+                      (long long)g.s1);
+        o += b;
+        for (int w = 0; w < ns; ++w) {
+            std::string body;
+            for (size_t c = w; c < cp.size(); c += ns)
+                body += "            cpa(stg + " + std::to_string(cp[c].first * kStSlot + 2) + " + 2 * lane, " +
+                        cp[c].second + " + xo);\n";
+            if (!body.empty()) o += "        case " + std::to_string(w) + ":\n" + body + "            break;\n";
+        }
+        o += "        default: break;\n        }\n        }\n";
+        if (!R.xs.empty()) {
+            std::snprintf(b, sizeof b,
+                          "        if (lane < 2) {\n"
+                          "            const int hx = lane == 0 ? c0 - 2 : c0 + %d;\n"
+                          "            if (hx >= 0 && hx + 2 <= %lld) {\n"
+                          "            double* hd = stg + (lane == 0 ? 0 : %d);\n"
+                          "            switch (warp) {\n",
+                          kStW, (long long)g.s1, kStW + 2);
+            o += b;
+            for (int w = 0; w < ns; ++w) {
+                std::string body;
+                for (size_t c = w; c < R.xs.size(); c += ns)
+                    body += "                cpa(hd + " + std::to_string(R.slot_x(R.xs[c].first) * kStSlot) + ", Ur + " +
+                            std::to_string((long long)R.xs[c].first * g.cs) + " + hx);\n";
+                if (!body.empty()) o += "            case " + std::to_string(w) + ":\n" + body + "                break;\n";
+            }
+            o += "            default: break;\n            }\n            }\n        }\n";
+        }
+        o += "    };\n";
+        std::snprintf(b, sizeof b, "    for (int i = 0; i < %d; ++i) { issue(i); cpa_commit(); }\n", st - 1);
+        o += b;
+    }
+    if (loader == 1)
+        std::snprintf(b, sizeof b,
+                      "    for (int q = q0, it = 0; q < q1; ++q, ++it) {\n"
+                      "        const int s = it %% %d;\n"
+                      "        if (!mb_wait(&bar[s], (it / %d) & 1)) { atomicExch(err, 1); return; }\n",
+                      st, st);
+    else
+        std::snprintf(b, sizeof b,
+                      "    for (int q = q0, it = 0; q < q1; ++q, ++it) {\n"
+                      "        const int s = it %% %d;\n"
+                      "        cpa_wait<%d>();\n"
+                      "        __syncthreads();\n"
+                      "        issue(it + %d);\n"
+                      "        cpa_commit();\n",
+                      st, st - 2, st - 1);
+    o += b;
     std::snprintf(b, sizeof b,
-                  "    for (int q = q0, it = 0; q < q1; ++q, ++it) {\n"
-                  "        const int s = it %% %d;\n"
-                  "        if (!mb_wait(&bar[s], (it / %d) & 1)) { atomicExch(err, 1); return; }\n"
                   "        const int y = q %% %d, z = q / %d;\n"
                   "        const int pt = z * %lld + y * %lld + x0;\n"
                   "        const double* st = sm + (long long)s * %lld + 2 + 2 * lane;\n"
                   "        (void)pt;\n"
                   "        if (act) {\n"
                   "        switch (warp) {\n",
-                  st, st, E1, E1, (long long)g.s2, (long long)g.s1, stage);
+                  E1, E1, (long long)g.s2, (long long)g.s1, stage);
     o += b;
     // slices: contiguous runs of the group's destinations (the group order
     // puts destinations that share sources next to each other)
@@ -1378,10 +1482,13 @@ void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, co
         }
         o += "        } break;\n";
     }
-    o += "        default: break;\n        }\n        }\n"
-         "        __syncwarp();\n"
-         "        if (lane == 0) mb_arrive(&bar[" + std::to_string(st) + " + s]);\n"
-         "    }\n}\n";
+    o += "        default: break;\n        }\n        }\n";
+    if (loader == 1)
+        o += "        __syncwarp();\n"
+             "        if (lane == 0) mb_arrive(&bar[" + std::to_string(st) + " + s]);\n"
+             "    }\n}\n";
+    else
+        o += "    }\n    cpa_wait<0>();\n}\n";
 }
 
 // Shape of the staged kernels of a handle.
@@ -1408,29 +1515,30 @@ StagedShape staged_shape(const smg_handle* h, int ngroups_phase) {
     return S;
 }
 
-// Whether the plain kernels take the staged form: SMG_TUNE_JIT_STAGED 1, or
-// -1 (default) for 2D problems; never with separately compiled groups, and
-// only when every group's ring fits in one CTA's shared memory.
-bool staged_form(const smg_handle* h) {
-    const int want = h->jit_staged;
-    if (want == 0 || h->jit_calls) return false;
-    if (want < 0 && !(h->g.B[2] == 1 && h->g.B[1] > 1)) return false;
+// The loader of the plain kernels' staged form (0: register form):
+// SMG_TUNE_JIT_STAGED 1 (bulk copies) or 2 (asynchronous copies by the
+// consumer warps), or -1 (default): 2 for 2D problems; never with separately
+// compiled groups, and only when every group's ring fits in one CTA's shared
+// memory.
+int staged_form(const smg_handle* h) {
+    const int want = h->jit_staged < 0 ? ((h->g.B[2] == 1 && h->g.B[1] > 1) ? 2 : 0) : h->jit_staged;
+    if (want == 0 || h->jit_calls) return 0;
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
         if (D.empty()) continue;
         for (const auto& P : shared_groups(h, phase, h->jit_group)) {
             const long long smem = (16 + (long long)h->jit_stages * staged_rows(h, phase, D, P).nslots() * kStSlot) * 8;
-            if (smem > 227LL * 1024) return false;
+            if (smem > 227LL * 1024) return 0;
         }
     }
-    return true;
+    return want;
 }
 
 // Kernel over staged groups [k0, k1) of one phase: CTA -> (band, group,
 // chunk), band-major, so that the CTAs running at one time cover the same
 // rows of every group and the sources they share are read from L2.
 void emit_staged_dispatch(std::string& o, int phase, int k0, int k1, const StagedShape& S, int minb,
-                          const std::string& name) {
+                          const std::string& name, int loader) {
     char b[1024];
     const int ngk = k1 - k0;
     std::snprintf(b, sizeof b,
@@ -1442,7 +1550,7 @@ void emit_staged_dispatch(std::string& o, int phase, int k0, int k1, const Stage
                   "    const int band = bid / %d, rest = bid - band * %d;\n"
                   "    const int grp = %d + rest / %d, chunk = rest %% %d;\n"
                   "    switch (grp) {\n",
-                  32 * (S.ns + 1), minb, name.c_str(), ngk * S.nch, ngk * S.nch, k0, S.nch, S.nch);
+                  32 * (S.ns + (loader == 1 ? 1 : 0)), minb, name.c_str(), ngk * S.nch, ngk * S.nch, k0, S.nch, S.nch);
     o += b;
     for (int k = k0; k < k1; ++k)
         o += "    case " + std::to_string(k) + ": " + staged_group_name(phase, k) +
@@ -1458,6 +1566,7 @@ struct KernelSrc {
     long long grid;
     int block = 0;
     int smem = 0;
+    int form = 0;   // 0 register form, 1 staged by bulk copies, 2 staged by asynchronous copies
 };
 
 // The generated code of one handle.
@@ -1502,7 +1611,8 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         const std::vector<std::vector<int>> G = shared_groups(h, phase, group);
         const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
-        if (!rec && staged_form(h)) {
+        const int loader = rec ? 0 : staged_form(h);
+        if (loader) {
             const StagedShape S = staged_shape(h, ng);
             for (int k0 = 0; k0 < ng; k0 += step) {
                 const int k1 = std::min(ng, k0 + step);
@@ -1514,15 +1624,17 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
                 KernelSrc k{std::string(kPrelude) + kStagePrelude,
                             "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
                             S.nb * (k1 - k0) * S.nch};
-                k.block = 32 * (S.ns + 1);
+                k.block = 32 * (S.ns + (loader == 1 ? 1 : 0));
                 k.smem = (int)smem;
+                k.form = loader;
                 ConstTable tab;
                 std::string body;
                 g_ctab = h->jit_const ? &tab : nullptr;
-                for (int j = k0; j < k1; ++j) emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage);
+                for (int j = k0; j < k1; ++j)
+                    emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage, loader);
                 g_ctab = nullptr;
                 k.src += ctab_decl(tab) + body;
-                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name);
+                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name, loader);
                 P.push_back(std::move(k));
             }
             continue;
@@ -2013,6 +2125,7 @@ struct JitKernel {
     long long grid = 0;
     int block = 0;   // CTA size (0: the state's)
     int smem = 0;    // dynamic shared memory (staged form)
+    int form = 0;    // as KernelSrc::form
 };
 
 struct JitState {
@@ -2105,11 +2218,12 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
             k.grid = P[i].grid;
             k.block = P[i].block;
             k.smem = P[i].smem;
+            k.form = P[i].form;
             if (a.ModuleGetFunction(&k.fn, J->mods[i], P[i].name.c_str()) != 0)
                 return fail("cuModuleGetFunction " + P[i].name);
             if (k.smem > 48 * 1024 && a.FuncSetAttribute(k.fn, kFuncAttrMaxDynamicSmem, k.smem) != 0)
                 return fail("cuFuncSetAttribute " + P[i].name + " (" + std::to_string(k.smem) + " bytes of shared memory)");
-            if (k.smem > 0 && !J->dErr) {
+            if (k.form == 1 && !J->dErr) {
                 if (cudaMalloc(&J->dErr, sizeof(int)) != cudaSuccess) return fail("cudaMalloc (staged kernels' flag)");
                 if (cudaMemset(J->dErr, 0, sizeof(int)) != cudaSuccess) return fail("cudaMemset");
             }
@@ -2198,12 +2312,12 @@ int jit_status(smg_handle* h) {
     return SMG_ETIMEOUT;
 }
 
-bool jit_staged_active(const smg_handle* h) {
-    if (!h->jit) return false;
+int jit_form(const smg_handle* h) {
+    if (!h->jit) return 0;
     for (int p = 0; p < 2; ++p)
         for (const JitKernel& k : h->jit->k[p])
-            if (k.smem > 0) return true;
-    return false;
+            if (k.form) return k.form;
+    return 0;
 }
 
 // ---- sources evaluated on the device --------------------------------------

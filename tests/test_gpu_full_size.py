@@ -100,7 +100,11 @@ def test_adjoint_at_full_size_vs_cpu_adjoint():
     """Gradients of the misfit on the zeroth moment for the 2D P15 200^2
     problem over a 20-step prefix, checkpointed every 20 steps: GPU against
     the oracle's CPU adjoint (oracle/adjoint_np.py), relative L2 1e-11 per
-    output array (the GPU sums gradient contributions with atomics)."""
+    output array (the GPU sums gradient contributions with atomics).  The
+    initial-condition gradient is one vector over all components: its
+    high-order components are as small as 1e-271 after near-total
+    cancellation, so each component's error is measured against the norm of
+    the whole vector."""
     from oracle import adjoint_np as A
     from starmap_b200.batch import _tables
     from starmap_b200.solver import GpuSolver, handle_tables
@@ -137,8 +141,11 @@ def test_adjoint_at_full_size_vs_cpu_adjoint():
         err = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-300)
         assert err <= 1e-11, (what, err)
 
+    norm_all = np.sqrt(sum(np.linalg.norm(np.ravel(ref["lam0"][j])) ** 2 for j in range(S.n_sys)))
     for j in range(S.n_sys):
-        close(gU[j], ref["lam0"][j], ("U0", j))
+        got = np.asarray(gU[j], dtype=np.float64).ravel(order="F")
+        want = np.asarray(ref["lam0"][j], dtype=np.float64).ravel(order="F")
+        assert np.linalg.norm(got - want) <= 1e-11 * norm_all, ("U0", j)
     for key in keys:
         k = T.index[key]
         if key[0] == "sT":
