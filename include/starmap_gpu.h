@@ -251,7 +251,8 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
                                     2 = one 128-bit load and the neighbouring lane's value (warp shuffle) */
 #define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them */
 #define SMG_TUNE_JIT_BAND   13   /* CTA order of the generated kernels: 0 group-major, R > 0 bands of R rows,
-                                    -1 (default) group-major below 4 MB per component, else bands of about 48 MB */
+                                    -1 (default) group-major below 4 MB per component, else bands of about 48 MB;
+                                    staged kernels: 0 group-major, else band-major (bands of SMG_TUNE_JIT_ROWS) */
 #define SMG_TUNE_JIT_CONST  14   /* 1 (default): coupling weights and grid constants read from a __constant__ table; 0: immediates */
 #define SMG_TUNE_GRAPH_STEPS 15  /* steps per captured CUDA graph of smg_run: 0 direct launches, no graph; -1 (default)
                                     direct launches when a step moves 1 GB or more, else 64 */

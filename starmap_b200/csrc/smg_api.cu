@@ -1363,7 +1363,7 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->jit_failed = false;
             break;
         case SMG_TUNE_JIT_STAGED:
-            if (value < -1 || value > 2) return fail(h, SMG_EINVAL, "smg_tune: jit staged must be -1, 0, 1 or 2");
+            if (value < -1 || value > 3) return fail(h, SMG_EINVAL, "smg_tune: jit staged must be -1..3");
             h->jit_staged = value;
             smg::jit_free(h);
             h->jit_failed = false;
@@ -1417,8 +1417,10 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap) 
     if (why && cap > 0) {
         // with the generated kernels active: their form; otherwise why AUTO could not use them
         const std::string m = v == SMG_VARIANT_JIT
-                                  ? (smg::jit_form(h) == 1 ? "bulk-staged"
-                                                           : (smg::jit_form(h) == 2 ? "async-staged" : "register"))
+                                  ? std::string(smg::jit_form(h) == 1   ? "bulk-staged"
+                                                : smg::jit_form(h) == 2 ? "async-staged"
+                                                : smg::jit_form(h) == 3 ? "prefetch-ring"
+                                                                        : "register")
                                   : h->jit_err;
         const size_t n = std::min<size_t>((size_t)cap - 1, m.size());
         std::memcpy(why, m.data(), n);

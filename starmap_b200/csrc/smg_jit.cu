@@ -351,6 +351,13 @@ static __device__ __forceinline__ void cpa(double* dst, const double* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(sa(dst)), "l"(src) : "memory");
 }
 static __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// the same, cached in L1 as well, 16 or 8 bytes
+static __device__ __forceinline__ void cpa16(double2* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" :: "r"(sa(dst)), "l"(src) : "memory");
+}
+static __device__ __forceinline__ void cpa8(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(sa(dst)), "l"(src) : "memory");
+}
 template <int N> static __device__ __forceinline__ void cpa_wait() {
     asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
 }
@@ -1491,6 +1498,254 @@ void emit_staged_group(std::string& o, const smg_handle* h, int phase, int k, co
         o += "    }\n    cpa_wait<0>();\n}\n";
 }
 
+
+// ---- register form with a per-thread prefetch ring (SMG_TUNE_JIT_STAGED 3) ----
+// The register form's CTA mapping and straight-line group code, but every
+// value a destination reads from global memory for the first time is copied
+// by the thread itself (cp.async, 8 or 16 bytes) into its own column of a
+// small shared ring one destination ahead: while destination d computes, the
+// copies of destination d+1 are in flight without holding registers.  Each
+// thread reads only what it copied itself, so no barrier is needed.
+struct PfItem {
+    int kind;    // 0 array coefficient, 1 x source (four 8-byte values), 2 y/z source (two rows), 3 destination
+    int id;      // field, source component or destination
+    int a, g2;   // axis and grid flag of a source
+    int slot[2];
+};
+
+std::vector<std::vector<PfItem>> prefetch_items(const smg_handle* h, int phase, const std::vector<int>& D,
+                                                const std::vector<int>& P) {
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    std::vector<std::vector<PfItem>> items(P.size());
+    std::set<int> coef_done;
+    std::set<std::pair<int, int>> val_done;
+    for (size_t pi = 0; pi < P.size(); ++pi) {
+        const int j = D[P[pi]];
+        const smg::DevComp& c = h->comps[j];
+        const Coefs f = coefs_of(h, phase, j);
+        std::vector<int> fl = {f.q, f.s, f.E};
+        if (filt) fl.insert(fl.end(), {f.F1, f.F2});
+        for (int fi : fl)
+            if (is_array(h, fi) && coef_done.insert(fi).second) items[pi].push_back({0, fi, 0, 0, {-1, -1}});
+        for (int qq = c.cbeg; qq < c.cend; ++qq) {
+            const smg::DevCoup& cp = h->coups[qq];
+            const int a = cp.code >> 1, g2 = cp.code & 1;
+            if (!val_done.insert({a, cp.src}).second) continue;
+            items[pi].push_back({a == 0 ? 1 : 2, cp.src, a, g2, {-1, -1}});
+        }
+        items[pi].push_back({3, j, 0, 0, {-1, -1}});
+    }
+    return items;
+}
+
+int item_slots(const PfItem& it) { return it.kind == 1 || it.kind == 2 ? 2 : 1; }
+
+// ring slots one destination ahead needs: the largest sum over two consecutive destinations
+int prefetch_ring(const std::vector<std::vector<PfItem>>& items) {
+    int best = 1;
+    for (size_t d = 0; d < items.size(); ++d) {
+        int n = 0;
+        for (size_t e = d; e < std::min(items.size(), d + 2); ++e)
+            for (const PfItem& it : items[e]) n += item_slots(it);
+        best = std::max(best, n);
+    }
+    return best;
+}
+
+void emit_prefetch_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, int ring,
+                         int block) {
+    const smg::DevGrid& g = h->g;
+    const std::vector<int> D = phase_dests(h, phase);
+    std::vector<std::vector<PfItem>> items = prefetch_items(h, phase, D, P);
+    int next = 0;
+    for (auto& v : items)
+        for (PfItem& it : v)
+            for (int q = 0; q < item_slots(it); ++q) {
+                it.slot[q] = next;
+                next = (next + 1) % ring;
+            }
+    const bool filt = h->filter_mode == SMG_FILTER_SUBSTEP;
+    const char* an[3] = {"x", "y", "z"};
+    char b[4096];
+    o += "static __device__ __forceinline__ void " + group_name(phase, k) + group_args(false) + " {\n";
+    std::snprintf(b, sizeof b,
+                  "    const int x1 = x0 + 1;\n"
+                  "    const int pt = z * %lld + y * %lld + x0;\n"
+                  "    const double* Up = U + pt;\n"
+                  "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
+                  (long long)g.s2, (long long)g.s1);
+    o += b;
+    bool used[3] = {false, false, false};
+    for (int p : P)
+        for (int q = h->comps[D[p]].cbeg; q < h->comps[D[p]].cend; ++q) used[h->coups[q].code >> 1] = true;
+    if (used[0])
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int hx0_%d, lx0_%d, hx1_%d, lx1_%d;\n"
+                          "    { int hi, lo; stencil(x0, %d, %d, %d, hi, lo); hx0_%d = hi - x0; lx0_%d = lo - x0;\n"
+                          "      stencil(x1, %d, %d, %d, hi, lo); hx1_%d = hi - x0; lx1_%d = lo - x0; }\n",
+                          g2, g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2, g.n[0], g.bc[0], g2, g2, g2);
+            o += b;
+        }
+    for (int a = 1; a < 3; ++a) {
+        if (!used[a]) continue;
+        const long long st = a == 1 ? g.s1 : g.s2;
+        const char* pp = a == 1 ? "y" : "z";
+        for (int g2 = 0; g2 < 2; ++g2) {
+            std::snprintf(b, sizeof b,
+                          "    int h%s_%d, l%s_%d;\n"
+                          "    { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); h%s_%d = (int)((hi - %s) * %lld); "
+                          "l%s_%d = (int)((lo - %s) * %lld); }\n",
+                          an[a], g2, an[a], g2, pp, g.n[a], g.bc[a], g2, an[a], g2, pp, st, an[a], g2, pp, st);
+            o += b;
+        }
+    }
+    const smg::DevComp& c0 = h->comps[D[P[0]]];
+    std::string cond;
+    const char* ax[3] = {"x0", "y", "z"};
+    for (int a = 0; a < 3; ++a)
+        if (c0.ext[a] < g.B[a]) {
+            if (!cond.empty()) cond += " && ";
+            cond += std::string(ax[a]) + " < " + std::to_string(c0.ext[a]);
+        }
+    o += cond.empty() ? "    {\n" : "    if (" + cond + ") {\n";
+    const bool v1_always = c0.ext[0] % 2 == 0;
+    if (!v1_always) o += "    const bool v1 = x1 < " + std::to_string(c0.ext[0]) + ";\n";
+    const std::string sel1 = v1_always ? "" : "v1 ? ", sel2 = v1_always ? "" : " : 0";
+    o += "    double2* R = smg_ring + threadIdx.x;\n";
+    auto slot = [&](int s) { return "R[" + std::to_string(s * block) + "]"; };
+    auto issue = [&](const std::vector<PfItem>& v) {
+        for (const PfItem& it : v) {
+            if (it.kind == 0) {
+                std::snprintf(b, sizeof b, "    cpa16(&%s, fp(F, %d) + pt);\n", slot(it.slot[0]).c_str(), it.id);
+            } else if (it.kind == 1) {
+                const long long so = (long long)it.id * g.cs;
+                const int g2 = it.g2;
+                std::snprintf(b, sizeof b,
+                              "    cpa8(&%s.x, Up + %lld + hx0_%d); cpa8(&%s.y, Up + %lld + lx0_%d);\n"
+                              "    cpa8(&%s.x, Up + %lld + (%shx1_%d%s)); cpa8(&%s.y, Up + %lld + (%slx1_%d%s));\n",
+                              slot(it.slot[0]).c_str(), so, g2, slot(it.slot[0]).c_str(), so, g2,
+                              slot(it.slot[1]).c_str(), so, sel1.c_str(), g2, sel2.c_str(), slot(it.slot[1]).c_str(), so,
+                              sel1.c_str(), g2, sel2.c_str());
+            } else if (it.kind == 2) {
+                const long long so = (long long)it.id * g.cs;
+                std::snprintf(b, sizeof b, "    cpa16(&%s, Up + %lld + h%s_%d); cpa16(&%s, Up + %lld + l%s_%d);\n",
+                              slot(it.slot[0]).c_str(), so, an[it.a], it.g2, slot(it.slot[1]).c_str(), so, an[it.a],
+                              it.g2);
+            } else {
+                std::snprintf(b, sizeof b, "    cpa16(&%s, Up + %lld);\n", slot(it.slot[0]).c_str(),
+                              (long long)it.id * g.cs);
+            }
+            o += b;
+        }
+        o += "    cpa_commit();\n";
+    };
+    issue(items[0]);
+    std::set<int> scal_done;
+    for (size_t pi = 0; pi < P.size(); ++pi) {
+        if (pi + 1 < P.size()) {
+            issue(items[pi + 1]);
+            o += "    cpa_wait<1>();\n";
+        } else {
+            o += "    cpa_wait<0>();\n";
+        }
+        const int j = D[P[pi]];
+        const smg::DevComp& c = h->comps[j];
+        const Coefs f = coefs_of(h, phase, j);
+        int uslot = -1;
+        for (const PfItem& it : items[pi]) {
+            if (it.kind == 0)
+                std::snprintf(b, sizeof b, "    const double2 C%d = %s;\n", it.id, slot(it.slot[0]).c_str());
+            else if (it.kind == 1)
+                std::snprintf(b, sizeof b,
+                              "    const double X%d_a0 = %s.x, X%d_b0 = %s.y, X%d_a1 = %s.x, X%d_b1 = %s.y;\n", it.id,
+                              slot(it.slot[0]).c_str(), it.id, slot(it.slot[0]).c_str(), it.id, slot(it.slot[1]).c_str(),
+                              it.id, slot(it.slot[1]).c_str());
+            else if (it.kind == 2)
+                std::snprintf(b, sizeof b, "    const double2 %c%d_h = %s, %c%d_l = %s;\n", it.a == 1 ? 'Y' : 'Z', it.id,
+                              slot(it.slot[0]).c_str(), it.a == 1 ? 'Y' : 'Z', it.id, slot(it.slot[1]).c_str());
+            else {
+                uslot = it.slot[0];
+                b[0] = 0;
+            }
+            o += b;
+        }
+        auto coef = [&](int fi) {
+            const std::string n = "C" + std::to_string(fi);
+            if (!is_array(h, fi) && scal_done.insert(fi).second) {
+                std::snprintf(b, sizeof b, "    const double %s = fs(F, %d);\n", n.c_str(), fi);
+                o += b;
+            }
+            return std::make_pair(is_array(h, fi) ? n + ".x" : n, is_array(h, fi) ? n + ".y" : n);
+        };
+        const auto q = coef(f.q), sv = coef(f.s), E = coef(f.E);
+        std::pair<std::string, std::string> k1{"1.0", "1.0"}, k2{"1.0", "1.0"};
+        if (filt) {
+            k1 = coef(f.F1);
+            k2 = coef(f.F2);
+        }
+        std::snprintf(b, sizeof b,
+                      "    {\n        double* Uj = U + pt + %lld;\n"
+                      "        const double2 u = %s;\n"
+                      "        double SA = 0.0, SB = 0.0;\n",
+                      (long long)j * g.cs, slot(uslot).c_str());
+        o += b;
+        bool first = true;
+        for (int qq = c.cbeg; qq < c.cend; ++qq) {
+            const smg::DevCoup& cp = h->coups[qq];
+            const int a = cp.code >> 1;
+            const int mode_div = h->exact_recip[a];
+            const std::string H = clit(g.h[a]), RH = clit(h->rh[a]), W = clit(cp.w);
+            const char* dv = mode_div == 2 ? "div2" : (mode_div == 1 ? "div1" : "div0");
+            const char* fold = first ? "SA = tA; SB = tB;" : "SA = __dadd_rn(SA, tA); SB = __dadd_rn(SB, tB);";
+            first = false;
+            std::string dA, dB;
+            if (a == 0) {
+                dA = "__dsub_rn(X" + std::to_string(cp.src) + "_a0, X" + std::to_string(cp.src) + "_b0)";
+                dB = "__dsub_rn(X" + std::to_string(cp.src) + "_a1, X" + std::to_string(cp.src) + "_b1)";
+            } else {
+                const std::string n = std::string(1, a == 1 ? 'Y' : 'Z') + std::to_string(cp.src);
+                dA = "__dsub_rn(" + n + "_h.x, " + n + "_l.x)";
+                dB = "__dsub_rn(" + n + "_h.y, " + n + "_l.y)";
+            }
+            std::snprintf(b, sizeof b,
+                          "        { const double tA = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                          "          const double tB = __dmul_rn(%s(%s, %s, %s), %s);\n"
+                          "          %s }\n",
+                          dv, dA.c_str(), H.c_str(), RH.c_str(), W.c_str(), dv, dB.c_str(), H.c_str(), RH.c_str(),
+                          W.c_str(), fold);
+            o += b;
+        }
+        o += "        double u0 = u.x, u1 = u.y;\n";
+        auto sub = [&]() {
+            std::snprintf(b, sizeof b, "u0 = upd(u0, -SA, %s, %s, %s, hdt); u1 = upd(u1, -SB, %s, %s, %s, hdt);",
+                          q.first.c_str(), sv.first.c_str(), E.first.c_str(), q.second.c_str(), sv.second.c_str(),
+                          E.second.c_str());
+            return std::string(b);
+        };
+        auto fl = [&](const std::pair<std::string, std::string>& Fp) {
+            return filt ? " u0 = __dmul_rn(u0, " + Fp.first + "); u1 = __dmul_rn(u1, " + Fp.second + ");"
+                        : std::string();
+        };
+        if (phase == 0) {
+            const std::string one =
+                "        " + sub() +
+                (filt ? " u0 = __dmul_rn(u0, kf == 1 ? " + k1.first + " : " + k2.first +
+                            "); u1 = __dmul_rn(u1, kf == 1 ? " + k1.second + " : " + k2.second + ");"
+                      : std::string()) +
+                "\n";
+            const std::string two = "        " + sub() + fl(k2) + "\n        " + sub() + fl(k1) + "\n";
+            if (h->filter_mode == SMG_FILTER_FULL) o += one;
+            else o += "        if (mode == 0) {\n" + one + "        } else {\n" + two + "        }\n";
+        } else {
+            o += "        " + sub() + fl(k1) + "\n        " + sub() + fl(k2) + "\n";
+        }
+        if (v1_always) o += "        *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1);\n    }\n";
+        else o += "        if (v1) *reinterpret_cast<double2*>(Uj) = make_double2(u0, u1); else *Uj = u0;\n    }\n";
+    }
+    o += "    }\n}\n";
+}
+
 // Shape of the staged kernels of a handle.
 struct StagedShape {
     int ns, st, nch, rb;
@@ -1522,7 +1777,7 @@ StagedShape staged_shape(const smg_handle* h, int ngroups_phase) {
 // memory.
 int staged_form(const smg_handle* h) {
     const int want = h->jit_staged < 0 ? ((h->g.B[2] == 1 && h->g.B[1] > 1) ? 2 : 0) : h->jit_staged;
-    if (want == 0 || h->jit_calls) return 0;
+    if (want == 0 || want == 3 || h->jit_calls) return 0;
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
         if (D.empty()) continue;
@@ -1536,21 +1791,33 @@ int staged_form(const smg_handle* h) {
 
 // Kernel over staged groups [k0, k1) of one phase: CTA -> (band, group,
 // chunk), band-major, so that the CTAs running at one time cover the same
-// rows of every group and the sources they share are read from L2.
+// rows of every group and the sources they share are read from L2; or
+// (group_major) CTA -> (group, band, chunk), every band of a group together.
 void emit_staged_dispatch(std::string& o, int phase, int k0, int k1, const StagedShape& S, int minb,
-                          const std::string& name, int loader) {
+                          const std::string& name, int loader, bool group_major) {
     char b[1024];
     const int ngk = k1 - k0;
+    std::string map;
+    if (group_major)
+        std::snprintf(b, sizeof b,
+                      "    const int grp = %d + bid / %lld, rest = bid %% %lld;\n"
+                      "    const int band = rest / %d, chunk = rest %% %d;\n",
+                      k0, S.nb * S.nch, S.nb * S.nch, S.nch, S.nch);
+    else
+        std::snprintf(b, sizeof b,
+                      "    const int band = bid / %d, rest = bid - band * %d;\n"
+                      "    const int grp = %d + rest / %d, chunk = rest %% %d;\n",
+                      ngk * S.nch, ngk * S.nch, k0, S.nch, S.nch);
+    map = b;
     std::snprintf(b, sizeof b,
                   "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s(double* __restrict__ U, "
                   "const DevField* __restrict__ F, double hdt, int kf, int mode, double* WR, double* PR, int* err) {\n"
                   "    extern __shared__ __align__(128) double smem_st[];\n"
                   "    (void)WR; (void)PR;\n"
                   "    const int bid = (int)blockIdx.x;\n"
-                  "    const int band = bid / %d, rest = bid - band * %d;\n"
-                  "    const int grp = %d + rest / %d, chunk = rest %% %d;\n"
+                  "%s"
                   "    switch (grp) {\n",
-                  32 * (S.ns + (loader == 1 ? 1 : 0)), minb, name.c_str(), ngk * S.nch, ngk * S.nch, k0, S.nch, S.nch);
+                  32 * (S.ns + (loader == 1 ? 1 : 0)), minb, name.c_str(), map.c_str());
     o += b;
     for (int k = k0; k < k1; ++k)
         o += "    case " + std::to_string(k) + ": " + staged_group_name(phase, k) +
@@ -1566,7 +1833,7 @@ struct KernelSrc {
     long long grid;
     int block = 0;
     int smem = 0;
-    int form = 0;   // 0 register form, 1 staged by bulk copies, 2 staged by asynchronous copies
+    int form = 0;   // 0 register form, 1 staged by bulk copies, 2 staged by asynchronous copies, 3 prefetch ring
 };
 
 // The generated code of one handle.
@@ -1634,7 +1901,7 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
                     emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage, loader);
                 g_ctab = nullptr;
                 k.src += ctab_decl(tab) + body;
-                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name, loader);
+                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name, loader, h->jit_band == 0);
                 P.push_back(std::move(k));
             }
             continue;
@@ -1649,7 +1916,19 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
             ConstTable tab;
             std::string body;
             g_ctab = h->jit_const ? &tab : nullptr;
-            for (int j = k0; j < k1; ++j) emit_shared_group(body, h, phase, j, G[j], rec);
+            int ring = 0;
+            if (!rec && h->jit_staged == 3 && !h->jit_xpair && !h->jit_prefetch) {
+                for (int j = k0; j < k1; ++j) ring = std::max(ring, prefetch_ring(prefetch_items(h, phase, D, G[j])));
+                if ((long long)ring * block * 16 > 48 * 1024) ring = 0;   // static shared memory limit
+            }
+            if (ring > 0) {
+                k.src += kStagePrelude;
+                k.form = 3;
+                body = "__shared__ double2 smg_ring[" + std::to_string(ring * block) + "];\n";
+                for (int j = k0; j < k1; ++j) emit_prefetch_group(body, h, phase, j, G[j], ring, block);
+            } else {
+                for (int j = k0; j < k1; ++j) emit_shared_group(body, h, phase, j, G[j], rec);
+            }
             g_ctab = nullptr;
             k.src += ctab_decl(tab) + body;
             emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);

@@ -370,12 +370,13 @@ STAGED_CASES = ["lattice_p5_substep", "lattice_p4_full", "lattice_p6_nofilter", 
 
 
 @pytest.mark.parametrize("shape", [(1, 4, 3, 0), (1, 1, 2, 1), (1, 3, 6, 5), (2, 4, 3, 0), (2, 1, 2, 1), (2, 3, 6, 5),
-                                   (2, 8, 2, 0), (2, 16, 4, 0), (0, 4, 3, 0)])
+                                   (2, 8, 2, 0), (2, 16, 4, 0), (3, 4, 3, 0), (0, 4, 3, 0)])
 @pytest.mark.parametrize("name", STAGED_CASES)
 def test_staged_kernels_vs_oracle(name, shape):
     """The generated kernels in the staged forms (row segments copied into a
     shared-memory ring by the bulk copy engine, or by the consumer warps' own
-    asynchronous copies) and in the register form, with several CTA shapes
+    asynchronous copies), with a per-thread prefetch ring, and in the register
+    form, with several CTA shapes
     (consumer warps, ring stages, rows per CTA; 0 = automatic), 2D and 3D,
     against the numpy oracle: bit-identical."""
     from starmap_b200 import _lib
@@ -399,7 +400,8 @@ def test_staged_kernels_vs_oracle(name, shape):
         v, form = solver.active_variant()
     finally:
         solver.close()
-    assert v == _lib.SMG_VARIANT_JIT and form == ["register", "bulk-staged", "async-staged"][staged], (v, form)
+    assert v == _lib.SMG_VARIANT_JIT and form == ["register", "bulk-staged", "async-staged", "prefetch-ring"][staged], \
+        (v, form)
     worst, mism = 0.0, 0
     for j in range(S.n_sys):
         worst = max(worst, rel_l2(U[j], ref.U[j]))
