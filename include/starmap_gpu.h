@@ -256,9 +256,11 @@ int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* val
 #define SMG_TUNE_JIT_CONST  14   /* 1 (default): coupling weights and grid constants read from a __constant__ table; 0: immediates */
 #define SMG_TUNE_GRAPH_STEPS 15  /* steps per captured CUDA graph of smg_run: 0 direct launches, no graph; -1 (default)
                                     direct launches when a step moves 1 GB or more, else 64 */
-#define SMG_TUNE_JIT_STAGED 16   /* generated kernels that stage each row's segments in a shared-memory ring: 0 off
-                                    (loads to registers), 1 bulk copies (cp.async.bulk) by a producer thread, 2 16-byte
-                                    asynchronous copies by the consumer warps, -1 (default): 2 for 2D problems */
+#define SMG_TUNE_JIT_STAGED 16   /* form of the generated kernels: 0 (default) loads to registers at first use; 1 each
+                                    row's segments staged in a shared-memory ring by bulk copies (cp.async.bulk) from a
+                                    producer thread; 2 the same ring filled by the consumer warps' 16-byte asynchronous
+                                    copies; 3 the default form with a per-thread ring of asynchronous copies one
+                                    destination ahead.  All give identical results; 1-3 measured slower. */
 #define SMG_TUNE_JIT_SLICES 17   /* staged kernels: consumer warps per CTA, each taking a slice of a group (1..16) */
 #define SMG_TUNE_JIT_STAGES 18   /* staged kernels: shared-memory ring depth in rows (2..6) */
 #define SMG_TUNE_JIT_ROWS   19   /* staged kernels: rows per CTA (0: about eight waves of CTAs per phase) */

@@ -1363,7 +1363,7 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->jit_failed = false;
             break;
         case SMG_TUNE_JIT_STAGED:
-            if (value < -1 || value > 3) return fail(h, SMG_EINVAL, "smg_tune: jit staged must be -1..3");
+            if (value < 0 || value > 3) return fail(h, SMG_EINVAL, "smg_tune: jit staged must be 0..3");
             h->jit_staged = value;
             smg::jit_free(h);
             h->jit_failed = false;

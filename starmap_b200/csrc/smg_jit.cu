@@ -1770,13 +1770,12 @@ StagedShape staged_shape(const smg_handle* h, int ngroups_phase) {
     return S;
 }
 
-// The loader of the plain kernels' staged form (0: register form):
-// SMG_TUNE_JIT_STAGED 1 (bulk copies) or 2 (asynchronous copies by the
-// consumer warps), or -1 (default): 2 for 2D problems; never with separately
-// compiled groups, and only when every group's ring fits in one CTA's shared
-// memory.
+// The loader of the plain kernels' staged form (0: none): SMG_TUNE_JIT_STAGED
+// 1 (bulk copies) or 2 (asynchronous copies by the consumer warps); never
+// with separately compiled groups, and only when every group's ring fits in
+// one CTA's shared memory.
 int staged_form(const smg_handle* h) {
-    const int want = h->jit_staged < 0 ? ((h->g.B[2] == 1 && h->g.B[1] > 1) ? 2 : 0) : h->jit_staged;
+    const int want = h->jit_staged;
     if (want == 0 || want == 3 || h->jit_calls) return 0;
     for (int phase = 0; phase < 2; ++phase) {
         const std::vector<int> D = phase_dests(h, phase);
