@@ -31,6 +31,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# the generated kernels' on-disk cache of this run stays in the tree
+os.environ.setdefault("SMG_JIT_CACHE_DIR", os.path.join(ROOT, "_build", "jit_cache"))
 
 WORKLOAD_NAME = ("2D checkerboard lattice P39 filtered (820 moments), 350x350 cells, bc=1, "
                  "substep exp filter p=4 f_eff=10, dt=0.5h, t_final=3.2 (321 steps)")
@@ -348,6 +350,50 @@ def bench_3d(steps: int = 96, n: int = 128):
                          "traffic": ncu_traffic(name="phase_kernels_jit_pointsource3d_p9.txt") if n == 128 else None}}
 
 
+def cold_call():
+    """--cold-call (run in a fresh process by bench_cold): the whole public
+    call a MATLAB user makes -- starmap_init, starmap_solver to t_final with
+    host setup, hook sampling, handle creation, kernel compilation (or its
+    load from the on-disk cache), upload, all 321 steps and the download of
+    the output moment -- timed by the wall clock from before starmap_init."""
+    import ctypes
+    t0 = time.perf_counter()
+    from starmap_b200 import _lib, configs, starmap_init
+    from starmap_b200.solver import starmap_solver
+    prob = configs.lattice(n=350, n_mom=39, tfinal=3.2, filter_order=4, f_eff=10.0, f_position="substep")
+    par = starmap_init(prob)
+    out = starmap_solver(par)
+    secs = time.perf_counter() - t0
+    c, d = ctypes.c_int64(), ctypes.c_int64()
+    _lib.lib().smg_jit_stats(ctypes.byref(c), ctypes.byref(d))
+    print(json.dumps({"seconds": secs, "programs_compiled": c.value, "programs_from_disk": d.value,
+                      "finite": bool(np.all(np.isfinite(out[0]["U"])))}), flush=True)
+    return 0
+
+
+def bench_cold(upd_step: float, nsteps: int = 321):
+    """Cold start: the first starmap_solver call of two new processes, the
+    first with an empty kernel cache (NVRTC compiles), the second with the
+    cache the first one wrote."""
+    import shutil
+    d = os.path.join(ROOT, "_build", "bench_cold_cache")
+    shutil.rmtree(d, ignore_errors=True)
+    res = []
+    for _ in range(2):
+        env = dict(os.environ, SMG_JIT_CACHE_DIR=d)
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cold-call"], env=env,
+                           capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            return {"error": r.stderr[-500:]}
+        res.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    shutil.rmtree(d, ignore_errors=True)
+    mk = lambda r: {"value": upd_step * nsteps / r["seconds"], "unit": UNIT, "seconds": r["seconds"],
+                    "programs_compiled": r["programs_compiled"], "programs_from_disk": r["programs_from_disk"]}
+    return {"what": "first starmap_solver call of a new process, starmap_init to the returned output, "
+                    f"{nsteps} steps, host setup, compilation or cache load, transfers included",
+            "empty_cache": mk(res[0]), "warm_cache": mk(res[1])}
+
+
 def host_buffers(S):
     """Initial state and output buffers per component in pinned host memory
     (page-locked through torch; pageable numpy arrays if that is unavailable)."""
@@ -418,7 +464,11 @@ def main():
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D P9 measurement")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline stepping")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of reference-arm stepping")
+    ap.add_argument("--no-cold", action="store_true", help="skip the cold-start measurement")
+    ap.add_argument("--cold-call", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cold_call:
+        return cold_call()
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
@@ -509,6 +559,8 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
+    if world == 1 and not args.no_cold and e2e:
+        line["e2e"]["cold"] = bench_cold(upd_step)
     if world == 1 and not args.no_batch:
         line["batched"] = bench_batch()
     if world == 1 and not args.no_adjoint:

@@ -234,6 +234,15 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap);
 int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune, int32_t compile,
                    char* buf, int64_t cap, int64_t* len);
 
+/* Process-wide counts of generated-kernel programs compiled with NVRTC and
+ * of programs loaded from the on-disk cache instead.  Compiled kernels are
+ * kept in $SMG_JIT_CACHE_DIR (else $XDG_CACHE_HOME/starmap_b200, else
+ * $HOME/.cache/starmap_b200), keyed by their source, compile options and the
+ * NVRTC and library versions, so that a new process (a new MATLAB session)
+ * does not compile the same problem's kernels again; SMG_JIT_CACHE=0 turns
+ * the cache off.  No reference counterpart. */
+int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
+
 /* Tuning parameters of the kernels (no reference counterpart).  They change
  * performance only, never results.  Keys: */
 #define SMG_TUNE_PAIR_GROUP  1   /* destinations per CTA of the pair kernel (1..256) */

@@ -120,6 +120,7 @@ SIGNATURES = {
     "smg_adjoint_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "smg_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_active_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_char_p, C.c_int64]),
+    "smg_jit_stats": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_jit_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32,
                                  C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),

@@ -38,8 +38,11 @@
 // keeps the precompiled kernels.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <atomic>
 #include <cinttypes>
 #include <cmath>
@@ -81,6 +84,7 @@ struct Api {
     nvrtcResult_t (*GetCUBIN)(nvrtcProgram_t, char*) = nullptr;
     nvrtcResult_t (*DestroyProgram)(nvrtcProgram_t*) = nullptr;
     const char* (*GetErrorString)(nvrtcResult_t) = nullptr;
+    nvrtcResult_t (*Version)(int*, int*) = nullptr;
     bool link_ok = false;
     std::string link_why;
     nvJitLinkResult_t (*LinkCreate)(nvJitLinkHandle_t*, uint32_t, const char**) = nullptr;
@@ -142,7 +146,7 @@ void load_api() {
                sym(nv, "nvrtcGetProgramLogSize", a.GetProgramLogSize) &&
                sym(nv, "nvrtcGetProgramLog", a.GetProgramLog) && sym(nv, "nvrtcGetCUBINSize", a.GetCUBINSize) &&
                sym(nv, "nvrtcGetCUBIN", a.GetCUBIN) && sym(nv, "nvrtcDestroyProgram", a.DestroyProgram) &&
-               sym(nv, "nvrtcGetErrorString", a.GetErrorString)) {
+               sym(nv, "nvrtcGetErrorString", a.GetErrorString) && sym(nv, "nvrtcVersion", a.Version)) {
         a.ok = true;
     } else {
         a.why = "NVRTC entry points missing";
@@ -2316,13 +2320,110 @@ std::vector<KernelSrc> fam_programs(const smg_handle* h, int block, int group, i
 
 std::map<std::string, std::vector<std::vector<char>>> g_cubins;   // sources -> cubins, process-wide
 std::mutex g_cubin_mu;
+std::atomic<long long> g_programs_compiled(0), g_programs_from_disk(0);
+
+// ---- on-disk cache of compiled kernels ----------------------------------------
+// A process's first compilation of a problem's kernels takes seconds (NVRTC on
+// all host threads); a MATLAB session calling starmap_solver would pay it on
+// every first call.  The cubins are therefore also kept on disk, one file per
+// (sources, options, NVRTC version, library version), named by two 64-bit
+// FNV-1a hashes of that key and holding the key's length for a check.
+// Directory: $SMG_JIT_CACHE_DIR, else $XDG_CACHE_HOME/starmap_b200, else
+// $HOME/.cache/starmap_b200; SMG_JIT_CACHE=0 turns the cache off.  Files are
+// written to a temporary name and renamed, so concurrent processes see whole
+// files only.
+unsigned long long fnv1a(const std::string& s, unsigned long long h) {
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+std::string cache_dir() {
+    const char* off = std::getenv("SMG_JIT_CACHE");
+    if (off && std::string(off) == "0") return "";
+    if (const char* d = std::getenv("SMG_JIT_CACHE_DIR")) return *d ? std::string(d) : "";
+    if (const char* x = std::getenv("XDG_CACHE_HOME"))
+        if (*x) return std::string(x) + "/starmap_b200";
+    if (const char* hm = std::getenv("HOME"))
+        if (*hm) return std::string(hm) + "/.cache/starmap_b200";
+    return "";
+}
+
+// mkdir -p
+bool make_dirs(const std::string& d) {
+    for (size_t i = 1; i <= d.size(); ++i)
+        if (i == d.size() || d[i] == '/') {
+            const std::string p = d.substr(0, i);
+            if (mkdir(p.c_str(), 0755) != 0 && errno != EEXIST) return false;
+        }
+    return true;
+}
+
+std::string cache_file(const std::string& key) {
+    const std::string d = cache_dir();
+    if (d.empty()) return "";
+    char name[64];
+    std::snprintf(name, sizeof name, "/%016llx%016llx.cubins", fnv1a(key, 1469598103934665603ull),
+                  fnv1a(key, 0x9e3779b97f4a7c15ull));
+    return d + name;
+}
+
+bool cache_load(const std::string& key, std::vector<std::vector<char>>& out) {
+    const std::string f = cache_file(key);
+    if (f.empty()) return false;
+    FILE* fp = std::fopen(f.c_str(), "rb");
+    if (!fp) return false;
+    char magic[8] = {0};
+    unsigned long long klen = 0, n = 0;
+    bool ok = std::fread(magic, 1, 8, fp) == 8 && std::memcmp(magic, "SMGCUB1\n", 8) == 0 &&
+              std::fread(&klen, sizeof klen, 1, fp) == 1 && klen == key.size() && std::fread(&n, sizeof n, 1, fp) == 1 &&
+              n < (1u << 16);
+    std::vector<std::vector<char>> v;
+    for (unsigned long long i = 0; ok && i < n; ++i) {
+        unsigned long long sz = 0;
+        ok = std::fread(&sz, sizeof sz, 1, fp) == 1 && sz < (1ull << 31);
+        if (!ok) break;
+        v.emplace_back(sz);
+        ok = std::fread(v.back().data(), 1, sz, fp) == sz;
+    }
+    std::fclose(fp);
+    if (!ok) return false;
+    out = std::move(v);
+    return true;
+}
+
+void cache_store(const std::string& key, const std::vector<std::vector<char>>& cub) {
+    const std::string f = cache_file(key);
+    if (f.empty() || !make_dirs(cache_dir())) return;
+    const std::string tmp = f + "." + std::to_string((long long)getpid()) + ".tmp";
+    FILE* fp = std::fopen(tmp.c_str(), "wb");
+    if (!fp) return;
+    const unsigned long long klen = key.size(), n = cub.size();
+    bool ok = std::fwrite("SMGCUB1\n", 1, 8, fp) == 8 && std::fwrite(&klen, sizeof klen, 1, fp) == 1 &&
+              std::fwrite(&n, sizeof n, 1, fp) == 1;
+    for (const auto& c : cub) {
+        const unsigned long long sz = c.size();
+        ok = ok && std::fwrite(&sz, sizeof sz, 1, fp) == 1 && std::fwrite(c.data(), 1, sz, fp) == sz;
+    }
+    ok = std::fclose(fp) == 0 && ok;
+    if (ok) ok = std::rename(tmp.c_str(), f.c_str()) == 0;
+    if (!ok) std::remove(tmp.c_str());
+}
 
 // Compile the programs on all host threads; for the calls layout link them
 // into one cubin, for the inline layout keep one cubin per program.  Cached
 // per process by source text and options.
 int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std::vector<std::vector<char>>& out,
                      std::string& err) {
+    Api& a = api();
     std::string key = "regs " + std::to_string(regs) + (calls ? " calls\n" : " inline\n");
+    {
+        int major = 0, minor = 0;
+        if (a.ok) a.Version(&major, &minor);
+        key += "nvrtc " + std::to_string(major) + "." + std::to_string(minor) + " " + smg_version() + "\n";
+    }
     for (const auto& k : P) key += k.src;
     {
         std::lock_guard<std::mutex> lk(g_cubin_mu);
@@ -2332,7 +2433,12 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
             return SMG_OK;
         }
     }
-    Api& a = api();
+    if (a.ok && cache_load(key, out)) {
+        g_programs_from_disk += (long long)P.size();
+        std::lock_guard<std::mutex> lk(g_cubin_mu);
+        g_cubins[key] = out;
+        return SMG_OK;
+    }
     if (!a.ok) {
         err = a.why;
         return SMG_EINVAL;
@@ -2389,6 +2495,8 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
         a.LinkedCubin(L, out[0].data());
         a.LinkDestroy(&L);
     }
+    g_programs_compiled += (long long)P.size();
+    cache_store(key, out);
     std::lock_guard<std::mutex> lk(g_cubin_mu);
     g_cubins[key] = out;
     return SMG_OK;
@@ -3203,4 +3311,10 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
     }
     delete h;
     return rc;
+}
+
+extern "C" int smg_jit_stats(int64_t* compiled, int64_t* from_disk) {
+    if (compiled) *compiled = g_programs_compiled.load();
+    if (from_disk) *from_disk = g_programs_from_disk.load();
+    return SMG_OK;
 }

@@ -128,3 +128,51 @@ def test_generated_source_is_deterministic(name):
     _source("odd_mixed_bc", split=4)
     _, b = _source(name, split=16)
     assert a == b
+
+
+_CACHE_PROBE = r"""
+import ctypes, json, sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+from test_cpu_jit import _source
+from starmap_b200 import _lib
+_source("lattice_p5_substep", compile=True, split=2)
+c, d = ctypes.c_int64(), ctypes.c_int64()
+_lib.lib().smg_jit_stats(ctypes.byref(c), ctypes.byref(d))
+print(json.dumps([c.value, d.value]))
+"""
+
+
+def test_compiled_kernels_are_cached_on_disk_across_processes():
+    """A second process generating the same problem's kernels loads them from
+    the on-disk cache instead of compiling (smg_jit_stats); SMG_JIT_CACHE=0
+    compiles again and writes nothing."""
+    import json
+    import os
+    import shutil
+    import subprocess
+    import sys
+    if not _nvrtc_available():
+        pytest.skip("NVRTC library not present")
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    d = os.path.join(root, "_build", "cache_test_%d" % os.getpid())
+    shutil.rmtree(d, ignore_errors=True)
+    code = _CACHE_PROBE.format(root=root, tests=here)
+
+    def run(**env):
+        e = dict(os.environ, SMG_JIT_CACHE_DIR=d, **env)
+        out = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+        return json.loads(out.stdout.strip().splitlines()[-1])
+
+    try:
+        compiled, from_disk = run()
+        assert compiled > 0 and from_disk == 0
+        assert len([f for f in os.listdir(d) if f.endswith(".cubins")]) == 1
+        compiled, from_disk = run()
+        assert compiled == 0 and from_disk > 0
+        shutil.rmtree(d)
+        compiled, from_disk = run(SMG_JIT_CACHE="0")
+        assert compiled > 0 and from_disk == 0 and not os.path.exists(d)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
