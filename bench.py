@@ -312,6 +312,19 @@ def bench_adjoint(nsteps: int = 400, n: int = 200, ckpts=(0, 20)):
         ad += float(np.sum(gv * bump(Y, Z).reshape(np.shape(gv), order="F")))
     out.update({"n_sys": Sx.n_sys, "fd_directional": fd, "adjoint_directional": ad,
                 "fd_rel_err": abs(fd - ad) / abs(fd)})
+    # 32 such inverse problems batched (each its own observations), checkpoints every 20 steps
+    from starmap_b200.adjoint import batched_gradients
+    n_inst, threads = 32, 16
+    try:
+        grads, tf, tb = batched_gradients([par] * n_inst, [obs * (1.0 + 0.01 * i) for i in range(n_inst)], nsteps,
+                                          ckpt_every=20, threads=threads)
+        out["batch32"] = {"instances": n_inst, "ckpt_every": 20, "host_threads": threads, "forward_s": tf,
+                          "backward_s": tb, "gradients_per_s": n_inst / (tf + tb),
+                          "gradient_ms_per_instance": (tf + tb) / n_inst * 1e3,
+                          "gradient_over_plain_forward": (tf + tb) / n_inst / (plain_ms / 1e3),
+                          "finite": bool(all(np.all(np.isfinite(g["sigma_a"][(1, 1, 1)])) for g in grads))}
+    except Exception as e:   # e.g. not enough device memory for 32 recordings
+        out["batch32"] = {"instances": n_inst, "error": str(e)[:300]}
     return out
 
 

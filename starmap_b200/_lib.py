@@ -41,6 +41,7 @@ SMG_TUNE_JIT_STAGED = 16
 SMG_TUNE_JIT_SLICES = 17
 SMG_TUNE_JIT_STAGES = 18
 SMG_TUNE_JIT_ROWS = 19
+SMG_TUNE_ADJ_PRIORITY = 20
 
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1

@@ -858,7 +858,13 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
             A_CUDA(h, cudaMalloc(&A->rec_state2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->rec_w2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->work2, sb));
-            A_CUDA(h, cudaStreamCreateWithFlags(&A->rstream, cudaStreamNonBlocking));
+            if (h->adj_priority) {
+                int least = 0, greatest = 0;
+                A_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+                A_CUDA(h, cudaStreamCreateWithPriority(&A->rstream, cudaStreamNonBlocking, greatest));
+            } else {
+                A_CUDA(h, cudaStreamCreateWithFlags(&A->rstream, cudaStreamNonBlocking));
+            }
             for (int b = 0; b < 2; ++b) {
                 A_CUDA(h, cudaEventCreateWithFlags(&A->ev_rec[b], cudaEventDisableTiming));
                 A_CUDA(h, cudaEventCreateWithFlags(&A->ev_free[b], cudaEventDisableTiming));

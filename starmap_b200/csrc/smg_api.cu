@@ -1390,6 +1390,10 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             if (value < -1 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: graph steps must be -1..4096");
             h->graph_block = value;
             break;
+        case SMG_TUNE_ADJ_PRIORITY:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj priority must be 0 or 1");
+            h->adj_priority = value;
+            return SMG_OK;
         case SMG_TUNE_ADJ_FUSED:
             if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj_fused must be 0 or 1");
             h->adj_fused = value;

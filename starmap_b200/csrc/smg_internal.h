@@ -138,6 +138,7 @@ struct smg_handle {
     bool strip_staged = false;       // stage slot-job loads with cp.async
     smg::AdjData* adj = nullptr;     // adjoint checkpoints and buffers (smg_forward)
     int adj_fused = 1;               // smg_backward kernel form (SMG_TUNE_ADJ_FUSED)
+    int adj_priority = 0;            // recompute stream at the highest priority (SMG_TUNE_ADJ_PRIORITY)
     smg::JitState* jit = nullptr;    // problem-specialised kernels (SMG_VARIANT_JIT)
     smg::JitState* jit_rec = nullptr;  // the same with adjoint recording (smg_forward / smg_backward)
     smg::JitState* jit_adj = nullptr;  // generated backward-phase kernels (smg_backward)
