@@ -250,8 +250,9 @@ int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
 #define SMG_TUNE_PAIR_UNROLL 3   /* couplings per inner iteration (1 or 2) */
 #define SMG_TUNE_PAIR_MINB   4   /* register budget: 3 or 4 resident CTAs of 256 threads (64/85 regs) */
 #define SMG_TUNE_ADJ_FUSED   5   /* smg_backward: 1 = one fused kernel per phase (default), 0 = pointwise + transpose kernels */
-#define SMG_TUNE_ADJ_PRIORITY 20 /* smg_backward: 1 = segments are recomputed on a stream of the device's highest
-                                    priority, 0 (default) = default priority; set before smg_forward */
+#define SMG_TUNE_ADJ_PRIORITY 20 /* smg_backward stream priorities, set before smg_forward: 0 (default) recompute and
+                                    sweep at the default priority, 1 recompute at the device's highest priority, 2
+                                    the sweep on a stream of the highest priority above the recompute */
 #define SMG_TUNE_JIT_BLOCK   6   /* threads per CTA of the generated kernels (32..256, multiple of 32) */
 #define SMG_TUNE_JIT_GROUP   7   /* destinations per CTA of the generated kernels (1..256) */
 #define SMG_TUNE_JIT_REGS    8   /* register limit per thread of the generated kernels (0: compiler's choice, else 32..255) */

@@ -78,6 +78,8 @@ struct AdjData {
     double* rec_w2 = nullptr;
     double* work2 = nullptr;
     cudaStream_t rstream = nullptr;
+    cudaStream_t sstream = nullptr;            // the sweep's stream at the highest priority (SMG_TUNE_ADJ_PRIORITY 2)
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaEvent_t ev_rec[2] = {nullptr, nullptr};    // recording into buffer b complete
     cudaEvent_t ev_free[2] = {nullptr, nullptr};   // adjoint done reading buffer b
     int maxdest = 0;
@@ -514,6 +516,9 @@ void free_adj(smg_handle* h) {
     cudaFree(A->rec_w2);
     cudaFree(A->work2);
     if (A->rstream) cudaStreamDestroy(A->rstream);
+    if (A->sstream) cudaStreamDestroy(A->sstream);
+    if (A->ev_in) cudaEventDestroy(A->ev_in);
+    if (A->ev_out) cudaEventDestroy(A->ev_out);
     for (int b = 0; b < 2; ++b) {
         if (A->ev_rec[b]) cudaEventDestroy(A->ev_rec[b]);
         if (A->ev_free[b]) cudaEventDestroy(A->ev_free[b]);
@@ -715,6 +720,13 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         return A->d_dests[0] + (kind == 0 ? 0 : (kind == 3 ? nA : 2 * nA));
     };
     auto substeps = [](int kind) { return kind < 0 ? 0 : (kind == 1 || kind == 2 ? 2 : 1); };
+    // the sweep's stream: the handle's, or one of the highest priority joined to it
+    cudaStream_t ss = A->sstream ? A->sstream : h->stream;
+    if (A->sstream) {
+        cudaError_t r = cudaEventRecord(A->ev_in, h->stream);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(ss, A->ev_in, 0);
+        if (r != cudaSuccess) return r;
+    }
     // targets l: 0 = sources of an A phase (B destinations), 1 = sources of a B phase
     auto launch = [&](int l, int coup, int pkind, const double* pre, const double* W, int nkind) -> cudaError_t {
         if (A->srcs[l].empty()) return cudaSuccess;
@@ -723,7 +735,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
             auto swap = [](int kind) { return kind == 2 || kind == 3 ? 1 : 0; };
             *launches += smg::jit_adj_launches(h, l);
             return smg::launch_jit_adj(h, l, coup, substeps(pkind), swap(pkind), substeps(nkind), swap(nkind), A->lam,
-                                       A->dDE, A->dG, pre, W, h->stream);
+                                       A->dDE, A->dG, pre, W, ss);
         }
         const dim3 grid(nbp, (unsigned)A->srcs[l].size());
         const int PM = substeps(pkind), NM = substeps(nkind);
@@ -731,7 +743,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         const smg::AdjDest* nt = table(nkind);
 #define SMG_FUSED(P, N)                                                                                 \
     if (PM == P && NM == N)                                                                             \
-        smg::k_adj_fused<P, N><<<grid, 128, 0, h->stream>>>(h->g, A->d_srcs[l], A->d_tcoup[l], coup, pt, pre, W, \
+        smg::k_adj_fused<P, N><<<grid, 128, 0, ss>>>(h->g, A->d_srcs[l], A->d_tcoup[l], coup, pt, pre, W, \
                                                             nt, A->lam, h->hdt);
         SMG_FUSED(0, 0) SMG_FUSED(0, 1) SMG_FUSED(0, 2) SMG_FUSED(1, 0) SMG_FUSED(1, 1) SMG_FUSED(1, 2)
         SMG_FUSED(2, 0) SMG_FUSED(2, 1) SMG_FUSED(2, 2)
@@ -751,7 +763,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
     auto recompute = [&](int64_t s) -> cudaError_t {
         const int b = buf(s);
         const int64_t ks = std::min<int64_t>(A->K, A->nsteps - s * A->K);
-        cudaStream_t st = dbl ? A->rstream : h->stream;
+        cudaStream_t st = dbl ? A->rstream : ss;
         cudaError_t r;
         if (dbl && (r = cudaStreamWaitEvent(st, A->ev_free[b], 0)) != cudaSuccess) return r;
         if ((r = cudaMemcpyAsync(WK[b], A->ckpt[s], sb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return r;
@@ -762,8 +774,8 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
     };
     if (dbl) {
         // the recompute stream starts after the work already queued on the handle's stream
-        if ((e = cudaEventRecord(A->ev_free[1], h->stream)) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(A->ev_free[0], h->stream)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(A->ev_free[1], ss)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(A->ev_free[0], ss)) != cudaSuccess) return e;
     }
     if (!A->tail_valid && (e = recompute(A->nseg - 1)) != cudaSuccess) return e;
     // the adjoint seed of the last phase's (A(k=2)) destinations, scaled
@@ -774,7 +786,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         const bool last = s == A->nseg - 1;
         const int b = buf(s);
         if (s >= 1 && (e = recompute(s - 1)) != cudaSuccess) return e;   // overlaps this segment's sweep
-        if (dbl && !(last && A->tail_valid) && (e = cudaStreamWaitEvent(h->stream, A->ev_rec[b], 0)) != cudaSuccess)
+        if (dbl && !(last && A->tail_valid) && (e = cudaStreamWaitEvent(ss, A->ev_rec[b], 0)) != cudaSuccess)
             return e;
         for (int64_t l = last ? 2 * ks : 2 * ks - 1; l >= 0; --l) {
             const int64_t p = l + 1;   // the phase after l (its pointwise part is pending)
@@ -787,10 +799,15 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
                        pkind < 0 ? nullptr : slot(RW[b], p), nkind);
             if (e != cudaSuccess) return e;
         }
-        if (dbl && s >= 1 && (e = cudaEventRecord(A->ev_free[b], h->stream)) != cudaSuccess) return e;
+        if (dbl && s >= 1 && (e = cudaEventRecord(A->ev_free[b], ss)) != cudaSuccess) return e;
     }
     // the first phase's (A(k=1)) pointwise part on its destinations
-    return launch(1, 0, 0, slot(RS[buf(0)], 0), slot(RW[buf(0)], 0), -1);
+    if ((e = launch(1, 0, 0, slot(RS[buf(0)], 0), slot(RW[buf(0)], 0), -1)) != cudaSuccess) return e;
+    if (A->sstream) {
+        if ((e = cudaEventRecord(A->ev_out, ss)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(h->stream, A->ev_out, 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -858,12 +875,14 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
             A_CUDA(h, cudaMalloc(&A->rec_state2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->rec_w2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->work2, sb));
-            if (h->adj_priority) {
-                int least = 0, greatest = 0;
-                A_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
-                A_CUDA(h, cudaStreamCreateWithPriority(&A->rstream, cudaStreamNonBlocking, greatest));
-            } else {
-                A_CUDA(h, cudaStreamCreateWithFlags(&A->rstream, cudaStreamNonBlocking));
+            int least = 0, greatest = 0;
+            A_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            A_CUDA(h, cudaStreamCreateWithPriority(&A->rstream, cudaStreamNonBlocking,
+                                                   h->adj_priority == 1 ? greatest : least));
+            if (h->adj_priority == 2) {   // the sweep above the recompute
+                A_CUDA(h, cudaStreamCreateWithPriority(&A->sstream, cudaStreamNonBlocking, greatest));
+                A_CUDA(h, cudaEventCreateWithFlags(&A->ev_in, cudaEventDisableTiming));
+                A_CUDA(h, cudaEventCreateWithFlags(&A->ev_out, cudaEventDisableTiming));
             }
             for (int b = 0; b < 2; ++b) {
                 A_CUDA(h, cudaEventCreateWithFlags(&A->ev_rec[b], cudaEventDisableTiming));

@@ -1391,7 +1391,7 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->graph_block = value;
             break;
         case SMG_TUNE_ADJ_PRIORITY:
-            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: adj priority must be 0 or 1");
+            if (value < 0 || value > 2) return fail(h, SMG_EINVAL, "smg_tune: adj priority must be 0, 1 or 2");
             h->adj_priority = value;
             return SMG_OK;
         case SMG_TUNE_ADJ_FUSED:

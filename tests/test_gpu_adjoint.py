@@ -273,3 +273,31 @@ def test_batched_gradients_match_one_at_a_time():
         for key in ("sigma_a", "sigma_s0"):
             for grid, v in ref[key].items():
                 np.testing.assert_array_equal(g[key][grid], v)
+
+
+@pytest.mark.parametrize("prio", [1, 2])
+def test_stream_priorities_do_not_change_gradient(prio):
+    """SMG_TUNE_ADJ_PRIORITY (recompute stream above the sweep, or the sweep on
+    a stream of the highest priority) reorders only the overlap of recompute
+    and sweep: gradients equal the default's to 1e-12 (atomics may sum in
+    another order)."""
+    S, fs = adjoint_problem(n=10, N=5)
+    res = []
+    for p in (0, prio):
+        solver, T = make_solver(S, fs)
+        try:
+            solver.tune(_lib.SMG_TUNE_ADJ_PRIORITY, p)
+            solver.set_state(S.U0)
+            solver.set_dt(fs["dt"])
+            solver.forward(11, 3)
+            u = solver.get_state([0])[0]
+            solver.misfit(0.9 * u)
+            res.append(solver.backward(fields=[T.index[("sA",)]]))
+        finally:
+            solver.close()
+    (gU0, gF0), (gU1, gF1) = res
+    for j in gU0:
+        np.testing.assert_allclose(gU1[j], gU0[j], rtol=0, atol=1e-12 * max(np.abs(gU0[j]).max(), 1e-300))
+    for k in gF0:
+        a, b = np.asarray(gF0[k]), np.asarray(gF1[k])
+        np.testing.assert_allclose(b, a, rtol=0, atol=1e-12 * max(np.abs(a).max(), 1e-300))
