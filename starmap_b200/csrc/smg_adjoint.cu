@@ -98,6 +98,10 @@ struct AdjData {
     DevField* dDE = nullptr;       // per field: d(decay)/d(sigma) (array slot or scalar), generated kernels
     double** dG = nullptr;         // per field: gradient slot or nullptr, generated kernels
     size_t bytes = 0;
+    // generated recording and sweep: the recording holds each destination's
+    // sigma-gradient factor per phase (rec_w) and no values before the phase
+    // (rec_state stays unallocated); the precompiled kernels record both
+    bool ds = false;
 };
 
 // phi'(x) for phi(x) = (exp(x)-1)/x with the reference's Taylor branch
@@ -468,8 +472,9 @@ smg::PairArgs rec_args(const smg_handle* h, int phase, double* U, double* wrec, 
     return a;
 }
 
-cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec, cudaStream_t st) {
-    if (h->jit_rec) return smg::launch_jit_rec(h, mode, kf, U, wrec, prec, st);
+cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double* wrec, double* prec, int dsm, int dsw,
+                       cudaStream_t st) {
+    if (h->adj && h->adj->ds) return smg::launch_jit_rec(h, mode, kf, U, wrec, prec, h->adj->dDE, dsm, dsw, st);
     const int phase = mode == 1 ? 1 : 0;
     const smg::PairArgs a = rec_args(h, phase, U, wrec, prec);
     if (a.ndest == 0) return cudaSuccess;
@@ -488,16 +493,25 @@ cudaError_t launch_rec(const smg_handle* h, int mode, int kf, double* U, double*
 
 // One segment of ks steps from state U with recording, in smg_run's phase
 // order: A(k=1), then per step B and the fused A(k=2)A(k=1) -- A(k=2) alone
-// after the last step.  Phase r records into slot r (2ks+1 slots).
-cudaError_t record_segment(smg_handle* h, int64_t ks, double* U, double* rec_w, double* rec_state, cudaStream_t st) {
+// after the last step.  Phase r records into slot r (2ks+1 slots).  The
+// sweep reads each slot as the phase kind it has there, which the
+// sigma-gradient factor recorded by the generated kernels must follow: one
+// substep for the first A(k=1) and for the run's final A(k=2) (last segment),
+// two for B, for the fused A-A and for a segment's closing A(k=2), which the
+// sweep fuses with the next segment's A(k=1); first filter k=2 for the A
+// phases after the first.
+cudaError_t record_segment(smg_handle* h, int64_t ks, double* U, double* rec_w, double* rec_state, cudaStream_t st,
+                           bool last) {
     const AdjData* A = h->adj;
     const size_t vb = (size_t)h->g.cs * std::max(A->maxdest, 1) * sizeof(double);
     for (int64_t r = 0; r <= 2 * ks; ++r) {
         const int kind = r == 0 ? 0 : (r & 1 ? 1 : (r < 2 * ks ? 2 : 3));
         const int mode = kind == 1 ? 1 : (kind == 2 ? 2 : 0);
         const int kf = kind == 3 ? 2 : 1;
+        const int dsm = (kind == 1 || kind == 2 || (kind == 3 && !last)) ? 2 : 1;
+        const int dsw = (kind == 2 || kind == 3) ? 1 : 0;
         const cudaError_t e = launch_rec(h, mode, kf, U, (double*)((char*)rec_w + vb * r),
-                                         (double*)((char*)rec_state + vb * r), st);
+                                         rec_state ? (double*)((char*)rec_state + vb * r) : nullptr, dsm, dsw, st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -662,7 +676,7 @@ cudaError_t backward_split(smg_handle* h, int64_t* launches) {
         if (!(s == A->nseg - 1 && A->tail_valid)) {
             cudaError_t e = cudaMemcpyAsync(A->work, A->ckpt[s], sb, cudaMemcpyDeviceToDevice, h->stream);
             if (e != cudaSuccess) return e;
-            e = record_segment(h, ks, A->work, A->rec_w, A->rec_state, h->stream);
+            e = record_segment(h, ks, A->work, A->rec_w, A->rec_state, h->stream, s == A->nseg - 1);
             if (e != cudaSuccess) return e;
             *launches += 2 * ks + 1;
         }
@@ -730,7 +744,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
     // targets l: 0 = sources of an A phase (B destinations), 1 = sources of a B phase
     auto launch = [&](int l, int coup, int pkind, const double* pre, const double* W, int nkind) -> cudaError_t {
         if (A->srcs[l].empty()) return cudaSuccess;
-        if (h->jit_adj && (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_JIT)) {
+        if (A->ds) {
             // kind -> (substeps, filters in k=2, k=1 order)
             auto swap = [](int kind) { return kind == 2 || kind == 3 ? 1 : 0; };
             *launches += smg::jit_adj_launches(h, l);
@@ -751,7 +765,9 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         ++*launches;
         return cudaGetLastError();
     };
-    auto slot = [&](const double* base, int64_t r) { return (const double*)((const char*)base + vb * r); };
+    auto slot = [&](const double* base, int64_t r) {
+        return base ? (const double*)((const char*)base + vb * r) : nullptr;
+    };
     // recording buffer of segment s (the last segment uses the first, which
     // smg_forward filled); with one buffer everything runs on the handle's stream
     const bool dbl = A->rec_w2 != nullptr;
@@ -767,7 +783,7 @@ cudaError_t backward_fused(smg_handle* h, int64_t* launches) {
         cudaError_t r;
         if (dbl && (r = cudaStreamWaitEvent(st, A->ev_free[b], 0)) != cudaSuccess) return r;
         if ((r = cudaMemcpyAsync(WK[b], A->ckpt[s], sb, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return r;
-        if ((r = record_segment(h, ks, WK[b], RW[b], RS[b], st)) != cudaSuccess) return r;
+        if ((r = record_segment(h, ks, WK[b], RW[b], RS[b], st, s == A->nseg - 1)) != cudaSuccess) return r;
         *launches += 2 * ks + 1;
         if (dbl && (r = cudaEventRecord(A->ev_rec[b], st)) != cudaSuccess) return r;
         return cudaSuccess;
@@ -865,14 +881,11 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
         A_CUDA(h, cudaMalloc(&A->work, sb));
         A_CUDA(h, cudaMalloc(&A->lam, sb));
         A_CUDA(h, cudaMalloc(&A->V, vb));
-        A_CUDA(h, cudaMalloc(&A->rec_state, vb * (2 * K + 1)));
         A_CUDA(h, cudaMalloc(&A->rec_w, vb * (2 * K + 1)));
         A_CUDA(h, cudaMemsetAsync(A->V, 0, vb, h->stream));
         A_CUDA(h, cudaMemsetAsync(A->rec_w, 0, vb * (2 * K + 1), h->stream));
-        A_CUDA(h, cudaMemsetAsync(A->rec_state, 0, vb * (2 * K + 1), h->stream));
-        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3);
+        A->bytes = sb * (nseg + 2) + vb * (2 * K + 2);
         if (nseg > 1) {   // second recording: recompute overlapped with the sweep
-            A_CUDA(h, cudaMalloc(&A->rec_state2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->rec_w2, vb * (2 * K + 1)));
             A_CUDA(h, cudaMalloc(&A->work2, sb));
             int least = 0, greatest = 0;
@@ -888,12 +901,13 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
                 A_CUDA(h, cudaEventCreateWithFlags(&A->ev_rec[b], cudaEventDisableTiming));
                 A_CUDA(h, cudaEventCreateWithFlags(&A->ev_free[b], cudaEventDisableTiming));
             }
-            A->bytes += sb + vb * (4 * K + 2);
+            A->bytes += sb + vb * (2 * K + 1);
         }
     } else {
         for (double* p : A->gfield) cudaFree(p);
         for (double* p : A->dEslot) cudaFree(p);
-        A->bytes = sb * (nseg + 2) + vb * (4 * K + 3) + (nseg > 1 ? sb + vb * (4 * K + 2) : 0);
+        A->bytes = sb * (nseg + 2) + vb * (2 * K + 2) + (nseg > 1 ? sb + vb * (2 * K + 1) : 0) +
+                   (A->rec_state ? vb * (2 * K + 1) * (nseg > 1 ? 2 : 1) : 0);
     }
     A->nsteps = nsteps;
     A->ready = false;
@@ -953,6 +967,21 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
             h->jit_err = why;
         }
     }
+    // the generated recording and fused sweep keep one value per destination
+    // and phase; the precompiled kernels (and the split sweep) need the values
+    // before each phase as well
+    A->ds = (h->variant == SMG_VARIANT_AUTO || h->variant == SMG_VARIANT_JIT) && !h->jit_failed && h->jit_rec &&
+            h->jit_adj && h->adj_fused && !h->jit_calls;
+    if (!A->ds && !A->rec_state) {
+        A_CUDA(h, cudaMalloc(&A->rec_state, vb * (2 * A->K + 1)));
+        A_CUDA(h, cudaMemsetAsync(A->rec_state, 0, vb * (2 * A->K + 1), h->stream));
+        A->bytes += vb * (2 * A->K + 1);
+        if (A->nseg > 1) {
+            A_CUDA(h, cudaMalloc(&A->rec_state2, vb * (2 * A->K + 1)));
+            A_CUDA(h, cudaMemsetAsync(A->rec_state2, 0, vb * (2 * A->K + 1), h->stream));
+            A->bytes += vb * (2 * A->K + 1);
+        }
+    }
     for (int l = 0; l < 2; ++l)
         for (const auto& sr : A->srcs[l])
             if (sr.pslot < 0) return afail(h, SMG_EINVAL, "smg_forward: a component is no phase's destination");
@@ -967,7 +996,7 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
             rc = smg::run_steps(h, ks, false);
             if (rc != SMG_OK) return rc;
         } else {
-            A_CUDA(h, record_segment(h, ks, h->dU, A->rec_w, A->rec_state, h->stream));
+            A_CUDA(h, record_segment(h, ks, h->dU, A->rec_w, A->rec_state, h->stream, true));
             h->last_launches += 2 * ks + 1;
         }
     }
@@ -1039,7 +1068,8 @@ int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fiel
         if (g) A_CUDA(h, cudaMemsetAsync(g, 0, (size_t)h->g.cs * sizeof(double), h->stream));
     A_CUDA(h, cudaEventRecord(h->ev0, h->stream));
     int64_t launches = 0;
-    const cudaError_t e = h->adj_fused ? backward_fused(h, &launches) : backward_split(h, &launches);
+    // a forward recorded for the generated fused sweep is swept by it
+    const cudaError_t e = (A->ds || h->adj_fused) ? backward_fused(h, &launches) : backward_split(h, &launches);
     if (e != cudaSuccess) return acuda(h, e, "smg_backward");
     A_CUDA(h, cudaEventRecord(h->ev1, h->stream));
     h->last_launches = launches;

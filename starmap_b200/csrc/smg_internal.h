@@ -186,8 +186,10 @@ void jit_family_free(JitFamilySet*& S);
 cudaError_t jit_family_geometry(JitFamilySet* S, const std::vector<smg_handle*>& inst, cudaStream_t s);
 cudaError_t jit_family_phase(JitFamilySet* S, int mode, int kfilter, cudaStream_t s, int64_t* launches);
 int jit_family_count(const JitFamilySet* S);
+// generated recording kernels: each destination's sigma-gradient factor for a phase of dsm substeps whose
+// first filter is k=2 when dsw, into wrec (prec unused)
 cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U, double* wrec, double* prec,
-                           cudaStream_t s);
+                           const DevField* DE, int dsm, int dsw, cudaStream_t s);
 std::string jit_source(const smg_handle* h, int block, int group);
 int jit_compile(const smg_handle* h, int block, int group, std::string& err);   // compile only (no device)
 int jit_launches(const smg_handle* h, int phase);                                 // kernels per phase

@@ -228,6 +228,20 @@ static __device__ __forceinline__ const double* fp(const DevField* F, int i) {
 static __device__ __forceinline__ double fs(const DevField* F, int i) { return __ldg(&F[i].s); }
 // request a line into L2 ahead of its load (no register, no wait)
 static __device__ __forceinline__ void pf(const void* p) { asm volatile("prefetch.global.L2 [%0];" :: "l"(p)); }
+// the sigma-gradient factor of a destination's phase (one substep: M = 1, two:
+// M = 2, F1 the first substep's filter) from its value before the phase u and
+// coupling sum w: the adjoint sweep adds factor * Y to dJ/dsigma; the same
+// expressions as the sweep's own evaluation from recorded u and w
+static __device__ __forceinline__ double dsdw(int M, double u, double w, double s, double E, double q, double F1,
+                                              double dE, double hdt) {
+    if (M == 1) return (-u * E + (w + q - s * u) * dE) / E;
+    const double r = 1.0 - hdt * s * E;
+    const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
+    const double G0 = w + q - s * u;
+    const double V1 = F1 * (u + hdt * G0 * E);
+    const double G1 = w + q - s * V1;
+    return (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
+}
 )";
 
 // Helpers of the generated adjoint kernels: D^T of a staggered difference
@@ -298,6 +312,21 @@ static __device__ __forceinline__ double pend(int M, double u, double w, double 
         dsdw = (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
     }
     ds += dsdw * Y;
+    if (gq) atomicAdd(gq + pt, Y);
+    return rho * Y;
+}
+// the same with the sigma-gradient factor D recorded by the forward (dsdw)
+static __device__ __forceinline__ double pend_ds(int M, double D, double Y, double s, double E, double F1, double& ds,
+                                                 double* gq, int pt, double hdt) {
+    const double r = 1.0 - hdt * s * E;
+    double rho;
+    if (M == 1) {
+        rho = r / (hdt * E);
+    } else {
+        const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
+        rho = F1 * r * r * den;
+    }
+    ds += D * Y;
     if (gq) atomicAdd(gq + pt, Y);
     return rho * Y;
 }
@@ -630,7 +659,9 @@ std::string group_name(int phase, int k) { return "smg_g" + std::to_string(phase
 std::string group_args(bool rec) {
     return std::string("(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, "
                        "int y, int z, bool act") +
-           (rec ? ", double* __restrict__ WR, double* __restrict__ PR)" : ")");
+           (rec ? ", double* __restrict__ WR, double* __restrict__ PR, const DevField* __restrict__ DE, int dsm, "
+                  "int dsw)"
+                : ")");
 }
 
 // device function of one group: the thread's stencil offsets, then the blocks
@@ -744,7 +775,10 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
                   "    %s\n"
                   "    switch (grp) {\n",
                   bounds(block, h->jit_regs).c_str(), name.c_str(),
-                  rec ? ", double* __restrict__ WR, double* __restrict__ PR" : "", map.c_str(), g.B[1], g.B[1],
+                  rec ? ", double* __restrict__ WR, double* __restrict__ PR, const DevField* __restrict__ DE, int dsm, "
+                        "int dsw"
+                      : "",
+                  map.c_str(), g.B[1], g.B[1],
                   block, g.B[0],
                   // with x differences from lane shuffles every lane of a warp takes part:
                   // lanes past the row compute on the last pair and store nothing
@@ -753,7 +787,7 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
     o += b;
     for (int k = k0; k < k1; ++k)
         o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z, act" +
-             (rec ? ", WR, PR" : "") + "); break;\n";
+             (rec ? ", WR, PR, DE, dsm, dsw" : "") + "); break;\n";
     o += "    default: break;\n    }\n}\n";
 }
 
@@ -1047,12 +1081,28 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         }
         o += "        double u0 = u.x, u1 = u.y;\n";
         if (rec) {
+            // the sigma-gradient factor of this phase for the adjoint sweep
+            // (phase kind dsm substeps, first filter k=2 when dsw), from the
+            // values before the phase and the coupling sum, in W's slot
             const long long so = (long long)p * g.cs;
+            std::string de0, de1;
+            if (is_array(h, f.s)) {
+                std::snprintf(b, sizeof b, "        const double2 DEv = ld2(fp(DE, %d) + pt);\n", f.s);
+                de0 = "DEv.x";
+                de1 = "DEv.y";
+            } else {
+                std::snprintf(b, sizeof b, "        const double DEv = fs(DE, %d);\n", f.s);
+                de0 = de1 = "DEv";
+            }
+            o += b;
             std::snprintf(b, sizeof b,
-                          "        if (%s) { double* wp = WR + pt + %lld; double* pp = PR + pt + %lld;\n"
-                          "          if (%s) { *reinterpret_cast<double2*>(wp) = make_double2(-SA, -SB); "
-                          "*reinterpret_cast<double2*>(pp) = u; } else { wp[0] = -SA; pp[0] = u.x; } }\n",
-                          stx.c_str(), so, so, v1.c_str());
+                          "        if (%s) { double* wp = WR + pt + %lld;\n"
+                          "          const double D0 = dsdw(dsm, u.x, -SA, %s, %s, %s, dsw ? %s : %s, %s, hdt);\n"
+                          "          if (%s) *reinterpret_cast<double2*>(wp) = make_double2(D0, "
+                          "dsdw(dsm, u.y, -SB, %s, %s, %s, dsw ? %s : %s, %s, hdt)); else wp[0] = D0; }\n",
+                          stx.c_str(), so, sv.first.c_str(), E.first.c_str(), q.first.c_str(), k2.first.c_str(),
+                          k1.first.c_str(), de0.c_str(), v1.c_str(), sv.second.c_str(), E.second.c_str(),
+                          q.second.c_str(), k2.second.c_str(), k1.second.c_str(), de1.c_str());
             o += b;
         }
         auto sub = [&]() {
@@ -2092,16 +2142,6 @@ void emit_adj_group(std::string& o, const smg_handle* h, int l, const std::vecto
         }
         return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
     };
-    std::set<int> ddone;
-    auto dEc = [&](int f) {   // d(decay)/d(sigma) of sigma field f
-        const std::string n = "DE" + std::to_string(f);
-        if (ddone.insert(f).second) {
-            if (is_array(h, f)) std::snprintf(b, sizeof b, "    const double2 %s = L2(fp(DE, %d) + pt);\n", n.c_str(), f);
-            else std::snprintf(b, sizeof b, "    const double %s = fs(DE, %d);\n", n.c_str(), f);
-            o += b;
-        }
-        return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
-    };
     std::set<std::pair<int, int>> tdone;
     auto tval = [&](int j, int a, int g2) {   // D^T Y_j along axis a at the point pair
         const std::string n = "T" + std::to_string(a) + "_" + std::to_string(j);
@@ -2125,13 +2165,12 @@ void emit_adj_group(std::string& o, const smg_handle* h, int l, const std::vecto
         for (size_t k = 0; k < Dother.size(); ++k)
             if (Dother[k] == i) pslot = (int)k;
         const Coefs f = coefs_of(h, 1 - l, i);
-        const auto sv = coef(f.s), E = coef(f.E), q = coef(f.q);
+        const auto sv = coef(f.s), E = coef(f.E);
         std::pair<std::string, std::string> k1{"1.0", "1.0"}, k2{"1.0", "1.0"};
         if (filt) {
             k1 = coef(f.F1);
             k2 = coef(f.F2);
         }
-        const auto dE = dEc(f.s);
         const auto terms = adj_terms(h, l, i);
         std::vector<std::pair<double, std::pair<std::string, std::string>>> tv;
         if (!terms.empty()) {
@@ -2157,14 +2196,12 @@ void emit_adj_group(std::string& o, const smg_handle* h, int l, const std::vecto
                           "        if (pm) {\n"
                           "          double* gq = %s;\n"
                           "          const long long rp = %lld + pt;\n"
-                          "          l0 = pend(pm, PRE[rp], WR[rp], l0, %s, %s, %s, %s, %s, gs%d_0, gq, pt, hdt);\n"
-                          "          if (v1) l1 = pend(pm, PRE[rp + 1], WR[rp + 1], l1, %s, %s, %s, %s, %s, gs%d_1, gq, "
-                          "pt + 1, hdt);\n"
+                          "          l0 = pend_ds(pm, WR[rp], l0, %s, %s, %s, gs%d_0, gq, pt, hdt);\n"
+                          "          if (v1) l1 = pend_ds(pm, WR[rp + 1], l1, %s, %s, %s, gs%d_1, gq, pt + 1, hdt);\n"
                           "        }\n",
                           f.q == h->field_zero ? "nullptr" : ("Gt[" + std::to_string(f.q) + "]").c_str(),
-                          (long long)pslot * g.cs, sv.first.c_str(), E.first.c_str(), q.first.c_str(), F0.c_str(),
-                          dE.first.c_str(), f.s, sv.second.c_str(), E.second.c_str(), q.second.c_str(), F1.c_str(),
-                          dE.second.c_str(), f.s);
+                          (long long)pslot * g.cs, sv.first.c_str(), E.first.c_str(), F0.c_str(), f.s,
+                          sv.second.c_str(), E.second.c_str(), F1.c_str(), f.s);
             o += b;
         }
         if (!terms.empty()) {
@@ -2636,7 +2673,7 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
 // streams after the work already queued on s and joined back into s (inside
 // a stream capture this becomes parallel branches of the graph).
 cudaError_t launch_state(const smg_handle* h, JitState* J, double* U, int mode, int kfilter, double* wrec,
-                         double* prec, cudaStream_t s) {
+                         double* prec, cudaStream_t s, const DevField* DE = nullptr, int dsm = 1, int dsw = 0) {
     const int phase = mode == 1 ? 1 : 0;
     const std::vector<JitKernel>& K = J->k[phase];
     if (K.empty()) return cudaSuccess;
@@ -2645,7 +2682,11 @@ cudaError_t launch_state(const smg_handle* h, JitState* J, double* U, int mode, 
     int kf = kfilter;
     int md = mode;
     int* err = J->dErr;
-    void* args[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec, &err};
+    // plain kernels: (U, F, hdt, kf, mode[, -, -, err]); recording kernels:
+    // (U, F, hdt, kf, mode, WR, PR, DE, dsm, dsw)
+    void* args_plain[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec, &err};
+    void* args_rec[] = {&U, &F, &hdt, &kf, &md, &wrec, &prec, &DE, &dsm, &dsw};
+    void** args = wrec ? args_rec : args_plain;
     auto go = [&](const JitKernel& k, cudaStream_t st) {
         const unsigned blk = (unsigned)(k.block > 0 ? k.block : J->block);
         return api().LaunchKernel(k.fn, (unsigned)k.grid, 1, 1, blk, 1, 1, (unsigned)k.smem, st, args, nullptr) == 0
@@ -2681,8 +2722,8 @@ cudaError_t launch_jit(const smg_handle* h, int mode, int kfilter, cudaStream_t 
 }
 
 cudaError_t launch_jit_rec(const smg_handle* h, int mode, int kfilter, double* U, double* wrec, double* prec,
-                           cudaStream_t s) {
-    return launch_state(h, h->jit_rec, U, mode, kfilter, wrec, prec, s);
+                           const DevField* DE, int dsm, int dsw, cudaStream_t s) {
+    return launch_state(h, h->jit_rec, U, mode, kfilter, wrec, prec, s, DE, dsm, dsw);
 }
 
 int jit_launches(const smg_handle* h, int phase) { return h->jit ? (int)h->jit->k[phase].size() : 0; }
