@@ -228,19 +228,19 @@ static __device__ __forceinline__ const double* fp(const DevField* F, int i) {
 static __device__ __forceinline__ double fs(const DevField* F, int i) { return __ldg(&F[i].s); }
 // request a line into L2 ahead of its load (no register, no wait)
 static __device__ __forceinline__ void pf(const void* p) { asm volatile("prefetch.global.L2 [%0];" :: "l"(p)); }
-// the sigma-gradient factor of a destination's phase (one substep: M = 1, two:
-// M = 2, F1 the first substep's filter) from its value before the phase u and
-// coupling sum w: the adjoint sweep adds factor * Y to dJ/dsigma; the same
-// expressions as the sweep's own evaluation from recorded u and w
+// the numerator of the sigma-gradient factor of a destination's phase (one
+// substep: M = 1, two: M = 2, F1 the first substep's filter) from its value
+// before the phase u and coupling sum w: the adjoint sweep divides it by E
+// (M = 1) or multiplies it by its own den (M = 2) and adds factor * Y to
+// dJ/dsigma -- the expressions of the sweep's evaluation from recorded u and w
 static __device__ __forceinline__ double dsdw(int M, double u, double w, double s, double E, double q, double F1,
                                               double dE, double hdt) {
-    if (M == 1) return (-u * E + (w + q - s * u) * dE) / E;
+    if (M == 1) return -u * E + (w + q - s * u) * dE;
     const double r = 1.0 - hdt * s * E;
-    const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
     const double G0 = w + q - s * u;
     const double V1 = F1 * (u + hdt * G0 * E);
     const double G1 = w + q - s * V1;
-    return (r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE)) * den;
+    return r * F1 * hdt * (-u * E + G0 * dE) + hdt * (-V1 * E + G1 * dE);
 }
 )";
 
@@ -315,16 +315,19 @@ static __device__ __forceinline__ double pend(int M, double u, double w, double 
     if (gq) atomicAdd(gq + pt, Y);
     return rho * Y;
 }
-// the same with the sigma-gradient factor D recorded by the forward (dsdw)
-static __device__ __forceinline__ double pend_ds(int M, double D, double Y, double s, double E, double F1, double& ds,
+// the same with the numerator N of the sigma-gradient factor recorded by the
+// forward (dsdw)
+static __device__ __forceinline__ double pend_ds(int M, double N, double Y, double s, double E, double F1, double& ds,
                                                  double* gq, int pt, double hdt) {
     const double r = 1.0 - hdt * s * E;
-    double rho;
+    double rho, D;
     if (M == 1) {
         rho = r / (hdt * E);
+        D = N / E;
     } else {
         const double den = 1.0 / (hdt * E * (r * F1 + 1.0));
         rho = F1 * r * r * den;
+        D = N * den;
     }
     ds += D * Y;
     if (gq) atomicAdd(gq + pt, Y);
