@@ -222,22 +222,48 @@ def bench_batch(steps: int = 200):
     setup_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     dev = 0.0
+    per_ms = []
     for sv in solvers:
         sv.run(steps)
         sv.sync()
-        dev += sv.last_run_stats()[0]
+        per_ms.append(sv.last_run_stats()[0])
+        dev += per_ms[-1]
     wall = time.perf_counter() - t0
     for sv in solvers:
         sv.close()
     batched = mc * steps / (ms / 1e3)
     loop = mc * steps / wall
+    # the loop's device rate by instance size, and the batch's own HBM fraction
+    from starmap_b200.roofline import algorithmic_bytes_per_step
+    buckets = {}
+    for (S, fs), t in zip(setups, per_ms):
+        key = "edge<=128" if int(S.n[1]) <= 128 else "edge>128"
+        b = buckets.setdefault(key, {"instances": 0, "moment_cells": 0, "loop_device_ms": 0.0})
+        b["instances"] += 1
+        b["moment_cells"] += S.n_sys * int(np.prod(S.n))
+        b["loop_device_ms"] += t
+    for b in buckets.values():
+        b["loop_device_value"] = b["moment_cells"] * steps / (b["loop_device_ms"] / 1e3)
+        b["share_of_moment_cells"] = b["moment_cells"] / mc
+    if len(buckets) == 2:
+        sm, lg = buckets["edge<=128"], buckets["edge>128"]
+        # if the batch ran the small instances for nothing and the large ones at the loop's rate
+        bound = (sm["loop_device_ms"] + lg["loop_device_ms"]) / lg["loop_device_ms"]
+    else:
+        bound = None
+    alg = sum(algorithmic_bytes_per_step(S, _tables(S, fs), fused=True)["step"] for S, fs in setups)
+    peak, kind = measured_peak()
+    batch_gbs = alg * steps / (ms / 1e3) / 1e9
     return {"value": batched, "unit": UNIT, "instances": len(pars), "moment_cells": mc, "steps": steps,
             "ms": ms, "launches": launches, "config": cfg, "kernels": "generated families" if used_jit else
             "precompiled", "families": families, "autotune_s": tune_s,
             "plain_loop_value": loop, "plain_loop_device_value": mc * steps / (dev / 1e3),
             "plain_loop_setup_s": setup_s,
             "batched_over_plain_loop": batched / loop,
-            "batched_over_plain_loop_device": batched / (mc * steps / (dev / 1e3))}
+            "batched_over_plain_loop_device": batched / (mc * steps / (dev / 1e3)),
+            "loop_by_size": buckets, "loop_speedup_bound_small_free": bound,
+            "roofline": {"bound": "hbm", "achieved": batch_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": batch_gbs / peak, "peak_kind": kind, "algorithmic_bytes_per_step": alg}}
 
 
 def bench_adjoint(nsteps: int = 400, n: int = 200, ckpts=(0, 20)):
