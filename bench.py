@@ -433,6 +433,32 @@ def bench_cold(upd_step: float, nsteps: int = 321):
             "empty_cache": mk(res[0]), "warm_cache": mk(res[1])}
 
 
+def bench_growth(n_mom: int = 39):
+    """One growth-factor evaluation of the parabolic time-step search for the
+    P39 lattice system (820 moments): on the host (numpy eigenvalues, all
+    host threads) and on the GPU (smg_growth_radius), same matrix."""
+    from starmap_b200 import configs, starmap_init, timestep
+    from starmap_b200.solver import first_step, prepare
+    prob = configs.lattice(n=20, n_mom=n_mom)
+    prob["timestep"] = 1
+    S = prepare(starmap_init(prob))
+    fs = first_step(S)
+    decay = timestep.decay_vector(S.n_sys, S.gt, S.mom_order, fs["sA"][1, 1, 1], fs["sT"])
+    dt = 2 * S.dt_hyp
+    out = {"n_sys": S.n_sys}
+    for flag, key in ((True, "device"), (False, "host")):
+        timestep.use_device_eigenvalues(flag)
+        timestep.growth_factor(S.M_sym, S.even, S.odd, decay, dt, 1)      # warm-up (handles, buffers)
+        t0 = time.perf_counter()
+        la = timestep.growth_factor(S.M_sym, S.even, S.odd, decay, dt, 1)
+        out[key + "_ms"] = (time.perf_counter() - t0) * 1e3
+        out[key + "_radius"] = la
+    timestep.use_device_eigenvalues(None)
+    out["host_threads"] = host_threads()
+    out["rel_diff"] = abs(out["device_radius"] - out["host_radius"]) / out["host_radius"]
+    return out
+
+
 def host_buffers(S):
     """Initial state and output buffers per component in pinned host memory
     (page-locked through torch; pageable numpy arrays if that is unavailable)."""
@@ -606,6 +632,11 @@ def main():
         line["adjoint"] = bench_adjoint()
     if world == 1 and not args.no_3d:
         line["pointsource_3d"] = bench_3d()
+    if world == 1:
+        try:
+            line["parabolic_step_p39"] = bench_growth()
+        except Exception as e:
+            line["parabolic_step_p39"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         steps, secs = cpu_sample(par, budget_s=args.cpu_budget, nthreads=threads, warm=0)

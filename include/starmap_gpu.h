@@ -311,6 +311,18 @@ int smg_state_sumsq(smg_handle* h, double* sumsq);
 int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t len, double* d_out,
                       void* stream);
 
+/* Spectral radius *la = max |eig(G_o G_e G_e G_o)| of the full-step growth
+ * matrix that the parabolic time step searches over (starmap_solver.m:
+ * 506-514, growth_factor): G is the n x n complex matrix
+ * diag(dt*expm1div(-decay*dt/2)) * (M + diag(-decay/2)), column-major with
+ * interleaved real and imaginary parts; odd[i] = 1 for the components that
+ * phase A updates (their rows of G_e are identity rows, the other rows of
+ * G_o are), 0 for phase B's.  The products run on the current device with
+ * cuBLAS and the eigenvalues with cuSOLVER (cusolverDnXgeev), both opened
+ * at the first call; synchronous.  Replaces the host eig of growth_factor;
+ * errors through smg_last_error(NULL). */
+int smg_growth_radius(int32_t n, const double* G, const int32_t* odd, double* la);
+
 /* Grid-type classification of starmap_solver.m:76-98 from the sparsity of
  * par.Mx/My/Mz (column-major n_sys x n_sys): writes gt_out[3*j+d] in {1,2}.
  * SMG_EINVAL when a component is not reached from component 1 (the

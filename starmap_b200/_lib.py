@@ -122,6 +122,7 @@ SIGNATURES = {
     "smg_adjoint_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "smg_active_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_char_p, C.c_int64]),
     "smg_jit_stats": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "smg_growth_radius": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "smg_jit_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32,
                                  C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "smg_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.POINTER(smg_problem)), C.POINTER(C.c_void_p)]),

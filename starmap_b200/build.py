@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstarmap_gpu.so")
-SOURCES = ["smg_api.cu", "smg_phase.cu", "smg_batch.cu", "smg_norms.cu", "smg_adjoint.cu", "smg_jit.cu"]
+SOURCES = ["smg_api.cu", "smg_phase.cu", "smg_batch.cu", "smg_norms.cu", "smg_adjoint.cu", "smg_jit.cu", "smg_growth.cu"]
 HEADERS = ["smg_device.cuh", "smg_internal.h", "smg_pair.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -13,16 +13,53 @@ the averaged materials fall back to those at time t when they are unstable
 with the chosen dt (:253-265).  Autonomous problems search once, at the
 first step.
 
-This is host work on n_sys x n_sys matrices (dense complex eigenvalues, as
-the reference's ``eig``); the device only receives the resulting dt.
+The search itself runs on the host; each trial's growth matrix is formed
+on the host (n_sys^2 work) and its spectral radius -- three n_sys^3 complex
+products and the dense complex eigenvalues of the reference's ``eig`` -- is
+computed on the GPU (``smg_growth_radius``: cuBLAS and cuSOLVER) when a
+CUDA device is present, else with numpy.  The device only receives the
+resulting dt.
 """
 from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["symbol", "decay_vector", "growth_factor", "search", "stable"]
+__all__ = ["symbol", "decay_vector", "growth_factor", "search", "stable", "use_device_eigenvalues"]
 
 LA0 = 1 + 1e-8
+_DEVICE = None   # None: decided at the first growth factor (a CUDA device is present)
+
+
+def use_device_eigenvalues(flag=None):
+    """Compute growth-matrix spectral radii on the GPU (True), with numpy
+    (False), or on the GPU when a CUDA device is present (None, default)."""
+    global _DEVICE
+    _DEVICE = flag
+
+
+def _device_enabled() -> bool:
+    global _DEVICE
+    if _DEVICE is None:
+        try:
+            from . import _lib
+            _DEVICE = _lib.lib().smg_device_count() > 0
+        except Exception:
+            _DEVICE = False
+    return bool(_DEVICE)
+
+
+def _device_radius(G, odd) -> float:
+    import ctypes as C
+
+    from . import _lib
+    n = G.shape[0]
+    Gc = np.asfortranarray(G, dtype=np.complex128)
+    mask = np.zeros(n, dtype=np.int32)
+    mask[list(odd)] = 1
+    la = C.c_double()
+    _lib.check(_lib.lib().smg_growth_radius(n, Gc.ctypes.data_as(C.POINTER(C.c_double)),
+                                            mask.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(la)))
+    return float(la.value)
 
 
 def symbol(Mx, My, Mz, h):
@@ -73,6 +110,11 @@ def growth_factor(M, even, odd, decay, dt, timestep) -> float:
     phi[big] = (np.exp(x[big]) - 1) / x[big]
     G = (dt * phi)[:, None] * (M + np.diag(-decay / 2))
     n = len(decay)
+    if _device_enabled():
+        la = _device_radius(G, odd)
+        if timestep == 2:
+            la *= float(np.exp(decay[0] * dt))
+        return la
     diag = (np.arange(n), np.arange(n))
     Ge = G.copy()
     Ge[odd, :] = 0
