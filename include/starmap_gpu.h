@@ -261,7 +261,9 @@ int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
                                     1: one kernel per phase calling the separately compiled groups */
 #define SMG_TUNE_JIT_XPAIR  11   /* x differences: 0 = four 64-bit loads per point pair, 1 = two aligned 128-bit loads,
                                     2 = one 128-bit load and the neighbouring lane's value (warp shuffle) */
-#define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them */
+#define SMG_TUNE_JIT_PREFETCH 12 /* 1: the generated kernels request a group's rows into L2 before loading them;
+                                    2, 3: each CTA's first thread requests into L2, with bulk prefetches, the row
+                                    segments that the group 1 or 2 places later in the same kernel reads there */
 #define SMG_TUNE_JIT_BAND   13   /* CTA order of the generated kernels: 0 group-major, R > 0 bands of R rows,
                                     -1 (default) group-major below 4 MB per component, else bands of about 48 MB;
                                     staged kernels: 0 group-major, else band-major (bands of SMG_TUNE_JIT_ROWS) */

@@ -1345,7 +1345,7 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             h->jit_failed = false;
             break;
         case SMG_TUNE_JIT_PREFETCH:
-            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: jit prefetch must be 0 or 1");
+            if (value < 0 || value > 3) return fail(h, SMG_EINVAL, "smg_tune: jit prefetch must be 0..3");
             h->jit_prefetch = value;
             smg::jit_free(h);
             h->jit_failed = false;

@@ -228,6 +228,11 @@ static __device__ __forceinline__ const double* fp(const DevField* F, int i) {
 static __device__ __forceinline__ double fs(const DevField* F, int i) { return __ldg(&F[i].s); }
 // request a line into L2 ahead of its load (no register, no wait)
 static __device__ __forceinline__ void pf(const void* p) { asm volatile("prefetch.global.L2 [%0];" :: "l"(p)); }
+// request a contiguous range into L2 with the bulk copy engine (16-byte
+// aligned, a multiple of 16 bytes; no register, no shared memory, no wait)
+static __device__ __forceinline__ void l2pf(const double* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
 // the numerator of the sigma-gradient factor of a destination's phase (one
 // substep: M = 1, two: M = 2, F1 the first substep's filter) from its value
 // before the phase u and coupling sum w: the adjoint sweep divides it by E
@@ -868,7 +873,7 @@ std::vector<std::vector<int>> shared_groups(const smg_handle* h, int phase, int 
 // one group's device function (inline layout): positions P into the phase's
 // destination list (the position is the destination's recording slot)
 void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, const std::vector<int>& P, bool rec,
-                       bool fam = false) {
+                       bool fam = false, const std::vector<int>* nextP = nullptr) {
     const smg::DevGrid& g = h->g;
     const std::vector<int> D = phase_dests(h, phase);
     char b[4096];
@@ -971,7 +976,65 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         }
         return std::make_pair(is_array(h, f) ? n + ".x" : n, is_array(h, f) ? n + ".y" : n);
     };
-    if (h->jit_prefetch && !fam) {
+    if (nextP && !fam) {
+        // SMG_TUNE_JIT_PREFETCH 2, 3: thread 0 of the CTA (x0 = the chunk's
+        // first point) requests into L2 the row segments that a later group
+        // of this kernel reads at this row chunk -- its destinations, array
+        // coefficients, x sources and both rows of every y/z source -- one
+        // bulk prefetch per segment, so that the later group's loads find
+        // them in L2
+        const std::vector<int>& NP = *nextP;
+        std::snprintf(b, sizeof b,
+                      "    if (threadIdx.x == 0) {\n"
+                      "        const unsigned nb = (unsigned)((x0 + %d < %lld ? %d : %lld - x0) * 8);\n",
+                      2 * h->jit_block, (long long)g.s1, 2 * h->jit_block, (long long)g.s1);
+        o += b;
+        bool nused[3][2] = {{false, false}, {false, false}, {false, false}};
+        for (int p : NP)
+            for (int q = h->comps[D[p]].cbeg; q < h->comps[D[p]].cend; ++q)
+                nused[h->coups[q].code >> 1][h->coups[q].code & 1] = true;
+        for (int a = 1; a < 3; ++a)
+            for (int g2 = 0; g2 < 2; ++g2) {
+                if (!nused[a][g2]) continue;
+                const long long stv = a == 1 ? g.s1 : g.s2;
+                const char* pv = a == 1 ? "y" : "z";
+                std::snprintf(b, sizeof b,
+                              "        int nh%s_%d, nl%s_%d;\n"
+                              "        { int hi, lo; stencil(%s, %d, %d, %d, hi, lo); nh%s_%d = (int)((hi - %s) * %lld); "
+                              "nl%s_%d = (int)((lo - %s) * %lld); }\n",
+                              an[a], g2, an[a], g2, pv, g.n[a], g.bc[a], g2, an[a], g2, pv, stv, an[a], g2, pv, stv);
+                o += b;
+            }
+        std::set<int> fdone;
+        std::set<std::pair<int, int>> sdone;
+        const bool nfilt = h->filter_mode == SMG_FILTER_SUBSTEP;
+        for (int p : NP) {
+            const int j = D[p];
+            const smg::DevComp& c = h->comps[j];
+            std::snprintf(b, sizeof b, "        l2pf(Up + %lld, nb);\n", (long long)j * g.cs);
+            o += b;
+            const Coefs f = coefs_of(h, phase, j);
+            std::vector<int> fl = {f.q, f.s, f.E};
+            if (nfilt) fl.insert(fl.end(), {f.F1, f.F2});
+            for (int fi : fl)
+                if (is_array(h, fi) && fdone.insert(fi).second) {
+                    std::snprintf(b, sizeof b, "        l2pf(fp(F, %d) + pt, nb);\n", fi);
+                    o += b;
+                }
+            for (int qq = c.cbeg; qq < c.cend; ++qq) {
+                const smg::DevCoup& cp = h->coups[qq];
+                const int a = cp.code >> 1, g2 = cp.code & 1;
+                if (!sdone.insert({a, cp.src}).second) continue;
+                const long long so = (long long)cp.src * g.cs;
+                if (a == 0) std::snprintf(b, sizeof b, "        l2pf(Up + %lld, nb);\n", so);
+                else std::snprintf(b, sizeof b, "        l2pf(Up + %lld + nh%s_%d, nb); l2pf(Up + %lld + nl%s_%d, nb);\n",
+                                   so, an[a], g2, so, an[a], g2);
+                o += b;
+            }
+        }
+        o += "    }\n";
+    }
+    if (h->jit_prefetch == 1 && !fam) {
         // every row the group reads, requested into L2 up front: the loads
         // below then wait for L2 rather than DRAM
         std::set<std::pair<int, int>> seen;
@@ -1983,7 +2046,11 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
                 body = "__shared__ double2 smg_ring[" + std::to_string(ring * block) + "];\n";
                 for (int j = k0; j < k1; ++j) emit_prefetch_group(body, h, phase, j, G[j], ring, block);
             } else {
-                for (int j = k0; j < k1; ++j) emit_shared_group(body, h, phase, j, G[j], rec);
+                for (int j = k0; j < k1; ++j) {
+                    const int ahead = h->jit_prefetch >= 2 && !rec ? h->jit_prefetch - 1 : 0;
+                    const std::vector<int>* nx = (ahead && j + ahead < k1) ? &G[j + ahead] : nullptr;
+                    emit_shared_group(body, h, phase, j, G[j], rec, false, nx);
+                }
             }
             g_ctab = nullptr;
             k.src += ctab_decl(tab) + body;

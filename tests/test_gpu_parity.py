@@ -408,3 +408,26 @@ def test_staged_kernels_vs_oracle(name, shape):
         mism += int(np.count_nonzero(U[j] != ref.U[j]))
     assert worst <= REL_L2_TOL, f"{name} {shape}: worst relative L2 {worst:.3e}"
     assert mism == 0, f"{name} {shape}: {mism} values differ"
+
+
+@pytest.mark.parametrize("prefetch", [2, 3])
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "odd_mixed_bc", "pt3d_p3"])
+def test_bulk_l2_prefetch_vs_oracle(name, prefetch):
+    """SMG_TUNE_JIT_PREFETCH 2/3 (bulk L2 prefetches of a later group's rows)
+    moves no data the kernels compute with: results stay bit-identical."""
+    from starmap_b200 import _lib
+    from starmap_b200.solver import setup_gpu
+    par = starmap_init(cases.ALL[name]())
+    ref = O.starmap_solver(par, max_steps=6)
+    S, fs, solver, T = setup_gpu(par)
+    try:
+        solver.tune(_lib.SMG_TUNE_JIT_PREFETCH, prefetch)
+        solver.set_variant(_lib.SMG_VARIANT_JIT)
+        solver.set_state(S.U0)
+        solver.set_dt(fs["dt"])
+        solver.run(6)
+        U = solver.get_state()
+    finally:
+        solver.close()
+    for j in range(S.n_sys):
+        assert np.count_nonzero(U[j] != ref.U[j]) == 0, (name, j)
