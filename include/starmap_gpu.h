@@ -253,7 +253,8 @@ int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
 #define SMG_TUNE_ADJ_PRIORITY 20 /* smg_backward stream priorities, set before smg_forward: 0 (default) recompute and
                                     sweep at the default priority, 1 recompute at the device's highest priority, 2
                                     the sweep on a stream of the highest priority above the recompute */
-#define SMG_TUNE_JIT_BLOCK   6   /* threads per CTA of the generated kernels (32..256, multiple of 32) */
+#define SMG_TUNE_JIT_BLOCK   6   /* threads per CTA of the generated kernels (32..256, multiple of 32; default: of
+                                    64 and 96 the one leaving the fewest idle points in a row, 96 on ties) */
 #define SMG_TUNE_JIT_GROUP   7   /* destinations per CTA of the generated kernels (1..256) */
 #define SMG_TUNE_JIT_REGS    8   /* register limit per thread of the generated kernels (0: compiler's choice, else 32..255) */
 #define SMG_TUNE_JIT_SPLIT   9   /* groups per separately compiled program (1..64; 0: one per phase) */
