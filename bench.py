@@ -148,7 +148,7 @@ def measured_peak():
 def ncu_traffic(family="jit", name=None):
     """DRAM bytes per step of the phase kernels of `family` from the committed ncu summary (or None)."""
     if name is None:
-        name = "phase_kernels_jit_lattice_p39.txt" if family == "jit" else "phase_kernels_lattice_p39_350.txt"
+        name = "phase_kernels_jit_lattice_p39_350_full.txt" if family == "jit" else "phase_kernels_lattice_p39_350.txt"
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
@@ -530,6 +530,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline stepping")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of reference-arm stepping")
     ap.add_argument("--no-cold", action="store_true", help="skip the cold-start measurement")
+    ap.add_argument("--no-growth", action="store_true", help="skip the parabolic-step eigenvalue measurement")
     ap.add_argument("--cold-call", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.cold_call:
@@ -632,7 +633,7 @@ def main():
         line["adjoint"] = bench_adjoint()
     if world == 1 and not args.no_3d:
         line["pointsource_3d"] = bench_3d()
-    if world == 1:
+    if world == 1 and not args.no_growth:
         try:
             line["parabolic_step_p39"] = bench_growth()
         except Exception as e:
