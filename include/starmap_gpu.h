@@ -250,6 +250,8 @@ int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
 #define SMG_TUNE_PAIR_UNROLL 3   /* couplings per inner iteration (1 or 2) */
 #define SMG_TUNE_PAIR_MINB   4   /* register budget: 3 or 4 resident CTAs of 256 threads (64/85 regs) */
 #define SMG_TUNE_ADJ_FUSED   5   /* smg_backward: 1 = one fused kernel per phase (default), 0 = pointwise + transpose kernels */
+#define SMG_TUNE_DIRECT_XFER 21  /* state transfers: 1 (default) page-locked host arrays are read / written in place by
+                                    one kernel per 64 components, 0 always through the device staging buffer */
 #define SMG_TUNE_ADJ_PRIORITY 20 /* smg_backward stream priorities, set before smg_forward: 0 (default) recompute and
                                     sweep at the default priority, 1 recompute at the device's highest priority, 2
                                     the sweep on a stream of the highest priority above the recompute */

@@ -156,13 +156,99 @@ cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, bool to_slots, 
     return cudaGetLastError();
 }
 
+// Direct transfer: up to kXferMax whole components whose host arrays are
+// page-locked, so that the kernel reads (upload) or writes (download) them
+// in place through their device addresses (unified addressing); entry k is
+// component slot slot_off[k] with host array hp[k] of e0 x rows points.
+struct XferDirect {
+    int n;
+    int e0[kXferMax], e1[kXferMax], rows[kXferMax];
+    double* hp[kXferMax];
+    long long slot_off[kXferMax];
+};
+
+__global__ void k_xfer_direct(XferDirect c, double* __restrict__ U, const double* __restrict__ snap, double wa,
+                              double wb, long long s1, long long s2, int to_slots) {
+    const int k = blockIdx.z;
+    if (k >= c.n) return;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e0 = c.e0[k], e1 = c.e1[k];
+    if (x >= e0) return;
+    double* hp = c.hp[k];
+    double* sl = U + c.slot_off[k];
+    for (int r = blockIdx.y; r < c.rows[k]; r += gridDim.y) {
+        const long long d = (long long)(r / e1) * s2 + (long long)(r % e1) * s1 + x;
+        const long long q = (long long)r * e0 + x;
+        if (to_slots) sl[d] = hp[q];
+        else if (snap) hp[q] = __dadd_rn(__dmul_rn(wa, snap[c.slot_off[k] + d]), __dmul_rn(wb, sl[d]));
+        else hp[q] = sl[d];
+    }
+}
+
+// the device address of a page-locked host array, or nullptr (pageable memory)
+double* device_view(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();   // clear the error of an unregistered pointer
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<double*>(a.devicePointer) : nullptr;
+}
+
+// Transfer of the components with non-NULL host pointers.  When every one of
+// them is page-locked, one kernel per kXferMax components moves them between
+// the host arrays and the padded slots directly (no staging copies);
+// otherwise the staged form below.
+int direct_transfer(smg_handle* h, bool upload, const std::vector<double*>& hp, const double* snap, double wa,
+                    double wb) {
+    XferDirect c;
+    c.n = 0;
+    int e0max = 1, rows_max = 1;
+    auto flush = [&]() -> cudaError_t {
+        if (!c.n) return cudaSuccess;
+        dim3 grid((unsigned)((e0max + 127) / 128), (unsigned)std::min(rows_max, 2048), (unsigned)c.n);
+        k_xfer_direct<<<grid, 128, 0, h->stream>>>(c, h->dU, snap, wa, wb, h->g.s1, h->g.s2, upload ? 1 : 0);
+        c.n = 0;
+        e0max = rows_max = 1;
+        return cudaGetLastError();
+    };
+    for (int j = 0; j < h->n_sys; ++j) {
+        if (!hp[j]) continue;
+        const int* e = h->comps[j].ext;
+        if (c.n == kXferMax) SMG_CUDA(h, flush());
+        c.e0[c.n] = e[0];
+        c.e1[c.n] = e[1];
+        c.rows[c.n] = e[1] * e[2];
+        c.hp[c.n] = hp[j];
+        c.slot_off[c.n] = (long long)j * h->g.cs;
+        e0max = std::max(e0max, e[0]);
+        rows_max = std::max(rows_max, e[1] * e[2]);
+        ++c.n;
+    }
+    SMG_CUDA(h, flush());
+    SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SMG_OK;
+}
+
 // The staged transfer of the components with non-NULL host pointers: each
 // component in pieces of whole rows that fit the staging buffer (a piece is
 // one contiguous range of the column-major host array), up to kXferMax
 // pieces per kernel launch.  Upload: copy the pieces in, then scatter.
 // Download: gather (or interpolate with snap), then copy the pieces out.
+// Page-locked host arrays go through direct_transfer instead.
 int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double* const* Uout,
                     const double* snap, double wa, double wb) {
+    if (h->direct_xfer) {
+        std::vector<double*> hp(h->n_sys, nullptr);
+        bool direct = true;
+        for (int j = 0; j < h->n_sys && direct; ++j) {
+            const void* p = upload ? (const void*)Uin[j] : (const void*)Uout[j];
+            if (!p) continue;
+            hp[j] = device_view(p);
+            direct = hp[j] != nullptr;
+        }
+        if (direct) return direct_transfer(h, upload, hp, snap, wa, wb);
+    }
     XferChunk c;
     c.n = 0;
     size_t used = 0;
@@ -1404,6 +1490,10 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             if (value < -1 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: graph steps must be -1..4096");
             h->graph_block = value;
             break;
+        case SMG_TUNE_DIRECT_XFER:
+            if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: direct xfer must be 0 or 1");
+            h->direct_xfer = value;
+            return SMG_OK;
         case SMG_TUNE_ADJ_PRIORITY:
             if (value < 0 || value > 2) return fail(h, SMG_EINVAL, "smg_tune: adj priority must be 0, 1 or 2");
             h->adj_priority = value;

@@ -103,6 +103,8 @@ struct Api {
     CUresult_t (*LaunchKernel)(CUfunction_t, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                cudaStream_t, void**, void**) = nullptr;
     CUresult_t (*FuncSetAttribute)(CUfunction_t, int, int) = nullptr;
+    CUresult_t (*CtxGetCurrent)(void**) = nullptr;          // optional: module sharing between handles
+    CUresult_t (*CtxGetId)(void*, unsigned long long*) = nullptr;
 };
 constexpr int kFuncAttrMaxDynamicSmem = 8;   // CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES
 
@@ -173,6 +175,8 @@ void load_api() {
                sym(cu, "cuModuleGetFunction", a.ModuleGetFunction) && sym(cu, "cuLaunchKernel", a.LaunchKernel) &&
                sym(cu, "cuFuncSetAttribute", a.FuncSetAttribute)) {
         a.cu_ok = true;
+        if (!sym(cu, "cuCtxGetCurrent", a.CtxGetCurrent) || !sym(cu, "cuCtxGetId", a.CtxGetId))
+            a.CtxGetCurrent = nullptr, a.CtxGetId = nullptr;
     } else {
         a.cu_why = "CUDA driver entry points missing";
     }
@@ -181,6 +185,61 @@ void load_api() {
 Api& api() {
     std::call_once(g_api_once, load_api);
     return g_api;
+}
+
+// Loaded modules shared between the handles of a process: handles of the
+// same problem (a second starmap_solver call, the instances of an ensemble)
+// run identical generated code, and loading it again costs milliseconds per
+// program.  Keyed by the context and the cubin's size and two hashes;
+// reference-counted, unloaded with the last user.
+struct ModEntry {
+    CUmodule_t mod;
+    int refs;
+};
+std::map<std::tuple<unsigned long long, size_t, unsigned long long, unsigned long long>, ModEntry> g_mods;
+std::mutex g_mods_mu;
+
+unsigned long long bytes_hash(const std::vector<char>& v, unsigned long long h) {
+    for (char c : v) {
+        h ^= (unsigned char)c;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+int load_module(const std::vector<char>& cubin, CUmodule_t* m) {
+    Api& a = api();
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!a.CtxGetCurrent || a.CtxGetCurrent(&ctx) != 0 || !ctx || a.CtxGetId(ctx, &id) != 0)
+        return a.ModuleLoadData(m, cubin.data()) == 0 ? 0 : -1;   // no context id: not shared
+    const auto key = std::make_tuple(id, cubin.size(), bytes_hash(cubin, 1469598103934665603ull),
+                                     bytes_hash(cubin, 0x9e3779b97f4a7c15ull));
+    std::lock_guard<std::mutex> lk(g_mods_mu);
+    auto it = g_mods.find(key);
+    if (it != g_mods.end()) {
+        ++it->second.refs;
+        *m = it->second.mod;
+        return 0;
+    }
+    if (a.ModuleLoadData(m, cubin.data()) != 0) return -1;
+    g_mods[key] = ModEntry{*m, 1};
+    return 0;
+}
+
+void release_module(CUmodule_t m) {
+    {
+        std::lock_guard<std::mutex> lk(g_mods_mu);
+        for (auto it = g_mods.begin(); it != g_mods.end(); ++it)
+            if (it->second.mod == m) {
+                if (--it->second.refs == 0) {
+                    api().ModuleUnload(m);
+                    g_mods.erase(it);
+                }
+                return;
+            }
+    }
+    api().ModuleUnload(m);   // loaded without sharing
 }
 
 // ---- source generation -------------------------------------------------------
@@ -2651,7 +2710,7 @@ void free_state(JitState*& J) {
     for (cudaEvent_t e : J->join) cudaEventDestroy(e);
     if (J->dErr) cudaFree(J->dErr);
     if (api().cu_ok)
-        for (CUmodule_t m : J->mods) api().ModuleUnload(m);
+        for (CUmodule_t m : J->mods) release_module(m);
     delete J;
     J = nullptr;
 }
@@ -2690,7 +2749,7 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
     };
     for (const auto& c : cubins) {
         CUmodule_t m = nullptr;
-        if (a.ModuleLoadData(&m, c.data()) != 0) return fail("cuModuleLoadData failed");
+        if (load_module(c, &m) != 0) return fail("cuModuleLoadData failed");
         J->mods.push_back(m);
     }
     if (calls) {
@@ -3092,7 +3151,7 @@ int jit_build_adj(smg_handle* h, std::string& err) {
         CUmodule_t m = nullptr;
         JitKernel k;
         k.grid = P[i].grid;
-        if (a.ModuleLoadData(&m, cubins[i].data()) != 0 ||
+        if (load_module(cubins[i], &m) != 0 ||
             (J->mods.push_back(m), a.ModuleGetFunction(&k.fn, m, P[i].name.c_str()) != 0)) {
             err = "loading the generated adjoint kernels failed";
             free_state(J);

@@ -1,0 +1,53 @@
+"""State transfers: page-locked host arrays are moved by one kernel that
+reads or writes them in place (unified addressing), pageable ones through the
+device staging buffer; both forms give the same state bit for bit, for
+uploads, downloads and the output-time interpolation."""
+import numpy as np
+import pytest
+
+import cases
+from starmap_b200 import _lib, starmap_init
+from starmap_b200.solver import setup_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def pinned_like(arrs):
+    torch = pytest.importorskip("torch")
+    out = []
+    for a in arrs:
+        b = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy()
+        b[:] = np.asarray(a, dtype=np.float64).ravel(order="F")
+        out.append(b.reshape(a.shape, order="F"))
+    return out
+
+
+@pytest.mark.parametrize("name", ["lattice_p5_substep", "odd_mixed_bc", "box3d_bc1_p2_full"])
+def test_direct_and_staged_transfers_agree(name):
+    par = starmap_init(cases.ALL[name]())
+    res = {}
+    for direct in (1, 0):
+        S, fs, solver, T = setup_gpu(par)
+        try:
+            solver.tune(_lib.SMG_TUNE_DIRECT_XFER, direct)
+            rng = np.random.default_rng(3)
+            U0 = [rng.standard_normal(solver.extents(j)) for j in range(S.n_sys)]
+            solver.set_state(pinned_like(U0) if direct else U0)
+            back = solver.get_state(out={j: pinned_like([np.zeros(solver.extents(j))])[0] for j in range(S.n_sys)}
+                                    if direct else None)
+            for j in range(S.n_sys):
+                np.testing.assert_array_equal(back[j], U0[j])
+            solver.set_dt(fs["dt"])
+            solver.run(2)
+            solver.snapshot()
+            solver.run(1)
+            outs = {j: pinned_like([np.zeros(solver.extents(j))])[0] for j in range(S.n_sys)} if direct else None
+            U = solver.get_state(out=outs)
+            outs2 = {j: pinned_like([np.zeros(solver.extents(j))])[0] for j in range(S.n_sys)} if direct else None
+            V = solver.get_interp(0.3, out=outs2)
+            res[direct] = ({j: np.array(U[j]) for j in U}, {j: np.array(V[j]) for j in V})
+        finally:
+            solver.close()
+    for j in res[0][0]:
+        np.testing.assert_array_equal(res[1][0][j], res[0][0][j])
+        np.testing.assert_array_equal(res[1][1][j], res[0][1][j])
