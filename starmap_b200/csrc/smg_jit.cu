@@ -49,6 +49,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <set>
@@ -199,11 +201,17 @@ struct ModEntry {
 std::map<std::tuple<unsigned long long, size_t, unsigned long long, unsigned long long>, ModEntry> g_mods;
 std::mutex g_mods_mu;
 
-unsigned long long bytes_hash(const std::vector<char>& v, unsigned long long h) {
-    for (char c : v) {
-        h ^= (unsigned char)c;
-        h *= 1099511628211ull;
+// Word-at-a-time multiply-xorshift hash of a cubin (megabytes for hundreds of
+// moments: a byte-serial hash would cost milliseconds per new handle).
+unsigned long long bytes_hash(const std::vector<char>& v, unsigned long long h, unsigned long long mul) {
+    const size_t nw = v.size() / 8;
+    for (size_t i = 0; i < nw; ++i) {
+        unsigned long long w;
+        std::memcpy(&w, v.data() + 8 * i, 8);
+        h = (h ^ w) * mul;
+        h ^= h >> 29;
     }
+    for (size_t i = 8 * nw; i < v.size(); ++i) h = (h ^ (unsigned char)v[i]) * mul;
     return h;
 }
 
@@ -213,8 +221,8 @@ int load_module(const std::vector<char>& cubin, CUmodule_t* m) {
     unsigned long long id = 0;
     if (!a.CtxGetCurrent || a.CtxGetCurrent(&ctx) != 0 || !ctx || a.CtxGetId(ctx, &id) != 0)
         return a.ModuleLoadData(m, cubin.data()) == 0 ? 0 : -1;   // no context id: not shared
-    const auto key = std::make_tuple(id, cubin.size(), bytes_hash(cubin, 1469598103934665603ull),
-                                     bytes_hash(cubin, 0x9e3779b97f4a7c15ull));
+    const auto key = std::make_tuple(id, cubin.size(), bytes_hash(cubin, 1469598103934665603ull, 0x9e3779b97f4a7c15ull),
+                                     bytes_hash(cubin, 0x243f6a8885a308d3ull, 0xff51afd7ed558ccdull));
     std::lock_guard<std::mutex> lk(g_mods_mu);
     auto it = g_mods.find(key);
     if (it != g_mods.end()) {
@@ -2021,6 +2029,31 @@ struct KernelSrc {
 //   inline (calls false): `per` groups per program (0: all of the phase),
 //          each program one kernel over its groups with their code inlined;
 //          the kernels of a phase run concurrently.
+// Runs the generators on up to 16 threads; the programs keep their order.
+// An exception in a generator (out of memory) is passed on to the caller.
+std::vector<KernelSrc> run_jobs(const std::vector<std::function<KernelSrc()>>& jobs) {
+    std::vector<KernelSrc> out(jobs.size());
+    std::vector<std::exception_ptr> ex(jobs.size());
+    std::atomic<size_t> next(0);
+    auto work = [&]() {
+        for (size_t i = next++; i < jobs.size(); i = next++) {
+            try {
+                out[i] = jobs[i]();
+            } catch (...) {
+                ex[i] = std::current_exception();
+            }
+        }
+    };
+    const size_t nt = std::min<size_t>(jobs.size(), std::max(1u, std::min(std::thread::hardware_concurrency(), 16u)));
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (const auto& e : ex)
+        if (e) std::rethrow_exception(e);
+    return out;
+}
+
 std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int per, bool calls, bool rec = false) {
     const std::string sfx = rec ? "_r" : "";
     const smg::DevGrid& g = h->g;
@@ -2050,10 +2083,19 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
         }
         return P;
     }
+    // Each program's source depends only on the (read-only) handle, so the
+    // programs are generated concurrently: for hundreds of moments the text
+    // runs to megabytes and would otherwise add tens of milliseconds to every
+    // new handle of a problem whose kernels are already compiled.
+    std::vector<int> Ds[2];
+    std::vector<std::vector<int>> Gs[2];
+    std::vector<std::function<KernelSrc()>> jobs;
     for (int phase = 0; phase < 2; ++phase) {
-        const std::vector<int> D = phase_dests(h, phase);
-        if (D.empty()) continue;
-        const std::vector<std::vector<int>> G = shared_groups(h, phase, group);
+        Ds[phase] = phase_dests(h, phase);
+        if (Ds[phase].empty()) continue;
+        Gs[phase] = shared_groups(h, phase, group);
+        const std::vector<int>& D = Ds[phase];
+        const std::vector<std::vector<int>>& G = Gs[phase];
         const int ng = (int)G.size();
         const int step = per > 0 ? per : ng;
         const int loader = rec ? 0 : staged_form(h);
@@ -2061,63 +2103,68 @@ std::vector<KernelSrc> programs(const smg_handle* h, int block, int group, int p
             const StagedShape S = staged_shape(h, ng);
             for (int k0 = 0; k0 < ng; k0 += step) {
                 const int k1 = std::min(ng, k0 + step);
-                int slots = 1;
-                for (int j = k0; j < k1; ++j) slots = std::max(slots, staged_rows(h, phase, D, G[j]).nslots());
-                const long long stage = (long long)slots * kStSlot;
-                const long long smem = (16 + S.st * stage) * 8;
-                const int minb = (int)std::max(1LL, std::min(4LL, (227LL * 1024) / (smem + 1024)));
-                KernelSrc k{std::string(kPrelude) + kStagePrelude,
-                            "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
-                            S.nb * (k1 - k0) * S.nch};
-                k.block = 32 * (S.ns + (loader == 1 ? 1 : 0));
-                k.smem = (int)smem;
-                k.form = loader;
-                ConstTable tab;
-                std::string body;
-                g_ctab = h->jit_const ? &tab : nullptr;
-                for (int j = k0; j < k1; ++j)
-                    emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage, loader);
-                g_ctab = nullptr;
-                k.src += ctab_decl(tab) + body;
-                emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name, loader, h->jit_band == 0);
-                P.push_back(std::move(k));
+                jobs.push_back([h, phase, k0, k1, loader, S, &D, &G]() {
+                    int slots = 1;
+                    for (int j = k0; j < k1; ++j) slots = std::max(slots, staged_rows(h, phase, D, G[j]).nslots());
+                    const long long stage = (long long)slots * kStSlot;
+                    const long long smem = (16 + S.st * stage) * 8;
+                    const int minb = (int)std::max(1LL, std::min(4LL, (227LL * 1024) / (smem + 1024)));
+                    KernelSrc k{std::string(kPrelude) + kStagePrelude,
+                                "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0), phase,
+                                S.nb * (k1 - k0) * S.nch};
+                    k.block = 32 * (S.ns + (loader == 1 ? 1 : 0));
+                    k.smem = (int)smem;
+                    k.form = loader;
+                    ConstTable tab;
+                    std::string body;
+                    g_ctab = h->jit_const ? &tab : nullptr;
+                    for (int j = k0; j < k1; ++j)
+                        emit_staged_group(body, h, phase, j, G[j], S.ns, S.st, S.rb, stage, loader);
+                    g_ctab = nullptr;
+                    k.src += ctab_decl(tab) + body;
+                    emit_staged_dispatch(k.src, phase, k0, k1, S, minb, k.name, loader, h->jit_band == 0);
+                    return k;
+                });
             }
             continue;
         }
         for (int k0 = 0; k0 < ng; k0 += step) {
             const int k1 = std::min(ng, k0 + step);
-            const int R = band_rows(h);
-            const long long rows = (long long)g.B[1] * g.B[2];
-            const long long ctas = R > 0 ? (long long)(k1 - k0) * ((rows + R - 1) / R) * R * (cta_per_group / rows)
-                                         : (long long)(k1 - k0) * cta_per_group;
-            KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase, ctas};
-            ConstTable tab;
-            std::string body;
-            g_ctab = h->jit_const ? &tab : nullptr;
-            int ring = 0;
-            if (!rec && h->jit_staged == 3 && !h->jit_xpair && !h->jit_prefetch) {
-                for (int j = k0; j < k1; ++j) ring = std::max(ring, prefetch_ring(prefetch_items(h, phase, D, G[j])));
-                if ((long long)ring * block * 16 > 48 * 1024) ring = 0;   // static shared memory limit
-            }
-            if (ring > 0) {
-                k.src += kStagePrelude;
-                k.form = 3;
-                body = "__shared__ double2 smg_ring[" + std::to_string(ring * block) + "];\n";
-                for (int j = k0; j < k1; ++j) emit_prefetch_group(body, h, phase, j, G[j], ring, block);
-            } else {
-                for (int j = k0; j < k1; ++j) {
-                    const int ahead = h->jit_prefetch >= 2 && !rec ? h->jit_prefetch - 1 : 0;
-                    const std::vector<int>* nx = (ahead && j + ahead < k1) ? &G[j + ahead] : nullptr;
-                    emit_shared_group(body, h, phase, j, G[j], rec, false, nx);
+            jobs.push_back([h, phase, k0, k1, block, rec, cta_per_group, &sfx, &D, &G]() {
+                const smg::DevGrid& g = h->g;
+                const int R = band_rows(h);
+                const long long rows = (long long)g.B[1] * g.B[2];
+                const long long ctas = R > 0 ? (long long)(k1 - k0) * ((rows + R - 1) / R) * R * (cta_per_group / rows)
+                                             : (long long)(k1 - k0) * cta_per_group;
+                KernelSrc k{kPrelude, "smg_jit_p" + std::to_string(phase) + "_" + std::to_string(k0) + sfx, phase, ctas};
+                ConstTable tab;
+                std::string body;
+                g_ctab = h->jit_const ? &tab : nullptr;
+                int ring = 0;
+                if (!rec && h->jit_staged == 3 && !h->jit_xpair && !h->jit_prefetch) {
+                    for (int j = k0; j < k1; ++j) ring = std::max(ring, prefetch_ring(prefetch_items(h, phase, D, G[j])));
+                    if ((long long)ring * block * 16 > 48 * 1024) ring = 0;   // static shared memory limit
                 }
-            }
-            g_ctab = nullptr;
-            k.src += ctab_decl(tab) + body;
-            emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
-            P.push_back(std::move(k));
+                if (ring > 0) {
+                    k.src += kStagePrelude;
+                    k.form = 3;
+                    body = "__shared__ double2 smg_ring[" + std::to_string(ring * block) + "];\n";
+                    for (int j = k0; j < k1; ++j) emit_prefetch_group(body, h, phase, j, G[j], ring, block);
+                } else {
+                    for (int j = k0; j < k1; ++j) {
+                        const int ahead = h->jit_prefetch >= 2 && !rec ? h->jit_prefetch - 1 : 0;
+                        const std::vector<int>* nx = (ahead && j + ahead < k1) ? &G[j + ahead] : nullptr;
+                        emit_shared_group(body, h, phase, j, G[j], rec, false, nx);
+                    }
+                }
+                g_ctab = nullptr;
+                k.src += ctab_decl(tab) + body;
+                emit_dispatch(k.src, h, phase, k0, k1, block, true, k.name, rec);
+                return k;
+            });
         }
     }
-    return P;
+    return run_jobs(jobs);
 }
 
 // regs > 0: register limit per thread of every function (--maxrregcount);
