@@ -731,8 +731,14 @@ std::string bounds(int block, int regs) {
 }
 
 std::string group_name(int phase, int k) { return "smg_g" + std::to_string(phase) + "_" + std::to_string(k); }
+// U and R are the same state pointer: the destinations are read and written
+// through U, the sources only read through R.  A phase never writes its
+// sources, so the two restrict-qualified names never touch one object that is
+// modified, and the compiler may move a later destination's source loads
+// above an earlier destination's store.
 std::string group_args(bool rec) {
-    return std::string("(double* __restrict__ U, const DevField* __restrict__ F, double hdt, int kf, int mode, int x0, "
+    return std::string("(double* __restrict__ U, const double* __restrict__ R, const DevField* __restrict__ F, double hdt, "
+                       "int kf, int mode, int x0, "
                        "int y, int z, bool act") +
            (rec ? ", double* __restrict__ WR, double* __restrict__ PR, const DevField* __restrict__ DE, int dsm, "
                   "int dsw)"
@@ -752,7 +758,7 @@ void emit_group(std::string& o, const smg_handle* h, int phase, int k, const std
     std::snprintf(b, sizeof b,
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
-                  "    const double* Up = U + pt;\n"
+                  "    const double* Up = R + pt;\n"
                   "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
                   (long long)g.s2, (long long)g.s1);
     o += b;
@@ -861,7 +867,7 @@ void emit_dispatch(std::string& o, const smg_handle* h, int phase, int k0, int k
                                              : "if (!act) return;");
     o += b;
     for (int k = k0; k < k1; ++k)
-        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, F, hdt, kf, mode, x0, y, z, act" +
+        o += "    case " + std::to_string(k) + ": " + group_name(phase, k) + "(U, U, F, hdt, kf, mode, x0, y, z, act" +
              (rec ? ", WR, PR, DE, dsm, dsw" : "") + "); break;\n";
     o += "    default: break;\n    }\n}\n";
 }
@@ -965,7 +971,7 @@ void emit_shared_group(std::string& o, const smg_handle* h, int phase, int k, co
         std::snprintf(b, sizeof b,
                       "    const int x1 = x0 + 1;\n"
                       "    const int pt = z * %lld + y * %lld + x0;\n"
-                      "    const double* Up = U + pt;\n"
+                      "    const double* Up = R + pt;\n"
                       "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
                       (long long)g.s2, (long long)g.s1);
         o += b;
@@ -1758,7 +1764,7 @@ void emit_prefetch_group(std::string& o, const smg_handle* h, int phase, int k, 
     std::snprintf(b, sizeof b,
                   "    const int x1 = x0 + 1;\n"
                   "    const int pt = z * %lld + y * %lld + x0;\n"
-                  "    const double* Up = U + pt;\n"
+                  "    const double* Up = R + pt;\n"
                   "    (void)x1; (void)kf; (void)mode; (void)hdt; (void)Up; (void)act;\n",
                   (long long)g.s2, (long long)g.s1);
     o += b;
