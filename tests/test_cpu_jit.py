@@ -119,15 +119,22 @@ def test_family_kernels_compile(name):
     assert fam.count("double* Uj = U + pt + ") == S.n_sys
 
 
+@pytest.mark.parametrize("split", [1, 16])
 @pytest.mark.parametrize("name", ["lattice_p5_substep", "pt3d_p3", "spn_3d"])
-def test_generated_source_is_deterministic(name):
+def test_generated_source_is_deterministic(name, split):
     """The per-process compile cache is keyed by source text, so the
     generator gives the same text for the same problem, also after another
-    problem was generated in between."""
-    _, a = _source(name, split=16)
+    problem was generated in between; with one group per program the
+    programs are written on several threads and must keep their order."""
+    _, a = _source(name, split=split)
     _source("odd_mixed_bc", split=4)
-    _, b = _source(name, split=16)
+    _, b = _source(name, split=split)
     assert a == b
+    names = [l.split("(")[1].rstrip(")") for l in a.splitlines() if l.startswith("// ---- program")]
+    assert len(names) >= 2
+    for phase in ("p0", "p1"):
+        firsts = [int(n.split("_")[-1]) for n in names if n.startswith("smg_jit_" + phase + "_")]
+        assert firsts == sorted(firsts) and len(firsts) == len(set(firsts))
 
 
 _CACHE_PROBE = r"""
