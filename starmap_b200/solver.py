@@ -468,11 +468,21 @@ def prepare(par: dict) -> _Setup:
     S.f_sg = sorted(set((*S.G(j), int(f_mom_order[j])) for j in range(1, n_sys))) if flag_filter else []
     # initial condition (starmap_solver.m:140-146)
     ic = par["ic"]
-    U = []
+    per_moment = nargin(ic) > 3
+    U, higher = [], {}
     for j in range(n_sys):
-        X, Y, Z = XYZ(S.G(j))
-        val = capargs(ic, X, Y, Z, j + 1)
-        U.append(X * 0 + np.asarray(val, dtype=np.float64) * float(nargin(ic) > 3 or j == 0))
+        g = S.G(j)
+        X, Y, Z = XYZ(g)
+        if per_moment or j == 0:
+            val = capargs(ic, X, Y, Z, j + 1)
+            U.append(X * 0 + np.asarray(val, dtype=np.float64) * 1.0)
+            continue
+        # a higher moment of an initial condition with at most three
+        # arguments: X*0 + ic(X,Y,Z)*0, which the call's arguments fix per
+        # grid, so it is evaluated once per grid and copied
+        if g not in higher:
+            higher[g] = X * 0 + np.asarray(capargs(ic, X, Y, Z, j + 1), dtype=np.float64) * 0.0
+        U.append(higher[g].copy(order="K"))
     S.U0 = U
     if S.timestep > 0:
         S.M_sym = timestep.symbol(Mx, My, Mz, h)
