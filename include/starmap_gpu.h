@@ -17,7 +17,9 @@
  *     message of the last failure on a handle is smg_last_error(handle), and
  *     of a failed smg_create / handle-less call smg_last_error(NULL).  The
  *     handle-less message is kept per host thread: the pointer stays valid
- *     until the same thread's next handle-less failure.
+ *     until the same thread's next handle-less failure.  No C++ exception
+ *     leaves the library: host memory exhausted inside a call returns
+ *     SMG_ENOMEM, any other C++ exception SMG_EINVAL, with its message.
  *   - Arrays follow MATLAB's column-major order.  Component j lives on the
  *     staggered grid gt[3*j+d] (1 = cell centres, 2 = staggered points) and
  *     has extent n[d] along solver dimension d, or n[d]+1 when gt == 2 and
@@ -48,7 +50,7 @@ extern "C" {
 #define SMG_ECUDA      -2   /* CUDA runtime/launch failure */
 #define SMG_ETIMEOUT   -3   /* a bounded device wait gave up (batched grid barrier) */
 #define SMG_ENONFINITE -4   /* non-finite state detected by smg_check_finite */
-#define SMG_ENOMEM     -5   /* device allocation failed */
+#define SMG_ENOMEM     -5   /* device or host allocation failed */
 #define SMG_ESTATE     -6   /* call out of order (e.g. run before the state is set) */
 
 #define SMG_VARIANT_AUTO    0  /* best available kernel family (JIT, else pair, else strip); phase A fused (default) */

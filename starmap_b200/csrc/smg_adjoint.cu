@@ -833,6 +833,7 @@ void smg_adjoint_free(smg_handle* h) { free_adj(h); }
 extern "C" {
 
 int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
+    SMG_TRY
     if (!h) return SMG_EINVAL;
     if (nsteps < 1 || ckpt_every < 0)
         return afail(h, SMG_EINVAL, "smg_forward: nsteps must be >= 1 and ckpt_every >= 0");
@@ -1006,9 +1007,11 @@ int smg_forward(smg_handle* h, int64_t nsteps, int64_t ckpt_every) {
     A->seeded = false;
     A->tail_valid = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_misfit(smg_handle* h, const double* obs, double* J) {
+    SMG_TRY
     if (!h || !obs) return SMG_EINVAL;
     AdjData* A = h->adj;
     if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_misfit: call smg_forward first");
@@ -1036,9 +1039,11 @@ int smg_misfit(smg_handle* h, const double* obs, double* J) {
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     A->seeded = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_adjoint_seed(smg_handle* h, const double* const* lam) {
+    SMG_TRY
     if (!h || !lam) return SMG_EINVAL;
     AdjData* A = h->adj;
     if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_adjoint_seed: call smg_forward first");
@@ -1057,9 +1062,11 @@ int smg_adjoint_seed(smg_handle* h, const double* const* lam) {
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     A->seeded = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fields) {
+    SMG_TRY
     if (!h) return SMG_EINVAL;
     AdjData* A = h->adj;
     if (!A || !A->ready) return afail(h, SMG_ESTATE, "smg_backward: call smg_forward first");
@@ -1123,19 +1130,24 @@ int smg_backward(smg_handle* h, double* const* grad_U0, double* const* grad_fiel
     }
     A_CUDA(h, cudaStreamSynchronize(h->stream));
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_adjoint_bytes(const smg_handle* h, int64_t* bytes) {
+    SMG_TRY
     if (!h || !bytes) return SMG_EINVAL;
     *bytes = h->adj ? (int64_t)h->adj->bytes : 0;
     return SMG_OK;
+    SMG_CATCH(h ? &const_cast<smg_handle*>(h)->err : nullptr)
 }
 
 int smg_adjoint_info(const smg_handle* h, int64_t* K, int64_t* nseg) {
+    SMG_TRY
     if (!h) return SMG_EINVAL;
     if (K) *K = h->adj ? h->adj->K : 0;
     if (nseg) *nseg = h->adj ? h->adj->nseg : 0;
     return SMG_OK;
+    SMG_CATCH(h ? &const_cast<smg_handle*>(h)->err : nullptr)
 }
 
 }  // extern "C"

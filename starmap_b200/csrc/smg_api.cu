@@ -12,6 +12,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -607,6 +609,30 @@ bool strip_usable(const smg_handle* h) {
 }  // namespace
 
 void smg::set_global_error(const std::string& msg) { fail(nullptr, 0, msg); }
+
+int smg::exception_status(std::string* err, const char* fn) noexcept {
+    int code = SMG_EINVAL;
+    const char* what = "unknown exception";
+    try {
+        throw;
+    } catch (const std::bad_alloc&) {
+        code = SMG_ENOMEM;
+        what = "out of host memory";
+    } catch (const std::length_error& e) {
+        code = SMG_ENOMEM;
+        what = e.what();
+    } catch (const std::exception& e) {
+        what = e.what();
+    } catch (...) {
+    }
+    try {
+        const std::string m = std::string(fn) + ": " + what;
+        if (err) *err = m;
+        else set_global_error(m);
+    } catch (...) {   // no memory left for the message either
+    }
+    return code;
+}
 int smg::create_host(const smg_problem* p, smg_handle** out) { return create_impl(p, out, false); }
 
 extern "C" {
@@ -619,20 +645,25 @@ const char* smg_last_error(const smg_handle* h) {
 }
 
 int smg_device_count(void) {
+    SMG_TRY
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return 0;
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
     return n;
+    SMG_CATCH(nullptr)
 }
 
 int smg_set_device(int32_t device) {
+    SMG_TRY
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
     return SMG_OK;
+    SMG_CATCH(nullptr)
 }
 
 int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double* Mz, int32_t* gt_out) {
+    SMG_TRY
     if (n_sys < 1 || !Mx || !My || !Mz || !gt_out) return fail(nullptr, SMG_EINVAL, "smg_classify: bad arguments");
     const double* M[3] = {Mx, My, Mz};
     // I[d][j]: sorted columns i with M_d(j,i) != 0 (starmap_solver.m:77-79)
@@ -678,9 +709,10 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
     for (int j = 0; j < n_sys; ++j)
         for (int d = 0; d < 3; ++d) gt_out[3 * j + d] = 1 + ((cls[j] >> d) & 1);
     return SMG_OK;
+    SMG_CATCH(nullptr)
 }
 
-int smg_create(const smg_problem* p, smg_handle** out) { return create_impl(p, out, true); }
+int smg_create(const smg_problem* p, smg_handle** out) { SMG_TRY return create_impl(p, out, true); SMG_CATCH(nullptr) }
 
 }  // extern "C"
 
@@ -989,6 +1021,7 @@ void smg_destroy(smg_handle* h) {
 }
 
 int smg_set_state(smg_handle* h, const double* const* U) {
+    SMG_TRY
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_set_state: NULL argument");
     for (int j = 0; j < h->n_sys; ++j)
         if (!U[j]) return fail(h, SMG_EINVAL, "smg_set_state: NULL component pointer");
@@ -996,18 +1029,22 @@ int smg_set_state(smg_handle* h, const double* const* U) {
     if (rc != SMG_OK) return rc;
     h->state_set = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_get_state(smg_handle* h, double* const* U) {
+    SMG_TRY
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_state: NULL argument");
     const int rc = staged_transfer(h, false, nullptr, U, nullptr, 0.0, 0.0);
     if (rc == SMG_OK && smg::jit_status(h) == SMG_ETIMEOUT)
         return fail(h, SMG_ETIMEOUT,
                     "smg_get_state: a staged kernel's shared-memory pipeline wait ran out (state undefined)");
     return rc;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_snapshot(smg_handle* h) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_snapshot: NULL handle");
     if (!h->state_set) return fail(h, SMG_ESTATE, "smg_snapshot: smg_set_state has not been called");
     const size_t bytes = (size_t)h->g.cs * h->n_sys * sizeof(double);
@@ -1018,16 +1055,20 @@ int smg_snapshot(smg_handle* h) {
     SMG_CUDA(h, cudaMemcpyAsync(h->dSnap, h->dU, bytes, cudaMemcpyDeviceToDevice, h->stream));
     h->snap_set = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_get_interp(smg_handle* h, double lambda, double* const* U) {
+    SMG_TRY
     if (!h || !U) return fail(h, SMG_EINVAL, "smg_get_interp: NULL argument");
     if (!h->snap_set) return fail(h, SMG_ESTATE, "smg_get_interp: smg_snapshot has not been called");
     if (!std::isfinite(lambda)) return fail(h, SMG_EINVAL, "smg_get_interp: lambda must be finite");
     return staged_transfer(h, false, nullptr, U, h->dSnap, 1.0 - lambda, lambda);
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_field: NULL handle");
     if (f < 0 || f >= h->field_one) return fail(h, SMG_EINVAL, "smg_set_field: field index out of range");
     DevField& F = h->fields_host[f];
@@ -1046,14 +1087,17 @@ int smg_set_field(smg_handle* h, int32_t f, const double* data, double scalar) {
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (h->dt_set) return smg_set_dt(h, h->dt);   // refresh derived decays
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_time(smg_handle* h, double t) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_time: NULL handle");
     if (!std::isfinite(t)) return fail(h, SMG_EINVAL, "smg_set_time: t must be finite");
     h->t = t;
     h->mat.init = false;   // materials re-evaluated at t before the next step
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 // The coordinate table of the material and filter expressions: per solver
@@ -1088,6 +1132,7 @@ static bool array_field(const smg_handle* h, int f) {
 
 int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0, const char* expr_sm, int32_t nrows,
                           const int32_t* rows, int32_t sA_field, int32_t EA_field, const double* const* coords) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL handle");
     smg::src_free(h, false);
     cudaFree(h->mat.dOld);
@@ -1120,10 +1165,12 @@ int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0
     M.init = false;
     h->mat = M;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const int32_t* rows,
                         const double* const* coords) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_filter_expr: NULL handle");
     smg::src_free(h, false);
     h->filt = smg_handle::FiltExpr{};
@@ -1147,10 +1194,12 @@ int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const in
     if (rc != SMG_OK) return rc;
     h->filt = F;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const double* x, const double* y,
                         const double* z) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_source_expr: NULL handle");
     if (comp < 0 || comp >= h->n_sys) return fail(h, SMG_EINVAL, "smg_set_source_expr: component out of range");
     const int f = h->comps[comp].Q;
@@ -1191,9 +1240,11 @@ int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const dou
     h->src_expr[at].expr = expr;
     h->src_expr[at].dC = d;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_dt(smg_handle* h, double dt) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_dt: NULL handle");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, SMG_EINVAL, "smg_set_dt: dt must be finite and > 0");
     h->dt = dt;
@@ -1220,6 +1271,7 @@ int smg_set_dt(smg_handle* h, double dt) {
     }
     h->dt_set = true;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 // Enqueue `nsteps` Strang steps; *launches receives the kernel count.
@@ -1285,11 +1337,13 @@ static cudaError_t enqueue_steps(smg_handle* h, int64_t nsteps, cudaStream_t s, 
 }
 
 int smg_run(smg_handle* h, int64_t nsteps) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_run: NULL handle");
     if (nsteps < 0) return fail(h, SMG_EINVAL, "smg_run: nsteps must be >= 0");
     if (!h->dt_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_dt has not been called");
     if (!h->state_set) return fail(h, SMG_ESTATE, "smg_run: smg_set_state has not been called");
     return smg::run_steps(h, nsteps, true);
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 }  // extern "C"
@@ -1390,6 +1444,7 @@ int smg::run_steps(smg_handle* h, int64_t nsteps, bool events) {
 extern "C" {
 
 int smg_tune(smg_handle* h, int32_t key, int32_t value) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_tune: NULL handle");
     switch (key) {
         case SMG_TUNE_PAIR_GROUP:
@@ -1511,9 +1566,11 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
         h->graph_steps = 0;
     }
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap) {
+    SMG_TRY
     if (!h || !variant) return fail(h, SMG_EINVAL, "smg_active_variant: NULL argument");
     int v;
     if (h->jit && (h->variant == SMG_VARIANT_JIT || h->variant == SMG_VARIANT_AUTO)) v = SMG_VARIANT_JIT;
@@ -1535,9 +1592,11 @@ int smg_active_variant(smg_handle* h, int32_t* variant, char* why, int64_t cap) 
         why[n] = '\0';
     }
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_set_variant(smg_handle* h, int32_t variant) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_set_variant: NULL handle");
     if (variant < SMG_VARIANT_AUTO || variant > SMG_VARIANT_JIT)
         return fail(h, SMG_EINVAL, "smg_set_variant: unknown variant");
@@ -1558,17 +1617,21 @@ int smg_set_variant(smg_handle* h, int32_t variant) {
         h->graph_steps = 0;
     }
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_sync(smg_handle* h) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_sync: NULL handle");
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (smg::jit_status(h) == SMG_ETIMEOUT)
         return fail(h, SMG_ETIMEOUT, "smg_sync: a staged kernel's shared-memory pipeline wait ran out (state undefined)");
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_last_run_stats(smg_handle* h, double* ms, int64_t* launches) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_last_run_stats: NULL handle");
     SMG_CUDA(h, cudaEventSynchronize(h->ev1));
     float f = 0.f;
@@ -1576,9 +1639,11 @@ int smg_last_run_stats(smg_handle* h, double* ms, int64_t* launches) {
     if (ms) *ms = f;
     if (launches) *launches = h->last_launches;
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 int smg_layout(const smg_handle* h, int64_t* bytes, int64_t dims_out[4]) {
+    SMG_TRY
     if (!h) return fail(nullptr, SMG_EINVAL, "smg_layout: NULL handle");
     if (bytes) *bytes = (int64_t)h->bytes;
     if (dims_out) {
@@ -1588,9 +1653,11 @@ int smg_layout(const smg_handle* h, int64_t* bytes, int64_t dims_out[4]) {
         dims_out[3] = h->g.cs;
     }
     return SMG_OK;
+    SMG_CATCH(h ? &const_cast<smg_handle*>(h)->err : nullptr)
 }
 
 int smg_check_finite(smg_handle* h) {
+    SMG_TRY
     if (!h) return fail(h, SMG_EINVAL, "smg_check_finite: NULL handle");
     int flag = 0;
     SMG_CUDA(h, cudaMemsetAsync(h->dFlag, 0, sizeof(int), h->stream));
@@ -1599,6 +1666,7 @@ int smg_check_finite(smg_handle* h) {
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (flag) return fail(h, SMG_ENONFINITE, "state holds NaN or Inf");
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 }  // extern "C"

@@ -172,7 +172,9 @@ struct smg_batch {
 
 namespace {
 
-std::string g_batch_err;
+thread_local std::string g_batch_err;   // message of smg_batch_last_error(NULL), per host thread
+
+std::string* batch_err(const smg_batch* b) { return b ? &const_cast<smg_batch*>(b)->err : &g_batch_err; }
 
 int bfail(smg_batch* b, int code, const std::string& m) {
     if (b) b->err = m;
@@ -360,6 +362,7 @@ cudaError_t enqueue_run(smg_batch* b, int64_t nsteps, int64_t* launches) {
 extern "C" {
 
 int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch** out) {
+    SMG_TRY
     if (!out || n_inst < 1 || !probs) return bfail(nullptr, SMG_EINVAL, "smg_batch_create: bad arguments");
     *out = nullptr;
     // the batch kernels apply no full-step filter (f_position 'full',
@@ -403,6 +406,7 @@ int smg_batch_create(int32_t n_inst, const smg_problem* const* probs, smg_batch*
     }
     *out = b;
     return SMG_OK;
+    SMG_CATCH(batch_err(nullptr))
 }
 
 void smg_batch_destroy(smg_batch* b) {
@@ -426,6 +430,7 @@ smg_handle* smg_batch_instance(smg_batch* b, int32_t i) {
 }
 
 int smg_batch_set_dt(smg_batch* b, const double* dt) {
+    SMG_TRY
     if (!b || !dt) return bfail(b, SMG_EINVAL, "smg_batch_set_dt: NULL argument");
     for (size_t i = 0; i < b->inst.size(); ++i) {
         const int rc = smg_set_dt(b->inst[i], dt[i]);
@@ -433,9 +438,11 @@ int smg_batch_set_dt(smg_batch* b, const double* dt) {
         b->dt[i] = dt[i];
     }
     return build_items(b);   // hdt and refreshed coefficient tables enter the argument table
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_run(smg_batch* b, int64_t nsteps) {
+    SMG_TRY
     if (!b) return bfail(b, SMG_EINVAL, "smg_batch_run: NULL batch");
     if (nsteps < 0) return bfail(b, SMG_EINVAL, "smg_batch_run: nsteps must be >= 0");
     for (size_t i = 0; i < b->inst.size(); ++i) {
@@ -497,16 +504,20 @@ int smg_batch_run(smg_batch* b, int64_t nsteps) {
     b->last_ms = ms;
     if (st.err) return bfail(b, SMG_ETIMEOUT, "batch grid barrier wait exceeded its spin limit");
     return SMG_OK;
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_last_run_stats(smg_batch* b, double* ms, int64_t* launches) {
+    SMG_TRY
     if (!b) return bfail(b, SMG_EINVAL, "smg_batch_last_run_stats: NULL batch");
     if (ms) *ms = b->last_ms;
     if (launches) *launches = b->last_launches;
     return SMG_OK;
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_tune(smg_batch* b, int32_t key, int64_t value) {
+    SMG_TRY
     if (!b) return bfail(b, SMG_EINVAL, "smg_batch_tune: NULL batch");
     switch (key) {
         case SMG_BATCH_BLOCK:
@@ -543,25 +554,31 @@ int smg_batch_tune(smg_batch* b, int32_t key, int64_t value) {
             return bfail(b, SMG_EINVAL, "smg_batch_tune: unknown key");
     }
     return build_items(b);
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_info(const smg_batch* b, int64_t* jit_active, int64_t* families) {
+    SMG_TRY
     if (!b) return bfail(nullptr, SMG_EINVAL, "smg_batch_info: NULL batch");
     if (jit_active) *jit_active = use_fam(b) ? 1 : 0;
     if (families) *families = smg::jit_family_count(b->fam);
     return SMG_OK;
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_config(const smg_batch* b, int64_t out[4]) {
+    SMG_TRY
     if (!b || !out) return bfail(nullptr, SMG_EINVAL, "smg_batch_config: NULL argument");
     out[0] = b->block;
     out[1] = b->group;
     out[2] = b->steps_per_launch;
     out[3] = b->persistent ? b->grid : 0;
     return SMG_OK;
+    SMG_CATCH(batch_err(b))
 }
 
 int smg_batch_autotune(smg_batch* b, int64_t probe_steps, double* best_ms) {
+    SMG_TRY
     if (!b || probe_steps < 1) return bfail(b, SMG_EINVAL, "smg_batch_autotune: bad arguments");
     // snapshot every instance's state; the probes advance it
     std::vector<double*> save(b->inst.size(), nullptr);
@@ -621,6 +638,7 @@ done:
     if (rc != SMG_OK) return rc;
     if (best_ms) *best_ms = best;
     return build_items(b);
+    SMG_CATCH(batch_err(b))
 }
 
 }  // extern "C"

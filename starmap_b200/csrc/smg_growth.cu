@@ -120,6 +120,7 @@ int fail(int code, const std::string& m) {
 }  // namespace
 
 extern "C" int smg_growth_radius(int32_t n, const double* G, const int32_t* odd, double* la) {
+    SMG_TRY
     if (n < 1 || !G || !odd || !la) return fail(SMG_EINVAL, "smg_growth_radius: need n >= 1 and non-NULL arrays");
     LinalgApi& a = linalg();
     if (!a.ok) return fail(SMG_EINVAL, "smg_growth_radius: " + a.why);
@@ -204,4 +205,5 @@ extern "C" int smg_growth_radius(int32_t n, const double* G, const int32_t* odd,
     for (const cuDoubleComplex& v : ev) m = std::fmax(m, std::hypot(v.x, v.y));
     *la = m;
     return SMG_OK;
+    SMG_CATCH(nullptr)
 }

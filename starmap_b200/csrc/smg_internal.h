@@ -9,6 +9,13 @@
 
 #include "smg_device.cuh"
 
+#define SMG_TRY try {
+#define SMG_CATCH(err)                                   \
+    }                                                    \
+    catch (...) {                                        \
+        return smg::exception_status((err), __func__);   \
+    }
+
 struct smg_problem;
 
 namespace smg {
@@ -172,6 +179,13 @@ constexpr int kStripWarps = 8;
 constexpr int kSumsqBlocks = 32;     // CTAs per component in the sum-of-squares reduction
 constexpr int kSumsqThreads = 256;
 void set_global_error(const std::string& msg);   // message of smg_last_error(NULL)
+// No C++ exception reaches a caller of the C ABI: every entry point's body
+// sits between SMG_TRY and SMG_CATCH(err), and an exception that escapes it
+// (host memory exhausted, a thread that cannot be started) becomes SMG_ENOMEM
+// or SMG_EINVAL with "<entry point>: <what>" in *err (the handle's message),
+// or in the handle-less message when err is NULL.  Called only from a catch
+// handler.
+int exception_status(std::string* err, const char* fn) noexcept;
 int run_steps(smg_handle* h, int64_t nsteps, bool events);   // smg_run without argument checks
 int jit_build(smg_handle* h, std::string& err);             // generate, compile, load (SMG_OK or error)
 void jit_free(smg_handle* h);

@@ -2035,6 +2035,19 @@ struct KernelSrc {
 //   inline (calls false): `per` groups per program (0: all of the phase),
 //          each program one kernel over its groups with their code inlined;
 //          the kernels of a phase run concurrently.
+// Starts up to n helper threads running `work`.  A thread that cannot be
+// started (no memory for its stack, a thread limit) is not an error: the
+// threads already running and the caller share the work, and no joinable
+// thread is left to an unwinding vector (which would end the process).
+template <typename F>
+void start_workers(std::vector<std::thread>& th, size_t n, F& work) {
+    try {
+        th.reserve(n);
+        for (size_t t = 0; t < n; ++t) th.emplace_back(work);
+    } catch (...) {
+    }
+}
+
 // Runs the generators on up to 16 threads; the programs keep their order.
 // An exception in a generator (out of memory) is passed on to the caller.
 std::vector<KernelSrc> run_jobs(const std::vector<std::function<KernelSrc()>>& jobs) {
@@ -2052,7 +2065,7 @@ std::vector<KernelSrc> run_jobs(const std::vector<std::function<KernelSrc()>>& j
     };
     const size_t nt = std::min<size_t>(jobs.size(), std::max(1u, std::min(std::thread::hardware_concurrency(), 16u)));
     std::vector<std::thread> th;
-    for (size_t t = 1; t < nt; ++t) th.emplace_back(work);
+    start_workers(th, nt - 1, work);
     work();
     for (auto& t : th) t.join();
     for (const auto& e : ex)
@@ -2676,7 +2689,7 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
         for (size_t i = next++; i < P.size(); i = next++) rcs[i] = compile_one(P[i].src, regs, link, obj[i], errs[i]);
     };
     std::vector<std::thread> th;
-    for (unsigned t = 1; t < std::min<size_t>(nt, P.size()); ++t) th.emplace_back(work);
+    start_workers(th, std::min<size_t>(nt, P.size()) - 1, work);
     work();
     for (auto& t : th) t.join();
     for (size_t i = 0; i < P.size(); ++i)
@@ -3473,6 +3486,7 @@ static size_t adj_count(const std::vector<KernelSrc>& v) {
 
 extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const int32_t* values, int32_t ntune,
                               int32_t compile, char* buf, int64_t cap, int64_t* len) {
+    SMG_TRY
     if (!p || ntune < 0 || (ntune > 0 && (!keys || !values))) {
         smg::set_global_error("smg_jit_source: bad arguments");
         return SMG_EINVAL;
@@ -3534,10 +3548,13 @@ extern "C" int smg_jit_source(const smg_problem* p, const int32_t* keys, const i
     }
     delete h;
     return rc;
+    SMG_CATCH(nullptr)
 }
 
 extern "C" int smg_jit_stats(int64_t* compiled, int64_t* from_disk) {
+    SMG_TRY
     if (compiled) *compiled = g_programs_compiled.load();
     if (from_disk) *from_disk = g_programs_from_disk.load();
     return SMG_OK;
+    SMG_CATCH(nullptr)
 }

@@ -59,6 +59,7 @@ cudaError_t launch_sumsq(const double* x, int ncomp, long long stride, long long
 }  // namespace smg
 
 extern "C" int smg_state_sumsq(smg_handle* h, double* sumsq) {
+    SMG_TRY
     if (!h || !sumsq) return SMG_EINVAL;
     if (!h->dSumsq) {
         h->err = "smg_state_sumsq: no reduction buffer";
@@ -75,6 +76,7 @@ extern "C" int smg_state_sumsq(smg_handle* h, double* sumsq) {
         return SMG_ECUDA;
     }
     return SMG_OK;
+    SMG_CATCH(h ? &h->err : nullptr)
 }
 
 // ---------------------------------------------------------------------------
@@ -141,6 +143,7 @@ unsigned long long current_ctx_id() {
 
 extern "C" int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t stride, int64_t len, double* d_out,
                                  void* stream) {
+    SMG_TRY
     if (!d_x || !d_out) return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: NULL device pointer");
     if (ncomp < 1 || len < 1 || stride < len)
         return noalloc_fail(SMG_EINVAL, "smg_sumsq_noalloc: need ncomp >= 1, len >= 1 and stride >= len");
@@ -176,4 +179,5 @@ extern "C" int smg_sumsq_noalloc(const double* d_x, int32_t ncomp, int64_t strid
     e = smg::launch_sumsq(d_x, ncomp, stride, len, scratch, d_out, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return noalloc_fail(SMG_ECUDA, std::string("smg_sumsq_noalloc: ") + cudaGetErrorString(e));
     return SMG_OK;
+    SMG_CATCH(nullptr)
 }
