@@ -43,6 +43,7 @@ SMG_TUNE_JIT_STAGES = 18
 SMG_TUNE_JIT_ROWS = 19
 SMG_TUNE_ADJ_PRIORITY = 20
 SMG_TUNE_DIRECT_XFER = 21
+SMG_TUNE_JIT_LANES = 22
 
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1

@@ -1545,6 +1545,10 @@ int smg_tune(smg_handle* h, int32_t key, int32_t value) {
             if (value < -1 || value > 4096) return fail(h, SMG_EINVAL, "smg_tune: graph steps must be -1..4096");
             h->graph_block = value;
             break;
+        case SMG_TUNE_JIT_LANES:
+            if (value < 0 || value > 64) return fail(h, SMG_EINVAL, "smg_tune: jit lanes must be 0..64");
+            h->jit_lanes = value;
+            break;
         case SMG_TUNE_DIRECT_XFER:
             if (value != 0 && value != 1) return fail(h, SMG_EINVAL, "smg_tune: direct xfer must be 0 or 1");
             h->direct_xfer = value;

@@ -156,6 +156,7 @@ struct smg_handle {
     int jit_prefetch = 0;            // L2 prefetch of a group's rows before its loads
     int jit_const = 1;               // coupling weights and grid constants from a __constant__ table
     int jit_band = -1;               // rows per band of the CTA order (0: group-major; -1: by slot size)
+    int jit_lanes = 0;               // kernels of a phase at the same time, 0 = all (SMG_TUNE_JIT_LANES)
     int direct_xfer = 1;             // page-locked host arrays are moved by one kernel without staging
     int jit_staged = 0;              // 0 register form, 1 staged by bulk copies, 2 by async copies, 3 prefetch ring
     int jit_slices = 4;              // consumer warps (destination slices) per staged CTA

@@ -2889,11 +2889,16 @@ cudaError_t launch_state(const smg_handle* h, JitState* J, double* U, int mode, 
                    : cudaErrorLaunchFailure;
     };
     if (K.size() == 1) return go(K[0], s);
+    // at most `lanes` kernels at a time: kernel i runs on side stream i mod
+    // lanes, after kernel i - lanes
+    const size_t lanes = h->jit_lanes > 0 ? std::min<size_t>((size_t)h->jit_lanes, K.size()) : K.size();
     cudaError_t e = cudaEventRecord(J->fork, s);
     if (e != cudaSuccess) return e;
-    for (size_t i = 0; i < K.size(); ++i) {
+    for (size_t i = 0; i < lanes; ++i)
         if ((e = cudaStreamWaitEvent(J->side[i], J->fork, 0)) != cudaSuccess) return e;
-        if ((e = go(K[i], J->side[i])) != cudaSuccess) return e;
+    for (size_t i = 0; i < K.size(); ++i)
+        if ((e = go(K[i], J->side[i % lanes])) != cudaSuccess) return e;
+    for (size_t i = 0; i < lanes; ++i) {
         if ((e = cudaEventRecord(J->join[i], J->side[i])) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s, J->join[i], 0)) != cudaSuccess) return e;
     }
@@ -3267,11 +3272,16 @@ cudaError_t launch_jit_adj(const smg_handle* h, int l, int coup, int pm, int pm_
                    : cudaErrorLaunchFailure;
     };
     if (K.size() == 1) return go(K[0], s);
+    // at most `lanes` kernels at a time: kernel i runs on side stream i mod
+    // lanes, after kernel i - lanes
+    const size_t lanes = h->jit_lanes > 0 ? std::min<size_t>((size_t)h->jit_lanes, K.size()) : K.size();
     cudaError_t e = cudaEventRecord(J->fork, s);
     if (e != cudaSuccess) return e;
-    for (size_t i = 0; i < K.size(); ++i) {
+    for (size_t i = 0; i < lanes; ++i)
         if ((e = cudaStreamWaitEvent(J->side[i], J->fork, 0)) != cudaSuccess) return e;
-        if ((e = go(K[i], J->side[i])) != cudaSuccess) return e;
+    for (size_t i = 0; i < K.size(); ++i)
+        if ((e = go(K[i], J->side[i % lanes])) != cudaSuccess) return e;
+    for (size_t i = 0; i < lanes; ++i) {
         if ((e = cudaEventRecord(J->join[i], J->side[i])) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s, J->join[i], 0)) != cudaSuccess) return e;
     }
