@@ -96,6 +96,11 @@ def test_generated_source_compiles(name, layout):
 def test_bad_tuning_rejected():
     with pytest.raises(_lib.SmgError):
         _source("one_d_p5", block=48)
+    for lanes in (-1, 65):
+        with pytest.raises(_lib.SmgError):
+            _source("one_d_p5", lanes=lanes)
+    _source("one_d_p5", lanes=2)   # launch setting: the source is the same
+    assert _source("one_d_p5", lanes=2)[1] == _source("one_d_p5")[1]
 
 
 @pytest.mark.parametrize("name", ["odd_mixed_bc", "pt3d_p3", "lattice_p5_substep", "lattice_p6_nofilter"])

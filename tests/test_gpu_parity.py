@@ -260,6 +260,7 @@ def test_jit_tuning_keeps_results(block, group, split, calls, xpair, prefetch, b
                 solver.tune(_lib.SMG_TUNE_JIT_PREFETCH, prefetch)
                 solver.tune(_lib.SMG_TUNE_JIT_BAND, band)
                 solver.tune(_lib.SMG_TUNE_JIT_CONST, const)
+                solver.tune(_lib.SMG_TUNE_JIT_LANES, group % 3)   # 0 (all), 1 or 2 kernels at a time
                 solver.set_variant(5)
             else:
                 solver.set_variant(4)
