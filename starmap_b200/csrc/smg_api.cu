@@ -188,13 +188,24 @@ __global__ void k_xfer_direct(XferDirect c, double* __restrict__ U, const double
 }
 
 // the device address of a page-locked host array, or nullptr (pageable memory)
-double* device_view(const void* p) {
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();   // clear the error of an unregistered pointer
-        return nullptr;
-    }
-    return a.type == cudaMemoryTypeHost ? static_cast<double*>(a.devicePointer) : nullptr;
+// Device address of the page-locked host range [p, p + bytes), or NULL when
+// its first or last byte is not page-locked or the two are not mapped as one
+// contiguous range (an array only partly registered goes through staging:
+// the direct kernel must never touch an unmapped host page).
+double* device_view(const void* p, size_t bytes) {
+    auto view = [](const void* q) -> char* {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();   // clear the error of an unregistered pointer
+            return nullptr;
+        }
+        return a.type == cudaMemoryTypeHost ? static_cast<char*>(a.devicePointer) : nullptr;
+    };
+    if (bytes == 0) return nullptr;
+    char* first = view(p);
+    if (!first) return nullptr;
+    char* last = view(static_cast<const char*>(p) + (bytes - 1));
+    return last == first + (bytes - 1) ? reinterpret_cast<double*>(first) : nullptr;
 }
 
 // Transfer of the components with non-NULL host pointers.  When every one of
@@ -246,7 +257,8 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
         for (int j = 0; j < h->n_sys && direct; ++j) {
             const void* p = upload ? (const void*)Uin[j] : (const void*)Uout[j];
             if (!p) continue;
-            hp[j] = device_view(p);
+            const int* e = h->comps[j].ext;
+            hp[j] = device_view(p, (size_t)e[0] * e[1] * e[2] * sizeof(double));
             direct = hp[j] != nullptr;
         }
         if (direct) return direct_transfer(h, upload, hp, snap, wa, wb);

@@ -51,3 +51,39 @@ def test_direct_and_staged_transfers_agree(name):
     for j in res[0][0]:
         np.testing.assert_array_equal(res[1][0][j], res[0][0][j])
         np.testing.assert_array_equal(res[1][1][j], res[0][1][j])
+
+
+@pytest.mark.parametrize("half", ["first", "second"])
+def test_partly_page_locked_arrays_take_the_staged_path(half):
+    """An array of which only one half is page-locked (cudaHostRegister of a
+    sub-range) must not be read or written in place: its other half has no
+    device mapping.  Such arrays go through the staging buffer and the values
+    arrive intact in both directions."""
+    torch = pytest.importorskip("torch")
+    cudart = torch.cuda.cudart()
+    par = starmap_init(cases.ALL["lattice_p5_substep"]())
+    S, fs, solver, T = setup_gpu(par)
+    regs = []
+    try:
+        rng = np.random.default_rng(5)
+        U0 = [np.asfortranarray(rng.standard_normal(solver.extents(j))) for j in range(S.n_sys)]
+        outs = {j: np.zeros(int(np.prod(solver.extents(j)))) for j in range(S.n_sys)}
+        page = 4096
+        for a in list(U0) + list(outs.values()):
+            nbytes = a.size * 8
+            assert nbytes > 4 * page
+            base = a.ctypes.data
+            lo = (base + page - 1) // page * page           # whole pages inside the array
+            hi = (base + nbytes) // page * page
+            mid = (lo + hi) // 2 // page * page
+            start, end = (lo, mid) if half == "first" else (mid, hi)
+            assert int(cudart.cudaHostRegister(start, end - start, 0)) == 0
+            regs.append(start)
+        solver.set_state(U0)
+        back = solver.get_state(out=outs)
+        for j in range(S.n_sys):
+            np.testing.assert_array_equal(back[j], U0[j])
+    finally:
+        for r in regs:
+            cudart.cudaHostUnregister(r)
+        solver.close()
