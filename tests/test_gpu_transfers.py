@@ -61,7 +61,8 @@ def test_partly_page_locked_arrays_take_the_staged_path(half):
     arrive intact in both directions."""
     torch = pytest.importorskip("torch")
     cudart = torch.cuda.cudart()
-    par = starmap_init(cases.ALL["lattice_p5_substep"]())
+    from starmap_b200 import configs
+    par = starmap_init(configs.lattice(n=100, n_mom=3))   # 80 KB per component
     S, fs, solver, T = setup_gpu(par)
     regs = []
     try:
