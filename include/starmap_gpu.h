@@ -153,8 +153,9 @@ int smg_set_time(smg_handle* h, double t);
  * every step of smg_run the library writes Q_comp = expr at each point of the
  * component's grid, at the step's t - dt/2 (starmap_solver.m:276-282), then
  * runs the step; such runs are not fused across steps and use no CUDA graph.
- * `expr` is a C++ expression (compiled with NVRTC for sm_100a at the next
- * smg_run; trusted input only) in x, y, z, t and k: the point's coordinates
+ * `expr` is an arithmetic expression in C++ syntax (compiled with NVRTC for
+ * sm_100a at the next smg_run; see smg_check_expr for what it may contain)
+ * in x, y, z, t and k: the point's coordinates
  * in the three solver dimensions, the time and the 1-based component number
  * -- the arguments of the reference's source hook after starmap_init.
  * x/y/z hold the coordinates of the component's grid along each solver
@@ -164,6 +165,24 @@ int smg_set_time(smg_handle* h, double t);
  * device-evaluable form of that hook. */
 int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const double* x, const double* y,
                         const double* z);
+
+/* Kinds of device expressions, for smg_check_expr. */
+#define SMG_EXPR_SOURCE   0   /* variables x, y, z, t, k */
+#define SMG_EXPR_MATERIAL 1   /* variables x, y, z, t, m */
+#define SMG_EXPR_FILTER   2   /* variables x, y, z, t, dt, k */
+
+/* SMG_OK when `expr` is a valid device expression of `kind`, else SMG_EINVAL
+ * with the reason in smg_last_error(NULL).  Device expressions are spliced
+ * into generated kernels, so they are held to a grammar that cannot reach
+ * memory or leave the expression: decimal or hexadecimal numbers, the kind's
+ * variables, the math functions sin cos tan asin acos atan atan2 sinh cosh
+ * tanh asinh acosh atanh exp exp2 exp10 expm1 log log2 log10 log1p pow sqrt
+ * rsqrt cbrt hypot fabs abs fmin fmax min max fmod remainder floor ceil round
+ * rint trunc copysign erf erfc tgamma lgamma sinpi cospi fdim nearbyint,
+ * true, false, the operators + - * / % < > <= >= == != && || ! ?: and
+ * parentheses and commas.  smg_set_source_expr, smg_set_material_expr and
+ * smg_set_filter_expr refuse anything else with SMG_EINVAL. */
+int smg_check_expr(int32_t kind, const char* expr);
 
 /* Time-dependent materials evaluated on the device: before every step of
  * smg_run the library evaluates sigma_a, sigma_s0 and (expr_sm non-NULL)

@@ -45,6 +45,9 @@ SMG_TUNE_ADJ_PRIORITY = 20
 SMG_TUNE_DIRECT_XFER = 21
 SMG_TUNE_JIT_LANES = 22
 
+# smg_check_expr kinds
+SMG_EXPR_SOURCE, SMG_EXPR_MATERIAL, SMG_EXPR_FILTER = 0, 1, 2
+
 SMG_VARIANT_AUTO = 0
 SMG_VARIANT_GENERIC = 1
 SMG_VARIANT_STRIP = 2
@@ -103,6 +106,7 @@ SIGNATURES = {
     "smg_set_material_expr": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int32,
                                         C.POINTER(C.c_int32), C.c_int32, C.c_int32,
                                         C.POINTER(C.POINTER(C.c_double))]),
+    "smg_check_expr": (C.c_int, [C.c_int32, C.c_char_p]),
     "smg_set_source_expr": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "smg_run": (C.c_int, [C.c_void_p, C.c_int64]),

@@ -8,11 +8,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <new>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -614,6 +616,80 @@ void reciprocals(smg_handle* h) {
     }
 }
 
+// Expressions evaluated on the device are spliced into generated kernels, so
+// they are held to a small grammar that cannot reach memory or leave the
+// expression: numbers, the variables of the expression's kind, the math
+// functions below, + - * / % < > <= >= == != && || ! ?: ( ) and commas.  No
+// brackets, braces, semicolons, assignments, address or pointer syntax, type
+// names or string/char literals.  Returns "" when the expression is
+// acceptable, else why not.
+std::string expr_problem(const char* expr, int kind) {
+    static const std::set<std::string> fns = {
+        "sin",   "cos",   "tan",   "asin",  "acos",     "atan",      "atan2", "sinh",  "cosh",   "tanh",
+        "asinh", "acosh", "atanh", "exp",   "exp2",     "exp10",     "expm1", "log",   "log2",   "log10",
+        "log1p", "pow",   "sqrt",  "rsqrt", "cbrt",     "hypot",     "fabs",  "abs",   "fmin",   "fmax",
+        "min",   "max",   "fmod",  "remainder", "floor", "ceil",     "round", "rint",  "trunc",  "copysign",
+        "erf",   "erfc",  "tgamma", "lgamma", "sinpi",  "cospi",     "fdim",  "nearbyint", "true", "false"};
+    static const char* vars[3][6] = {{"x", "y", "z", "t", "k", nullptr},
+                                     {"x", "y", "z", "t", "m", nullptr},
+                                     {"x", "y", "z", "t", "dt", "k"}};
+    if (kind < 0 || kind > 2) return "unknown expression kind";
+    if (!expr) return "NULL expression";
+    const size_t n = std::strlen(expr);
+    if (n == 0 || n > 65536) return "expression empty or over 64 KB";
+    auto is_var = [&](const std::string& w) {
+        for (const char* v : vars[kind])
+            if (v && w == v) return true;
+        return false;
+    };
+    int depth = 0;
+    for (size_t i = 0; i < n;) {
+        const unsigned char c = (unsigned char)expr[i];
+        if (std::isspace(c)) {
+            ++i;
+        } else if (std::isdigit(c) || (c == '.' && i + 1 < n && std::isdigit((unsigned char)expr[i + 1]))) {
+            // a decimal or hexadecimal floating literal with an optional exponent and suffix
+            size_t j = i + 1;
+            const bool hex = c == '0' && j < n && (expr[j] == 'x' || expr[j] == 'X');
+            if (hex) ++j;
+            while (j < n) {
+                const char d = expr[j];
+                const bool expo = hex ? (d == 'p' || d == 'P') : (d == 'e' || d == 'E');
+                if (expo && j + 1 < n && (expr[j + 1] == '+' || expr[j + 1] == '-')) j += 2;
+                else if (std::isxdigit((unsigned char)d) || d == '.' || expo) ++j;
+                else break;
+            }
+            while (j < n && std::strchr("fFlLuU", expr[j])) ++j;
+            if (j < n && (std::isalnum((unsigned char)expr[j]) || expr[j] == '_'))
+                return "malformed number at offset " + std::to_string(i);
+            i = j;
+        } else if (std::isalpha(c) || c == '_') {
+            size_t j = i;
+            while (j < n && (std::isalnum((unsigned char)expr[j]) || expr[j] == '_')) ++j;
+            const std::string w(expr + i, j - i);
+            if (!is_var(w) && !fns.count(w))
+                return "'" + w + "' is neither a variable of this expression nor an allowed math function";
+            i = j;
+        } else {
+            static const char* ops2[] = {"<=", ">=", "==", "!=", "&&", "||"};
+            bool two = false;
+            for (const char* o : ops2)
+                if (i + 1 < n && expr[i] == o[0] && expr[i + 1] == o[1]) two = true;
+            if (two) {
+                i += 2;
+            } else if (std::strchr("+-*/%<>!?:(),", c)) {
+                if (c == '(') ++depth;
+                if (c == ')' && --depth < 0) return "unbalanced ')' at offset " + std::to_string(i);
+                ++i;
+            } else {
+                return std::string("character '") + (char)c + "' at offset " + std::to_string(i) + " is not allowed";
+            }
+        }
+    }
+    if (depth != 0) return "unbalanced parentheses";
+    return "";
+}
+
 bool strip_usable(const smg_handle* h) {
     return h->sched[0].ok && h->sched[1].ok && h->variant != SMG_VARIANT_GENERIC;
 }
@@ -720,6 +796,14 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
                 }
     for (int j = 0; j < n_sys; ++j)
         for (int d = 0; d < 3; ++d) gt_out[3 * j + d] = 1 + ((cls[j] >> d) & 1);
+    return SMG_OK;
+    SMG_CATCH(nullptr)
+}
+
+int smg_check_expr(int32_t kind, const char* expr) {
+    SMG_TRY
+    const std::string why = expr_problem(expr, kind);
+    if (!why.empty()) return fail(nullptr, SMG_EINVAL, "smg_check_expr: " + why);
     return SMG_OK;
     SMG_CATCH(nullptr)
 }
@@ -1152,9 +1236,11 @@ int smg_set_material_expr(smg_handle* h, const char* expr_a, const char* expr_s0
     if (!expr_a) return SMG_OK;   // back to uploaded values
     if (!expr_s0 || nrows < 0 || (nrows > 0 && !rows) || !coords)
         return fail(h, SMG_EINVAL, "smg_set_material_expr: NULL argument");
-    for (const char* e : {expr_a, expr_s0, expr_sm})
-        if (e && (std::strlen(e) == 0 || std::strlen(e) > 65536))
-            return fail(h, SMG_EINVAL, "smg_set_material_expr: expression empty or over 64 KB");
+    for (const char* e : {expr_a, expr_s0, expr_sm}) {
+        if (!e) continue;
+        const std::string why = expr_problem(e, SMG_EXPR_MATERIAL);
+        if (!why.empty()) return fail(h, SMG_EINVAL, "smg_set_material_expr: " + why);
+    }
     smg_handle::MatExpr M;
     for (int r = 0; r < nrows; ++r) {
         if (!array_field(h, rows[3 * r]) || !array_field(h, rows[3 * r + 1]))
@@ -1188,8 +1274,10 @@ int smg_set_filter_expr(smg_handle* h, const char* expr, int32_t nrows, const in
     h->filt = smg_handle::FiltExpr{};
     if (!expr) return SMG_OK;   // back to uploaded values
     if (nrows < 1 || !rows || !coords) return fail(h, SMG_EINVAL, "smg_set_filter_expr: NULL argument or no rows");
-    if (std::strlen(expr) == 0 || std::strlen(expr) > 65536)
-        return fail(h, SMG_EINVAL, "smg_set_filter_expr: expression empty or over 64 KB");
+    {
+        const std::string why = expr_problem(expr, SMG_EXPR_FILTER);
+        if (!why.empty()) return fail(h, SMG_EINVAL, "smg_set_filter_expr: " + why);
+    }
     smg_handle::FiltExpr F;
     F.expr = expr;
     for (int r = 0; r < nrows; ++r) {
@@ -1231,8 +1319,10 @@ int smg_set_source_expr(smg_handle* h, int32_t comp, const char* expr, const dou
         if (j != comp && h->comps[j].Q == f)
             return fail(h, SMG_EINVAL, "smg_set_source_expr: the source field is shared with another component");
     if (!x || !y || !z) return fail(h, SMG_EINVAL, "smg_set_source_expr: NULL coordinate vector");
-    const size_t len = std::strlen(expr);
-    if (len == 0 || len > 65536) return fail(h, SMG_EINVAL, "smg_set_source_expr: expression empty or over 64 KB");
+    {
+        const std::string why = expr_problem(expr, SMG_EXPR_SOURCE);
+        if (!why.empty()) return fail(h, SMG_EINVAL, "smg_set_source_expr: " + why);
+    }
     // coordinates of the component's grid per kernel axis, from the
     // per-solver-dimension vectors
     const int* E = h->comps[comp].ext;

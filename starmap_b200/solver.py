@@ -20,6 +20,7 @@ interpolating linearly in time as the reference does (:425-473).
 from __future__ import annotations
 
 import math
+import re
 import time
 
 import numpy as np
@@ -824,17 +825,30 @@ def td_schedule(dt_hyp: float, tfinal: float, cn: float):
     return ts, dts
 
 
+_IDENT = re.compile(r"(?<![\w.])[A-Za-z_]\w*")
+
+
 def device_source_expr(expr: str, dim: int) -> str:
-    """The user's source expression, written in the variables of the user's
+    """The user's device expression, written in the variables of the user's
     own hook (x, y, t, k in 2D; x, y, z, t, k in 3D; x, t, k in 1D), as an
-    expression in the solver dimensions that ``smg_set_source_expr`` takes:
-    in 2D the user's (x, y) are the solver's second and third dimensions, in
-    1D the user's x is the third (the wrapping of starmap_init.m)."""
+    expression in the solver dimensions that ``smg_set_source_expr`` and the
+    other device-expression calls take: in 2D the user's (x, y) are the
+    solver's second and third dimensions, in 1D the user's x is the third
+    (the wrapping of starmap_init.m).  The variables are renamed token by
+    token (identifiers inside numbers such as 1e5 or 0x1p-3 are not
+    tokens); a variable the user's hook does not have is refused."""
     if dim == 3:
         return "(" + expr + ")"
-    if dim == 2:
-        return "[&](double x, double y) { return (double)(" + expr + "); }(y, z)"
-    return "[&](double x) { return (double)(" + expr + "); }(z)"
+    ren = {"x": "y", "y": "z"} if dim == 2 else {"x": "z"}
+    absent = {"z"} if dim == 2 else {"y", "z"}
+
+    def sub(m):
+        w = m.group(0)
+        if w in absent:
+            raise ValueError(f"device expression {expr!r}: '{w}' is not a variable of a {dim}D problem")
+        return ren.get(w, w)
+
+    return "(" + _IDENT.sub(sub, expr) + ")"
 
 
 def _call_output(S, outfn, par, Uplot, step):
