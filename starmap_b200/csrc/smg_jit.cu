@@ -2602,24 +2602,40 @@ std::string cache_file(const std::string& key) {
     return d + name;
 }
 
-bool cache_load(const std::string& key, std::vector<std::vector<char>>& out) {
+// File format: "SMGCUB2\n", the key's length and bytes (the whole source
+// with the options, compared in full on load: a file is used only for
+// exactly its own key), the number of cubins, each cubin's size and bytes,
+// and a checksum over the cubins.  A file that does not hold `count` cubins
+// or whose checksum differs (truncated, corrupted) is ignored.
+unsigned long long cubins_checksum(const std::vector<std::vector<char>>& v) {
+    unsigned long long h = 0x6a09e667f3bcc909ull;
+    for (const auto& c : v) h = bytes_hash(c, h ^ c.size(), 0x9e3779b97f4a7c15ull);
+    return h;
+}
+
+bool cache_load(const std::string& key, size_t count, std::vector<std::vector<char>>& out) {
     const std::string f = cache_file(key);
     if (f.empty()) return false;
     FILE* fp = std::fopen(f.c_str(), "rb");
     if (!fp) return false;
     char magic[8] = {0};
-    unsigned long long klen = 0, n = 0;
-    bool ok = std::fread(magic, 1, 8, fp) == 8 && std::memcmp(magic, "SMGCUB1\n", 8) == 0 &&
-              std::fread(&klen, sizeof klen, 1, fp) == 1 && klen == key.size() && std::fread(&n, sizeof n, 1, fp) == 1 &&
-              n < (1u << 16);
+    unsigned long long klen = 0, n = 0, sum = 0;
+    bool ok = std::fread(magic, 1, 8, fp) == 8 && std::memcmp(magic, "SMGCUB2\n", 8) == 0 &&
+              std::fread(&klen, sizeof klen, 1, fp) == 1 && klen == key.size();
+    if (ok) {
+        std::string k(key.size(), '\0');
+        ok = std::fread(&k[0], 1, k.size(), fp) == k.size() && k == key;
+    }
+    ok = ok && std::fread(&n, sizeof n, 1, fp) == 1 && n == count;
     std::vector<std::vector<char>> v;
     for (unsigned long long i = 0; ok && i < n; ++i) {
         unsigned long long sz = 0;
-        ok = std::fread(&sz, sizeof sz, 1, fp) == 1 && sz < (1ull << 31);
+        ok = std::fread(&sz, sizeof sz, 1, fp) == 1 && sz > 0 && sz < (1ull << 31);
         if (!ok) break;
         v.emplace_back(sz);
         ok = std::fread(v.back().data(), 1, sz, fp) == sz;
     }
+    ok = ok && std::fread(&sum, sizeof sum, 1, fp) == 1 && sum == cubins_checksum(v);
     std::fclose(fp);
     if (!ok) return false;
     out = std::move(v);
@@ -2632,13 +2648,14 @@ void cache_store(const std::string& key, const std::vector<std::vector<char>>& c
     const std::string tmp = f + "." + std::to_string((long long)getpid()) + ".tmp";
     FILE* fp = std::fopen(tmp.c_str(), "wb");
     if (!fp) return;
-    const unsigned long long klen = key.size(), n = cub.size();
-    bool ok = std::fwrite("SMGCUB1\n", 1, 8, fp) == 8 && std::fwrite(&klen, sizeof klen, 1, fp) == 1 &&
-              std::fwrite(&n, sizeof n, 1, fp) == 1;
+    const unsigned long long klen = key.size(), n = cub.size(), sum = cubins_checksum(cub);
+    bool ok = std::fwrite("SMGCUB2\n", 1, 8, fp) == 8 && std::fwrite(&klen, sizeof klen, 1, fp) == 1 &&
+              std::fwrite(key.data(), 1, key.size(), fp) == key.size() && std::fwrite(&n, sizeof n, 1, fp) == 1;
     for (const auto& c : cub) {
         const unsigned long long sz = c.size();
         ok = ok && std::fwrite(&sz, sizeof sz, 1, fp) == 1 && std::fwrite(c.data(), 1, sz, fp) == sz;
     }
+    ok = ok && std::fwrite(&sum, sizeof sum, 1, fp) == 1;
     ok = std::fclose(fp) == 0 && ok;
     if (ok) ok = std::rename(tmp.c_str(), f.c_str()) == 0;
     if (!ok) std::remove(tmp.c_str());
@@ -2665,7 +2682,8 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
             return SMG_OK;
         }
     }
-    if (a.ok && cache_load(key, out)) {
+    const bool link = calls && P.size() > 1;
+    if (a.ok && cache_load(key, link ? 1 : P.size(), out)) {
         g_programs_from_disk += (long long)P.size();
         std::lock_guard<std::mutex> lk(g_cubin_mu);
         g_cubins[key] = out;
@@ -2675,7 +2693,6 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
         err = a.why;
         return SMG_EINVAL;
     }
-    const bool link = calls && P.size() > 1;
     if (link && !a.link_ok) {
         err = a.link_why;
         return SMG_EINVAL;

@@ -156,8 +156,8 @@ print(json.dumps([c.value, d.value]))
 
 def test_compiled_kernels_are_cached_on_disk_across_processes():
     """A second process generating the same problem's kernels loads them from
-    the on-disk cache instead of compiling (smg_jit_stats); SMG_JIT_CACHE=0
-    compiles again and writes nothing."""
+    the on-disk cache instead of compiling (smg_jit_stats); a damaged cache
+    file is not used; SMG_JIT_CACHE=0 compiles again and writes nothing."""
     import json
     import os
     import shutil
@@ -183,6 +183,18 @@ def test_compiled_kernels_are_cached_on_disk_across_processes():
         assert len([f for f in os.listdir(d) if f.endswith(".cubins")]) == 1
         compiled, from_disk = run()
         assert compiled == 0 and from_disk > 0
+        # a damaged file (one cubin byte flipped, or cut short) is ignored,
+        # compiled again and rewritten
+        f = os.path.join(d, [f for f in os.listdir(d) if f.endswith(".cubins")][0])
+        good = open(f, "rb").read()
+        assert good.startswith(b"SMGCUB2\n")
+        bad = bytearray(good)
+        bad[-100] ^= 0x40
+        for damaged in (bytes(bad), good[:-9]):
+            open(f, "wb").write(damaged)
+            compiled, from_disk = run()
+            assert compiled > 0 and from_disk == 0
+            assert open(f, "rb").read() == good
         shutil.rmtree(d)
         compiled, from_disk = run(SMG_JIT_CACHE="0")
         assert compiled > 0 and from_disk == 0 and not os.path.exists(d)
