@@ -104,6 +104,13 @@ void free_device(smg_handle* h) {
     h->dDest = h->dFlag = nullptr;
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    for (cudaEvent_t* ev : {&h->xev_fork, &h->xev_join, &h->xev_full[0], &h->xev_full[1], &h->xev_free[0],
+                            &h->xev_free[1]}) {
+        if (*ev) cudaEventDestroy(*ev);
+        *ev = nullptr;
+    }
+    if (h->xstream) cudaStreamDestroy(h->xstream);
+    h->xstream = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
     h->ev0 = h->ev1 = nullptr;
     h->stream = nullptr;
@@ -148,15 +155,15 @@ __global__ void k_xfer(XferChunk c, double* __restrict__ stage, double* __restri
     }
 }
 
-cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, bool to_slots, const double* snap = nullptr,
-                        double wa = 0.0, double wb = 0.0) {
+cudaError_t xfer_launch(const smg_handle* h, const XferChunk& c, double* stage, bool to_slots,
+                        const double* snap = nullptr, double wa = 0.0, double wb = 0.0) {
     int e0max = 1, rows_max = 1;
     for (int k = 0; k < c.n; ++k) {
         e0max = std::max(e0max, c.e0[k]);
         rows_max = std::max(rows_max, c.rows[k]);
     }
     dim3 grid((unsigned)((e0max + 127) / 128), (unsigned)std::min(rows_max, 4096), (unsigned)c.n);
-    k_xfer<<<grid, 128, 0, h->stream>>>(c, h->dStage, h->dU, snap, wa, wb, h->g.s1, h->g.s2, to_slots ? 1 : 0);
+    k_xfer<<<grid, 128, 0, h->stream>>>(c, stage, h->dU, snap, wa, wb, h->g.s1, h->g.s2, to_slots ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -256,48 +263,111 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
     if (h->direct_xfer) {
         std::vector<double*> hp(h->n_sys, nullptr);
         bool direct = true;
+        int arrays = 0, runs = 0;
+        const char* end = nullptr;
         for (int j = 0; j < h->n_sys && direct; ++j) {
             const void* p = upload ? (const void*)Uin[j] : (const void*)Uout[j];
             if (!p) continue;
             const int* e = h->comps[j].ext;
-            hp[j] = device_view(p, (size_t)e[0] * e[1] * e[2] * sizeof(double));
+            const size_t bytes = (size_t)e[0] * e[1] * e[2] * sizeof(double);
+            hp[j] = device_view(p, bytes);
             direct = hp[j] != nullptr;
+            ++arrays;
+            if (static_cast<const char*>(p) != end) ++runs;
+            end = static_cast<const char*>(p) + bytes;
         }
-        if (direct) return direct_transfer(h, upload, hp, snap, wa, wb);
+        // page-locked arrays carved in order from one host block (a few
+        // contiguous runs) move faster by large copy-engine copies through
+        // the staging buffer (about 43 against 37 GB/s measured), separate
+        // arrays faster in place
+        if (direct && runs * 8 > arrays) return direct_transfer(h, upload, hp, snap, wa, wb);
     }
+    // Staged form.  The pieces of a chunk are packed into one half of the
+    // staging buffer while the other half is scattered into the slots
+    // (upload) or copied out to the host (download): the linear copies run on
+    // a copy stream, the kernels on the handle's stream, and events pass each
+    // half between the two, so the copy engine runs back to back.  Pieces
+    // whose host bytes follow each other (component arrays carved in order
+    // from one host block) are moved by one copy.  A problem whose rows do
+    // not fit half the buffer uses it whole, one chunk at a time.
+    if (!h->xstream) {
+        SMG_CUDA(h, cudaStreamCreateWithFlags(&h->xstream, cudaStreamNonBlocking));
+        for (cudaEvent_t* ev : {&h->xev_fork, &h->xev_join, &h->xev_full[0], &h->xev_full[1], &h->xev_free[0],
+                                &h->xev_free[1]})
+            SMG_CUDA(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    }
+    size_t row_max = 0;
+    for (int j = 0; j < h->n_sys; ++j)
+        if (upload ? Uin[j] : Uout[j]) row_max = std::max(row_max, (size_t)h->comps[j].ext[0] * 8);
+    const size_t half = h->stage_bytes / 2 / 256 * 256;
+    const int nbuf = half >= row_max && half > 0 ? 2 : 1;
+    const size_t cap = nbuf == 2 ? half : h->stage_bytes;
+    if (row_max > cap) return fail(h, SMG_EINVAL, "state transfer: a row exceeds the staging buffer");
+    auto base = [&](int b) { return reinterpret_cast<char*>(h->dStage) + (size_t)b * cap; };
+    // the copy stream starts after all work queued on the handle's stream
+    SMG_CUDA(h, cudaEventRecord(h->xev_fork, h->stream));
+    SMG_CUDA(h, cudaStreamWaitEvent(h->xstream, h->xev_fork, 0));
+    int buf = 0;
     XferChunk c;
     c.n = 0;
     size_t used = 0;
-    struct Piece { int j; size_t host_off, stage_off, bytes; };
+    struct Piece { char* host; size_t stage_off, bytes; };
     std::vector<Piece> pend;
+    // the chunk's linear copies, host-adjacent pieces merged (they are
+    // adjacent in the stage too)
+    auto copies = [&]() -> cudaError_t {
+        for (size_t i = 0; i < pend.size();) {
+            size_t k = i + 1, bytes = pend[i].bytes;
+            while (k < pend.size() && pend[k].host == pend[i].host + bytes) bytes += pend[k++].bytes;
+            const cudaError_t e =
+                upload ? cudaMemcpyAsync(base(buf) + pend[i].stage_off, pend[i].host, bytes, cudaMemcpyHostToDevice,
+                                         h->xstream)
+                       : cudaMemcpyAsync(pend[i].host, base(buf) + pend[i].stage_off, bytes, cudaMemcpyDeviceToHost,
+                                         h->xstream);
+            if (e != cudaSuccess) return e;
+            i = k;
+        }
+        return cudaSuccess;
+    };
     auto flush = [&]() -> cudaError_t {
+        if (!c.n) return cudaSuccess;
         cudaError_t e = cudaSuccess;
-        if (c.n) e = xfer_launch(h, c, upload, snap, wa, wb);
-        if (!upload)
-            for (size_t i = 0; i < pend.size() && e == cudaSuccess; ++i)
-                e = cudaMemcpyAsync(reinterpret_cast<char*>(Uout[pend[i].j]) + pend[i].host_off,
-                                    reinterpret_cast<const char*>(h->dStage) + pend[i].stage_off, pend[i].bytes,
-                                    cudaMemcpyDeviceToHost, h->stream);
+        double* stage = reinterpret_cast<double*>(base(buf));
+        if (upload) {
+            // copy into the half once its previous scatter is done, then scatter it
+            if ((e = cudaStreamWaitEvent(h->xstream, h->xev_free[buf], 0)) != cudaSuccess ||
+                (e = copies()) != cudaSuccess || (e = cudaEventRecord(h->xev_full[buf], h->xstream)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(h->stream, h->xev_full[buf], 0)) != cudaSuccess ||
+                (e = xfer_launch(h, c, stage, true)) != cudaSuccess ||
+                (e = cudaEventRecord(h->xev_free[buf], h->stream)) != cudaSuccess)
+                return e;
+        } else {
+            // gather into the half once its previous copies out are done, then copy it out
+            if ((e = cudaStreamWaitEvent(h->stream, h->xev_free[buf], 0)) != cudaSuccess ||
+                (e = xfer_launch(h, c, stage, false, snap, wa, wb)) != cudaSuccess ||
+                (e = cudaEventRecord(h->xev_full[buf], h->stream)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(h->xstream, h->xev_full[buf], 0)) != cudaSuccess ||
+                (e = copies()) != cudaSuccess || (e = cudaEventRecord(h->xev_free[buf], h->xstream)) != cudaSuccess)
+                return e;
+        }
         c.n = 0;
         used = 0;
         pend.clear();
-        return e;
+        buf = (buf + 1) % nbuf;
+        return cudaSuccess;
     };
     for (int j = 0; j < h->n_sys; ++j) {
-        if (upload ? !Uin[j] : !Uout[j]) continue;
+        char* host = upload ? const_cast<char*>(reinterpret_cast<const char*>(Uin[j]))
+                            : reinterpret_cast<char*>(Uout[j]);
+        if (!host) continue;
         const int* e = h->comps[j].ext;
         const size_t row_bytes = (size_t)e[0] * 8;
         const int rows = e[1] * e[2];
-        const int max_rows = (int)std::max<size_t>(1, h->stage_bytes / row_bytes);
-        if (row_bytes > h->stage_bytes) return fail(h, SMG_EINVAL, "state transfer: a row exceeds the staging buffer");
+        const int max_rows = (int)std::max<size_t>(1, cap / row_bytes);
         for (int r0 = 0; r0 < rows; r0 += max_rows) {
             const int nr = std::min(max_rows, rows - r0);
             const size_t bytes = (size_t)nr * row_bytes;
-            if (c.n == kXferMax || used + bytes > h->stage_bytes) SMG_CUDA(h, flush());
-            if (upload)
-                SMG_CUDA(h, cudaMemcpyAsync(reinterpret_cast<char*>(h->dStage) + used,
-                                            reinterpret_cast<const char*>(Uin[j]) + (size_t)r0 * row_bytes, bytes,
-                                            cudaMemcpyHostToDevice, h->stream));
+            if (c.n == kXferMax || used + bytes > cap) SMG_CUDA(h, flush());
             c.e0[c.n] = e[0];
             c.e1[c.n] = e[1];
             c.row0[c.n] = r0;
@@ -305,11 +375,14 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
             c.stage_off[c.n] = (long long)(used / 8);
             c.slot_off[c.n] = (long long)j * h->g.cs;
             ++c.n;
-            if (!upload) pend.push_back({j, (size_t)r0 * row_bytes, used, bytes});
-            used += (bytes + 255) / 256 * 256;
+            pend.push_back({host + (size_t)r0 * row_bytes, used, bytes});
+            used += bytes;
         }
     }
     SMG_CUDA(h, flush());
+    // everything of this transfer is ordered before later work on the handle's stream
+    SMG_CUDA(h, cudaEventRecord(h->xev_join, h->xstream));
+    SMG_CUDA(h, cudaStreamWaitEvent(h->stream, h->xev_join, 0));
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
     return SMG_OK;
 }

@@ -69,6 +69,11 @@ struct smg_handle {
     // run state
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // staged transfers: copy stream and the events that pass the two halves
+    // of the staging buffer between it and `stream` (created on first use)
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t xev_fork = nullptr, xev_join = nullptr, xev_full[2] = {nullptr, nullptr},
+                xev_free[2] = {nullptr, nullptr};
     double dt = 0.0, hdt = 0.0;
     bool dt_set = false, state_set = false;
     double last_ms = 0.0;
