@@ -273,8 +273,11 @@ int smg_jit_stats(int64_t* compiled, int64_t* from_disk);
 #define SMG_TUNE_ADJ_FUSED   5   /* smg_backward: 1 = one fused kernel per phase (default), 0 = pointwise + transpose kernels */
 #define SMG_TUNE_JIT_LANES   22  /* generated kernels of one phase that run at the same time: 0 (default) all of
                                     them, n >= 1 at most n (kernel i follows kernel i - n on its stream) */
-#define SMG_TUNE_DIRECT_XFER 21  /* state transfers: 1 (default) page-locked host arrays are read / written in place by
-                                    one kernel per 64 components, 0 always through the device staging buffer */
+#define SMG_TUNE_DIRECT_XFER 21  /* state transfers: 1 (default) separate page-locked host arrays are read / written
+                                    in place by one kernel per 64 components, while arrays carved in order from one
+                                    page-locked block (at most one contiguous run per eight arrays) and pageable
+                                    ones go through the double-buffered device staging buffer, host-adjacent pieces
+                                    in one copy; 0 always through the staging buffer */
 #define SMG_TUNE_ADJ_PRIORITY 20 /* smg_backward stream priorities, set before smg_forward: 0 (default) recompute and
                                     sweep at the default priority, 1 recompute at the device's highest priority, 2
                                     the sweep on a stream of the highest priority above the recompute */
