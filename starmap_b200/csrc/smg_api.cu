@@ -829,11 +829,14 @@ int smg_classify(int32_t n_sys, const double* Mx, const double* My, const double
     const double* M[3] = {Mx, My, Mz};
     // I[d][j]: sorted columns i with M_d(j,i) != 0 (starmap_solver.m:77-79)
     std::vector<std::vector<int>> I[3];
+    // (one pass in memory order: column i outer, so each row's list ascends)
     for (int d = 0; d < 3; ++d) {
         I[d].resize(n_sys);
-        for (int j = 0; j < n_sys; ++j)
-            for (int i = 0; i < n_sys; ++i)
-                if (M[d][j + (size_t)i * n_sys] != 0.0) I[d][j].push_back(i);
+        for (int i = 0; i < n_sys; ++i) {
+            const double* col = M[d] + (size_t)i * n_sys;
+            for (int j = 0; j < n_sys; ++j)
+                if (col[j] != 0.0) I[d][j].push_back(i);
+        }
     }
     // class index = (gx-1) + 2(gy-1) + 4(gz-1); membership flags
     std::vector<int> cls(n_sys, -1);
@@ -989,17 +992,29 @@ int create_impl(const smg_problem* p, smg_handle** out, bool device) {
         }
     }
 
-    // components and couplings in sumcell order
+    // components and couplings in sumcell order.  The nonzeros of every row
+    // are collected in one pass over each column-major matrix in memory order
+    // (column i outer, so each row's list ascends in i); a row-by-row scan
+    // strides by n_sys doubles and costs milliseconds for hundreds of moments.
     h->comps.resize(ns);
     const double* M[3] = {p->Mx, p->My, p->Mz};
+    std::vector<std::vector<std::pair<int, double>>> rownz[3];
+    for (int d = 0; d < 3; ++d) {
+        rownz[d].resize(ns);
+        for (int i = 0; i < ns; ++i) {
+            const double* col = M[d] + (size_t)i * ns;
+            for (int j = 0; j < ns; ++j)
+                if (col[j] != 0.0) rownz[d][j].push_back({i, col[j]});
+        }
+    }
     for (int j = 0; j < ns; ++j) {
         DevComp& c = h->comps[j];
         grid_extents(h, &p->gt[3 * j], c.ext);
         c.cbeg = (int)h->coups.size();
         for (int d = 0; d < 3; ++d) {
-            for (int i = 0; i < ns; ++i) {
-                const double w = M[d][j + (size_t)i * ns];
-                if (w == 0.0) continue;
+            for (const auto& iw : rownz[d][j]) {
+                const int i = iw.first;
+                const double w = iw.second;
                 const int gi = p->gt[3 * i + d];
                 // the staggered difference of component i along d lives on the
                 // grid of i with axis d flipped; MATLAB adds it elementwise to
