@@ -412,7 +412,8 @@ def prepare(par: dict) -> _Setup:
     """Host-side setup of starmap_solver.m:55-157 (no GPU work)."""
     S = _Setup()
     par = dict(par)
-    Mx, My, Mz = (np.asarray(par[k], dtype=np.float64) for k in ("Mx", "My", "Mz"))
+    # the coupling matrices in the C ABI's column-major layout (MATLAB's), once
+    Mx, My, Mz = (np.asfortranarray(np.asarray(par[k], dtype=np.float64)) for k in ("Mx", "My", "Mz"))
     n_sys = Mz.shape[0]
     flag_filter = ("filterfunction" in par) and ("f_position" in par) and ("mom_order" in par)
     f_mom_order = np.atleast_1d(np.asarray(par["mom_order"])).astype(int) if "mom_order" in par else None
@@ -551,6 +552,10 @@ class _Tables:
         self.index = {}
 
     def add(self, key, val, grid):
+        # arrays in the C ABI's column-major layout once, here, rather than
+        # at every handle creation
+        if np.ndim(val) > 0:
+            val = np.asfortranarray(np.asarray(val, dtype=np.float64))
         self.index[key] = len(self.fields)
         self.fields.append((val, grid))
         return self.index[key]
