@@ -105,13 +105,29 @@ class GpuSolver:
     def grid_extents(self, grid):
         return tuple((self.n[d] + 1) if (grid[d] == 2 and self.bc[d] == 1) else self.n[d] for d in range(3))
 
+    def _extents_all(self):
+        ext = getattr(self, "_ext", None)
+        if ext is None:
+            ext = self._ext = [self.extents(j) for j in range(self.n_sys)]
+        return ext
+
     def set_state(self, U):
-        arrs = []
+        # arrays already in the ABI's layout (float64, column-major, of the
+        # component's extents) are passed as they are; others are converted.
+        # For hundreds of components the per-array Python work is
+        # milliseconds, so the common case is kept to a few attribute checks.
+        ext = self._extents_all()
+        ptrs = (_lib.C.c_void_p * self.n_sys)()
+        keep = []
         for j in range(self.n_sys):
-            a = np.broadcast_to(np.asarray(U[j], dtype=np.float64), self.extents(j))
-            arrs.append(np.ascontiguousarray(np.asfortranarray(a).ravel(order="F")))
-        ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)(*[dptr(a) for a in arrs])
-        check(self._L.smg_set_state(self.h, ptrs), self.h)
+            a = U[j]
+            if not (type(a) is np.ndarray and a.dtype == np.float64 and a.flags.f_contiguous and a.shape == ext[j]):
+                a = np.ascontiguousarray(np.asfortranarray(
+                    np.broadcast_to(np.asarray(a, dtype=np.float64), ext[j])).ravel(order="F"))
+                keep.append(a)
+            ptrs[j] = a.ctypes.data
+        check(self._L.smg_set_state(self.h, _lib.C.cast(ptrs, _lib.C.POINTER(_lib.C.POINTER(_lib.C.c_double)))),
+              self.h)
 
     def get_state(self, which=None, out=None):
         """Components ``which`` (default all) as arrays of their extents.  With
@@ -129,21 +145,26 @@ class GpuSolver:
         return self._download(lambda ptrs: self._L.smg_get_interp(self.h, float(lam), ptrs), which, out)
 
     def _download(self, call, which, out):
+        ext = self._extents_all()
         which = range(self.n_sys) if which is None else which
         res = {}
-        ptrs = (_lib.C.POINTER(_lib.C.c_double) * self.n_sys)()
+        ptrs = (_lib.C.c_void_p * self.n_sys)()
         for j in which:
-            e = self.extents(j)
+            e = ext[j]
+            size = e[0] * e[1] * e[2]
             if out is not None:
-                buf = out[j].reshape(-1, order="A")
-                if buf.dtype != np.float64 or buf.size != int(np.prod(e)) or not buf.flags.c_contiguous:
-                    raise ValueError(f"out[{j}] must be a contiguous float64 buffer of {int(np.prod(e))} values")
+                buf = out[j]
+                if not (type(buf) is np.ndarray and buf.dtype == np.float64 and buf.size == size
+                        and (buf.flags.c_contiguous if buf.ndim == 1 else buf.flags.f_contiguous)):
+                    buf = buf.reshape(-1, order="A")
+                    if buf.dtype != np.float64 or buf.size != size or not buf.flags.c_contiguous:
+                        raise ValueError(f"out[{j}] must be a contiguous float64 buffer of {size} values")
             else:
-                buf = np.empty(int(np.prod(e)), dtype=np.float64)
-            res[j] = (buf, e)
-            ptrs[j] = dptr(buf)
-        check(call(ptrs), self.h)
-        return {j: buf.reshape(e, order="F") for j, (buf, e) in res.items()}
+                buf = np.empty(size, dtype=np.float64)
+            res[j] = buf
+            ptrs[j] = buf.ctypes.data
+        check(call(_lib.C.cast(ptrs, _lib.C.POINTER(_lib.C.POINTER(_lib.C.c_double)))), self.h)
+        return {j: buf.reshape(ext[j], order="F") for j, buf in res.items()}
 
     def set_field(self, k, val):
         if np.ndim(val) == 0:
