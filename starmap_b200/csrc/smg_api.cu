@@ -196,24 +196,25 @@ __global__ void k_xfer_direct(XferDirect c, double* __restrict__ U, const double
     }
 }
 
-// the device address of a page-locked host array, or nullptr (pageable memory)
+// Device address of one page-locked host byte, or NULL (pageable memory).
+char* host_byte_view(const void* q) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+        cudaGetLastError();   // clear the error of an unregistered pointer
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<char*>(a.devicePointer) : nullptr;
+}
+
 // Device address of the page-locked host range [p, p + bytes), or NULL when
 // its first or last byte is not page-locked or the two are not mapped as one
 // contiguous range (an array only partly registered goes through staging:
 // the direct kernel must never touch an unmapped host page).
 double* device_view(const void* p, size_t bytes) {
-    auto view = [](const void* q) -> char* {
-        cudaPointerAttributes a{};
-        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
-            cudaGetLastError();   // clear the error of an unregistered pointer
-            return nullptr;
-        }
-        return a.type == cudaMemoryTypeHost ? static_cast<char*>(a.devicePointer) : nullptr;
-    };
     if (bytes == 0) return nullptr;
-    char* first = view(p);
+    char* first = host_byte_view(p);
     if (!first) return nullptr;
-    char* last = view(static_cast<const char*>(p) + (bytes - 1));
+    char* last = host_byte_view(static_cast<const char*>(p) + (bytes - 1));
     return last == first + (bytes - 1) ? reinterpret_cast<double*>(first) : nullptr;
 }
 
@@ -260,27 +261,41 @@ int direct_transfer(smg_handle* h, bool upload, const std::vector<double*>& hp, 
 // Page-locked host arrays go through direct_transfer instead.
 int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double* const* Uout,
                     const double* snap, double wa, double wb) {
-    if (h->direct_xfer) {
-        std::vector<double*> hp(h->n_sys, nullptr);
-        bool direct = true;
-        int arrays = 0, runs = 0;
-        const char* end = nullptr;
-        for (int j = 0; j < h->n_sys && direct; ++j) {
-            const void* p = upload ? (const void*)Uin[j] : (const void*)Uout[j];
-            if (!p) continue;
-            const int* e = h->comps[j].ext;
-            const size_t bytes = (size_t)e[0] * e[1] * e[2] * sizeof(double);
-            hp[j] = device_view(p, bytes);
-            direct = hp[j] != nullptr;
-            ++arrays;
-            if (static_cast<const char*>(p) != end) ++runs;
-            end = static_cast<const char*>(p) + bytes;
-        }
-        // page-locked arrays carved in order from one host block (a few
-        // contiguous runs) move faster by large copy-engine copies through
-        // the staging buffer (about 43 against 37 GB/s measured), separate
-        // arrays faster in place
-        if (direct && runs * 8 > arrays) return direct_transfer(h, upload, hp, snap, wa, wb);
+    // page-lock state of every host array: whole (its device address), none,
+    // or only in part (its first byte locked, the rest not all)
+    const int ns = h->n_sys;
+    std::vector<char*> host(ns, nullptr);
+    std::vector<double*> lockdev(ns, nullptr);
+    std::vector<char> partly(ns, 0);
+    std::vector<size_t> nbytes(ns, 0);
+    int arrays = 0, runs = 0, locked = 0;
+    const char* end = nullptr;
+    for (int j = 0; j < ns; ++j) {
+        host[j] = upload ? const_cast<char*>(reinterpret_cast<const char*>(Uin[j])) : reinterpret_cast<char*>(Uout[j]);
+        if (!host[j]) continue;
+        const int* e = h->comps[j].ext;
+        nbytes[j] = (size_t)e[0] * e[1] * e[2] * sizeof(double);
+        lockdev[j] = device_view(host[j], nbytes[j]);
+        partly[j] = !lockdev[j] && host_byte_view(host[j]) != nullptr;
+        ++arrays;
+        locked += lockdev[j] != nullptr;
+        if (host[j] != end) ++runs;
+        end = host[j] + nbytes[j];
+    }
+    // every array page-locked: in place, unless the arrays are carved in
+    // order from one host block (a few contiguous runs), which large
+    // copy-engine copies through the staging buffer move faster (about 43
+    // against 37 GB/s measured; separate arrays are faster in place)
+    if (h->direct_xfer && arrays > 0 && locked == arrays && runs * 8 > arrays)
+        return direct_transfer(h, upload, lockdev, snap, wa, wb);
+    // An array page-locked only in part cannot be the range of one copy (the
+    // driver takes the range for page-locked memory and refuses it past the
+    // registration): it goes through a pageable host bounce buffer.
+    std::vector<std::vector<double>> bounce(ns);
+    for (int j = 0; j < ns; ++j) {
+        if (!partly[j]) continue;
+        bounce[j].resize(nbytes[j] / sizeof(double));
+        if (upload) std::memcpy(bounce[j].data(), host[j], nbytes[j]);
     }
     // Staged form.  The pieces of a chunk are packed into one half of the
     // staging buffer while the other half is scattered into the slots
@@ -311,14 +326,20 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
     XferChunk c;
     c.n = 0;
     size_t used = 0;
-    struct Piece { char* host; size_t stage_off, bytes; };
+    // dev: the piece's device address when its array is page-locked whole
+    struct Piece { char* host; char* dev; size_t stage_off, bytes; };
     std::vector<Piece> pend;
     // the chunk's linear copies, host-adjacent pieces merged (they are
-    // adjacent in the stage too)
+    // adjacent in the stage too) while the merged range stays one kind of
+    // memory for the driver: a run that starts in pageable memory takes any
+    // adjacent piece; a page-locked run only pieces that continue its device
+    // mapping
     auto copies = [&]() -> cudaError_t {
         for (size_t i = 0; i < pend.size();) {
             size_t k = i + 1, bytes = pend[i].bytes;
-            while (k < pend.size() && pend[k].host == pend[i].host + bytes) bytes += pend[k++].bytes;
+            while (k < pend.size() && pend[k].host == pend[i].host + bytes &&
+                   (!pend[i].dev || pend[k].dev == pend[i].dev + bytes))
+                bytes += pend[k++].bytes;
             const cudaError_t e =
                 upload ? cudaMemcpyAsync(base(buf) + pend[i].stage_off, pend[i].host, bytes, cudaMemcpyHostToDevice,
                                          h->xstream)
@@ -356,10 +377,10 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
         buf = (buf + 1) % nbuf;
         return cudaSuccess;
     };
-    for (int j = 0; j < h->n_sys; ++j) {
-        char* host = upload ? const_cast<char*>(reinterpret_cast<const char*>(Uin[j]))
-                            : reinterpret_cast<char*>(Uout[j]);
-        if (!host) continue;
+    for (int j = 0; j < ns; ++j) {
+        if (!host[j]) continue;
+        char* src = partly[j] ? reinterpret_cast<char*>(bounce[j].data()) : host[j];
+        char* dev = reinterpret_cast<char*>(lockdev[j]);
         const int* e = h->comps[j].ext;
         const size_t row_bytes = (size_t)e[0] * 8;
         const int rows = e[1] * e[2];
@@ -375,7 +396,7 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
             c.stage_off[c.n] = (long long)(used / 8);
             c.slot_off[c.n] = (long long)j * h->g.cs;
             ++c.n;
-            pend.push_back({host + (size_t)r0 * row_bytes, used, bytes});
+            pend.push_back({src + (size_t)r0 * row_bytes, dev ? dev + (size_t)r0 * row_bytes : nullptr, used, bytes});
             used += bytes;
         }
     }
@@ -384,6 +405,9 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
     SMG_CUDA(h, cudaEventRecord(h->xev_join, h->xstream));
     SMG_CUDA(h, cudaStreamWaitEvent(h->stream, h->xev_join, 0));
     SMG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (!upload)
+        for (int j = 0; j < ns; ++j)
+            if (partly[j]) std::memcpy(host[j], bounce[j].data(), nbytes[j]);
     return SMG_OK;
 }
 
