@@ -51,7 +51,9 @@
 #include <cstring>
 #include <exception>
 #include <functional>
+#include <list>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -2807,6 +2809,87 @@ void jit_free(smg_handle* h) {
 namespace {
 
 // Generate, compile and load one form of the kernels (plain or recording).
+// Generated programs and their cubins per generator input, shared by the
+// handles of a process: a second handle of the same problem (a new
+// starmap_solver call, the instances of an ensemble) skips writing the
+// sources again (megabytes of text for hundreds of moments) and the lookup
+// of their cubins by source text.  The key holds every handle field the
+// generator reads, so equal keys give equal programs.  At most 8 entries,
+// the least recently used dropped.
+struct Built {
+    std::vector<KernelSrc> P;
+    std::vector<std::vector<char>> cubins;
+};
+std::mutex g_built_mu;
+std::list<std::pair<std::string, std::shared_ptr<const Built>>> g_built;   // most recent first
+constexpr size_t kBuiltMax = 8;
+static_assert(sizeof(smg::DevComp) == 11 * sizeof(int), "DevComp is all ints (serialised as bytes)");
+
+std::string generator_key(const smg_handle* h, int block, int group, int per, bool calls, bool rec) {
+    std::string k;
+    k.reserve(64 + h->comps.size() * 48 + h->coups.size() * 24);
+    auto put = [&](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    auto i64 = [&](long long v) { put(&v, sizeof v); };
+    auto f64 = [&](double v) { put(&v, sizeof v); };
+    for (long long v : {(long long)block, (long long)group, (long long)per, (long long)calls, (long long)rec,
+                        (long long)h->n_sys, (long long)h->filter_mode, (long long)h->field_one,
+                        (long long)h->field_zero, (long long)h->sigma_a, (long long)h->decay_a,
+                        (long long)h->derived_decay_a, (long long)h->jit_block, (long long)h->jit_group,
+                        (long long)h->jit_split, (long long)h->jit_calls, (long long)h->jit_xpair,
+                        (long long)h->jit_prefetch, (long long)h->jit_band, (long long)h->jit_const,
+                        (long long)h->jit_regs, (long long)h->jit_staged, (long long)h->jit_slices,
+                        (long long)h->jit_stages, (long long)h->jit_rows})
+        i64(v);
+    const smg::DevGrid& g = h->g;
+    for (int a = 0; a < 3; ++a) {
+        i64(g.n[a]);
+        i64(g.bc[a]);
+        i64(g.B[a]);
+        f64(g.h[a]);
+        f64(h->rh[a]);
+        i64(h->exact_recip[a]);
+    }
+    i64(g.s1);
+    i64(g.s2);
+    i64(g.cs);
+    i64((long long)h->comps.size());
+    put(h->comps.data(), h->comps.size() * sizeof(smg::DevComp));
+    i64((long long)h->coups.size());
+    for (const smg::DevCoup& c : h->coups) {
+        i64(c.src);
+        i64(c.code);
+        f64(c.w);
+    }
+    for (const std::vector<int>* v : {&h->destA, &h->destB, &h->derived_decay}) {
+        i64((long long)v->size());
+        for (int x : *v) i64(x);
+    }
+    for (int ph = 0; ph < 2; ++ph) {
+        i64(h->pair[ph].ok);
+        i64((long long)h->pair[ph].dests.size());
+        for (const auto& d : h->pair[ph].dests) i64(d.off);
+    }
+    i64((long long)h->field_is_array.size());
+    put(h->field_is_array.data(), h->field_is_array.size());
+    return k;
+}
+
+std::shared_ptr<const Built> built_find(const std::string& key) {
+    std::lock_guard<std::mutex> lk(g_built_mu);
+    for (auto it = g_built.begin(); it != g_built.end(); ++it)
+        if (it->first == key) {
+            g_built.splice(g_built.begin(), g_built, it);
+            return g_built.front().second;
+        }
+    return nullptr;
+}
+
+void built_store(const std::string& key, std::shared_ptr<const Built> b) {
+    std::lock_guard<std::mutex> lk(g_built_mu);
+    g_built.emplace_front(key, std::move(b));
+    while (g_built.size() > kBuiltMax) g_built.pop_back();
+}
+
 int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
     if (!(h->pair[0].ok && h->pair[1].ok)) {
         err = "the problem exceeds 32-bit element offsets";
@@ -2819,10 +2902,18 @@ int build_state(smg_handle* h, bool rec, JitState*& out, std::string& err) {
     }
     const int block = h->jit_block, group = h->jit_group;
     const bool calls = h->jit_calls != 0;
-    const std::vector<KernelSrc> P = programs(h, block, group, h->jit_split, calls, rec);
-    std::vector<std::vector<char>> cubins;
-    int rc = compile_programs(P, h->jit_regs, calls, cubins, err);
-    if (rc != SMG_OK) return rc;
+    const std::string gkey = generator_key(h, block, group, h->jit_split, calls, rec);
+    std::shared_ptr<const Built> B = built_find(gkey);
+    if (!B) {
+        auto nb = std::make_shared<Built>();
+        nb->P = programs(h, block, group, h->jit_split, calls, rec);
+        const int rc = compile_programs(nb->P, h->jit_regs, calls, nb->cubins, err);
+        if (rc != SMG_OK) return rc;
+        built_store(gkey, nb);
+        B = nb;
+    }
+    const std::vector<KernelSrc>& P = B->P;
+    const std::vector<std::vector<char>>& cubins = B->cubins;
     JitState* J = new JitState();
     J->block = block;
     auto fail = [&](const std::string& m) {

@@ -48,6 +48,28 @@ def test_parity_small(name, variant, monkeypatch):
     assert mism == 0, f"{name}: {mism} values differ from the oracle (worst rel L2 {worst:.3e})"
 
 
+def test_program_cache_keys_on_every_generator_input():
+    """Generated programs are shared between handles of one process when
+    their generator inputs are equal.  Problems that differ only in the grid
+    spacing, the boundary conditions, the closure (coupling weights), the
+    filter position or the array-ness of a coefficient get programs of their
+    own: in one process, alternating between them, each matches the oracle
+    bit for bit."""
+    base = cases.lattice_p5_substep()
+    probs = [base,
+             dict(base, ax=[0.0, 9.0, 0.0, 9.0]),                 # spacing
+             dict(base, bc=[0, 0]),                                # boundary conditions
+             dict(base, closure="SP"),                             # coupling weights
+             dict(base, f_position="full"),                        # filter
+             dict(base, sigma_s0=lambda x, y: 1.0)]                # an array coefficient becomes a scalar
+    for prob in probs + probs[::-1]:
+        par = starmap_init(dict(prob))
+        ref = O.starmap_solver(par)
+        out = starmap_solver(par)
+        worst, mism = compare(out, ref.output)
+        assert mism == 0, f"{mism} values differ from the oracle (worst rel L2 {worst:.3e})"
+
+
 def test_output_times_and_callback():
     """t_plot interpolation and the output hook (starmap_solver.m:425-473)."""
     prob = cases.lattice_p5_substep()
