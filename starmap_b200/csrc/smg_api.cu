@@ -269,19 +269,37 @@ int staged_transfer(smg_handle* h, bool upload, const double* const* Uin, double
     std::vector<char> partly(ns, 0);
     std::vector<size_t> nbytes(ns, 0);
     int arrays = 0, runs = 0, locked = 0;
+    std::vector<std::pair<int, int>> run_span;   // first and last array of each host-contiguous run
     const char* end = nullptr;
     for (int j = 0; j < ns; ++j) {
         host[j] = upload ? const_cast<char*>(reinterpret_cast<const char*>(Uin[j])) : reinterpret_cast<char*>(Uout[j]);
         if (!host[j]) continue;
         const int* e = h->comps[j].ext;
         nbytes[j] = (size_t)e[0] * e[1] * e[2] * sizeof(double);
-        lockdev[j] = device_view(host[j], nbytes[j]);
-        partly[j] = !lockdev[j] && host_byte_view(host[j]) != nullptr;
         ++arrays;
-        locked += lockdev[j] != nullptr;
-        if (host[j] != end) ++runs;
+        if (host[j] != end) {
+            ++runs;
+            run_span.push_back({j, j});
+        }
+        run_span.back().second = j;
         end = host[j] + nbytes[j];
     }
+    // one query pair per run when the run is page-locked and mapped as one
+    // range (arrays carved from one block), else per array
+    for (const auto& rs : run_span) {
+        const size_t span = (size_t)(host[rs.second] + nbytes[rs.second] - host[rs.first]);
+        if (double* dv = rs.first < rs.second ? device_view(host[rs.first], span) : nullptr) {
+            for (int j = rs.first; j <= rs.second; ++j)
+                if (host[j]) lockdev[j] = reinterpret_cast<double*>(reinterpret_cast<char*>(dv) + (host[j] - host[rs.first]));
+            continue;
+        }
+        for (int j = rs.first; j <= rs.second; ++j) {
+            if (!host[j]) continue;
+            lockdev[j] = device_view(host[j], nbytes[j]);
+            partly[j] = !lockdev[j] && host_byte_view(host[j]) != nullptr;
+        }
+    }
+    for (int j = 0; j < ns; ++j) locked += lockdev[j] != nullptr;
     // every array page-locked: in place, unless the arrays are carved in
     // order from one host block (a few contiguous runs), which large
     // copy-engine copies through the staging buffer move faster (about 43
