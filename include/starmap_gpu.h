@@ -127,7 +127,10 @@ int smg_create(const smg_problem* p, smg_handle** out);
 void smg_destroy(smg_handle* h);
 
 /* Upload the state: U[j] is the column-major host array of component j
- * (U{j} of starmap_solver.m:140-146).  Pointers may not be NULL. */
+ * (U{j} of starmap_solver.m:140-146).  Pointers may not be NULL.  Any host
+ * memory works; page-locked arrays move fastest (see SMG_TUNE_DIRECT_XFER),
+ * and an array page-locked only in part is copied through a host bounce
+ * buffer.  The same holds for smg_get_state and smg_get_interp. */
 int smg_set_state(smg_handle* h, const double* const* U);
 
 /* Download the state into per-component host arrays; a NULL entry skips that
