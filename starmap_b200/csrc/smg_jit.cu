@@ -2053,6 +2053,7 @@ void start_workers(std::vector<std::thread>& th, size_t n, F& work) {
 // Runs the generators on up to 16 threads; the programs keep their order.
 // An exception in a generator (out of memory) is passed on to the caller.
 std::vector<KernelSrc> run_jobs(const std::vector<std::function<KernelSrc()>>& jobs) {
+    if (jobs.empty()) return {};
     std::vector<KernelSrc> out(jobs.size());
     std::vector<std::exception_ptr> ex(jobs.size());
     std::atomic<size_t> next(0);
@@ -2708,7 +2709,7 @@ int compile_programs(const std::vector<KernelSrc>& P, int regs, bool calls, std:
         for (size_t i = next++; i < P.size(); i = next++) rcs[i] = compile_one(P[i].src, regs, link, obj[i], errs[i]);
     };
     std::vector<std::thread> th;
-    start_workers(th, std::min<size_t>(nt, P.size()) - 1, work);
+    if (!P.empty()) start_workers(th, std::min<size_t>(nt, P.size()) - 1, work);
     work();
     for (auto& t : th) t.join();
     for (size_t i = 0; i < P.size(); ++i)
